@@ -1,0 +1,355 @@
+"""Benchmark of the DG-RAIN 2D shallow-water step on B200.
+
+Workload (the "plain method at scale" configuration): the synthetic coastal rectangle
+(10 km x 5 km) on a 2,000 x 1,000-cell split mesh, 4,000,000 triangles, node
+coordinates jittered by +-10 % of the cell size (seed), p=1 CR/RT0 DG, SSP-RK2, Roe flux,
+vertex limiter, wet/dry on, tide 0.5 m / 12.42 h on the x = 0 edges, Manning n 0.03,
+CFL 0.3, FP64.  A "step" is one SSP-RK2 time step of the whole mesh (2 element-stages per
+triangle).  Metric: element-stage updates per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Rank r of N runs its own replica of the workload (generator seed 2+r): the step does not
+exchange data between meshes, so scaling is weak and no collective is on the data path;
+the only collectives are the barrier and the max-reduction of the timings.
+
+Printed on rank 0: one JSON line (value from the device-resident loop, e2e through the
+C ABI with host buffers, roofline of the dominant kernel, CPU baseline of the reference
+C step on this host, clocks sampled during the timed region).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "dg-rain_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+NX, NY, JITTER, CFL, AMP, PERIOD = 2000, 1000, 0.1, 0.3, 0.5, 44712.0
+LAND_FILM = 0.5e-3      # dry land holds H0/2 (a film of exactly H0 makes the reference stop)
+ALG_BYTES = 216         # algorithmic bytes per element-stage (state in, step input, state out)
+METRIC = "element-stage updates/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_workload(seed: int, nx=NX, ny=NY):
+    import dgrain
+
+    t0 = time.perf_counter()
+    m = dgrain.rectangle(nx, ny, jitter=JITTER, seed=seed)
+    st = dgrain.initial_state(m, np.maximum(0.0, LAND_FILM - m.z))
+    log(f"[bench] mesh {m.num_el} triangles, {m.num_nodes} nodes, {m.num_edges} edges "
+        f"built in {time.perf_counter() - t0:.1f} s")
+    return m, st
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(num_el: int):
+    """DRAM bytes per launch of the element kernel from the committed ncu summary, scaled
+    to this mesh by the number of elements (see the file for the capture)."""
+    p = os.path.join(ROOT, "profiles", "k_element_stage2_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    vals = {}
+    for line in open(p):
+        if ":" in line:
+            k, v = line.split(":", 1)
+            vals[k.strip()] = v.strip()
+    try:
+        return float(vals["dram_bytes_per_element"]) * num_el
+    except (KeyError, ValueError):
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline_reference(m, st, steps: int = 2, warmup: int = 1, max_seconds: float = 60.0):
+    """The reference C step (oracle/_ref, unmodified 2DCode compiled with gcc -O2) on this
+    host, one core, on the same mesh and state; falls back to the oracle restatement."""
+    from oracle import oracle as O
+
+    if O.have_reference():
+        r = O.Reference(wet_dry=True)
+        r.set_mesh(m)
+        r.initialize()
+        r.set_state(*st)
+        kind = "reference"
+        run = lambda n, t, d: r.run(n, 1e9, CFL, tide_on=1, amp=AMP, period=PERIOD, time=t, dt=d)  # noqa: E731
+    else:
+        r = O.Oracle(m)
+        r.set_state(*st)
+        kind = "port"
+        run = lambda n, t, d: r.run(n, 1e9, CFL, wet_dry=1, tide_on=1, amp=AMP, period=PERIOD, time=t, dt=d)  # noqa
+    rc, t, dt, n, _ = run(warmup, -1.0, 0.0)
+    done, t0 = 0, time.perf_counter()
+    while done < steps and time.perf_counter() - t0 < max_seconds:
+        rc, t, dt, n, _ = run(1, t, dt)
+        if rc:
+            break
+        done += 1
+    el = time.perf_counter() - t0
+    value = m.num_el * 2 * done / el if done else 0.0
+    return {"value": value, "unit": METRIC, "cores": 1, "kind": kind,
+            "sample": f"{done} time steps of the {m.num_el}-triangle workload after {warmup} warm-up step(s), "
+                      f"{el:.1f} s, gcc -O2 build, one host core"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    m, st = make_workload(2)
+    cb = cpu_baseline_reference(m, st, steps=max(1, args.steps), warmup=max(0, min(args.warmup, 1)),
+                                max_seconds=args.ref_seconds)
+    line = {"metric": METRIC, "value": cb["value"], "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "impl": "reference", "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "coastal rectangle 2000x1000 cells, 4,000,000 triangles, jitter 0.1, "
+                                   "p=1 SSP-RK2 Roe limiter wet/dry on, tide 0.5 m, CFL 0.3",
+                       "num_el": m.num_el},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=NX)
+    ap.add_argument("--ny", type=int, default=NY)
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-seconds", type=float, default=90.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+
+    import dgrain
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier(device_ids=[local])
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    m, st = make_workload(2 + rank, args.nx, args.ny)
+    solver = dgrain.Solver(m, wet_dry=1, cfl=CFL, tide_on=1, tide_amp=AMP, tide_period=PERIOD, device=local)
+    solver.upload_state(*st)
+
+    # warm-up: W steps of the device loop (also builds the CUDA graph)
+    t, dt, n = solver.time_evolution(1e9, args.warmup)
+    assert n == args.warmup
+
+    # ---- value: device-resident loop, K steps, inputs already in HBM ----------------
+    barrier()
+    l0 = solver.kernel_launches()
+    with ClockSampler(local) as clocks:
+        t, dt, n = solver.time_evolution(1e9, args.steps, t, dt)
+        dev_ms = solver.last_device_ms()
+    launches = solver.kernel_launches() - l0
+    barrier()
+    if n != args.steps:
+        raise RuntimeError(f"device loop stopped after {n} of {args.steps} steps: {solver.last_error()}")
+    code, idx, stp = solver.last_error()
+    if code:
+        raise RuntimeError(f"step failure code {code} at index {idx} step {stp}")
+    ms = max_over_ranks(dev_ms)
+    units = m.num_el * 2 * args.steps * world
+    value = units / (ms / 1e3)
+
+    # ---- roofline of the dominant kernel (per-launch CUDA events, same stream) --------
+    kms = solver.profile_step(3)
+    names = ["k_edge_flux", "k_element", "k_node_bounds", "k_limit"]
+    top = int(np.argmax(kms))
+    peak, peak_kind = measured_peak()
+    units_per_launch = {0: m.num_el, 1: m.num_el, 2: m.num_el, 3: m.num_el}[top]
+    achieved = ALG_BYTES * units_per_launch / (kms[top] / 1e3) / 1e9
+    traffic = ncu_traffic(m.num_el) if top == 1 else None
+
+    # ---- e2e: the reference call surface through the C ABI with host buffers ----------
+    # per step: host boundary arrays -> dgr_set_boundary (H2D of the prescribed entries),
+    # dgr_step(time, dt) -> max_lambda (D2H), host CFL update; state uploaded from pinned
+    # host memory at the start and read back at the end of the timed region.
+    e2e = None
+    if args.e2e_steps > 0:
+        import ctypes as C
+
+        lib = dgrain.load()
+        ne3 = 3 * m.num_el
+        host = {}
+        for k in ("z", "qx", "qy"):
+            p = lib.dgr_host_alloc(ne3 * 8)
+            host[k] = np.ctypeslib.as_array((C.c_double * ne3).from_address(p))
+        wdp = lib.dgr_host_alloc(m.num_el * 4)
+        host["wd"] = np.ctypeslib.as_array((C.c_int * m.num_el).from_address(wdp))
+        host["z"][:], host["qx"][:], host["qy"][:], host["wd"][:] = st
+        bz = np.zeros(m.num_edges)
+        bq = np.zeros(m.num_edges)
+        typ = m.bdry
+        nbnd = int((typ != 0).sum())
+        from dgrain.mesh import _dp, _ip
+
+        barrier()
+        t0 = time.perf_counter()
+        lib.dgr_upload_state(solver.ctx, _dp(host["z"]), _dp(host["qx"]), _dp(host["qy"]), _ip(host["wd"]))
+        tt, dtt = 0.0, 1e-7
+        lam = C.c_double()
+        for _ in range(args.e2e_steps):
+            zb = AMP * np.sin(2 * np.pi * tt / PERIOD)   # boundary_conditions() with the tide
+            bz[typ == 2], bq[typ == 2] = zb, 1e6
+            lib.dgr_set_boundary(solver.ctx, _dp(bz), _dp(bq))
+            tt = tt + dtt
+            rc = lib.dgr_step(solver.ctx, tt, dtt, C.byref(lam))
+            if rc:
+                raise RuntimeError(f"dgr_step failed: {rc}")
+            dtt = CFL * m.min_edge / lam.value
+        lib.dgr_download_state(solver.ctx, _dp(host["z"]), _dp(host["qx"]), _dp(host["qy"]), _ip(host["wd"]))
+        el = time.perf_counter() - t0
+        barrier()
+        el = max_over_ranks(el)
+        state_bytes = 9 * m.num_el * 8 + 4 * m.num_el
+        e2e = {"value": m.num_el * 2 * args.e2e_steps * world / el, "unit": METRIC,
+               "h2d_bytes_per_step": int(2 * 8 * nbnd + state_bytes / args.e2e_steps),
+               "d2h_bytes_per_step": int(8 + state_bytes / args.e2e_steps),
+               "steps": args.e2e_steps,
+               "path": "dgr_upload_state, per step dgr_set_boundary + dgr_step (oneTimeStep2D), "
+                       "dgr_download_state; pageable->pinned host buffers"}
+        for k in ("z", "qx", "qy"):
+            lib.dgr_host_free(C.c_void_p(host[k].ctypes.data))
+        lib.dgr_host_free(C.c_void_p(wdp))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_reference(m, st)
+
+    if rank == 0:
+        cs = clocks.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "coastal rectangle 2000x1000 cells (10 km x 5 km), 4,000,000 triangles, "
+                                   "jitter 0.1, p=1 CR/RT0, SSP-RK2, Roe, vertex limiter, wet/dry on, "
+                                   "tide 0.5 m / 12.42 h, Manning 0.03, CFL 0.3, FP64",
+                       "num_el": m.num_el, "num_edges": m.num_edges, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (state 288 MB, geometry 2 GB per replica); no flush"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": names[top], "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": traffic, "alg_bytes_per_unit": ALG_BYTES,
+                         "launch_ms": {n_: k for n_, k in zip(names, kms)}},
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": cs,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist is not None:
+        dist.barrier(device_ids=[local])
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

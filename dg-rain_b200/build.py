@@ -1,0 +1,84 @@
+"""Build recipe of the native library libdgrain.so (C host code + sm_100a CUDA kernels).
+
+    python dg-rain_b200/build.py            # builds dg-rain_b200/dgrain/libdgrain.so
+
+The library is built in-tree so that it travels with the repository to the GPU host.
+Flags: sm_100a only; --fmad=false keeps every multiply and add a separately rounded IEEE
+operation so that the kernels reproduce the reference C step's arithmetic.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "dgrain")
+LIB = os.path.join(OUT_DIR, "libdgrain.so")
+BUILD = os.path.join(HERE, "_build")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+]
+CC_FLAGS = ["-std=c99", "-O2", "-ffp-contract=off", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter"]
+
+CU_SOURCES = ["dgr_capi.cu"]
+C_SOURCES = ["dgr_host.c"]
+DEPS = ["dgr_kernels.cuh", "dgr_device.cuh", "dgr_forcing.h", os.path.join("..", "..", "include", "dgrain.h")]
+
+
+def _nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(cand):
+        raise RuntimeError("nvcc not found: the CUDA toolkit is required to build libdgrain.so")
+    return cand
+
+
+def _newer(target: str, sources: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def _run(cmd: list[str], verbose: bool) -> None:
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError(f"build step failed: {' '.join(cmd[:3])} ...")
+    if verbose and (res.stdout or res.stderr):
+        sys.stderr.write(res.stdout + res.stderr)
+
+
+def build(verbose: bool = False, ptxas_verbose: bool = False, force: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    nvcc = _nvcc()
+    all_src = [os.path.join(CSRC, f) for f in CU_SOURCES + C_SOURCES + DEPS]
+    if not force and not _newer(LIB, all_src + [__file__]):
+        return LIB
+    objs = []
+    for f in C_SOURCES:
+        o = os.path.join(BUILD, f + ".o")
+        _run(["gcc", *CC_FLAGS, "-c", os.path.join(CSRC, f), "-o", o], verbose)
+        objs.append(o)
+    for f in CU_SOURCES:
+        o = os.path.join(BUILD, f + ".o")
+        extra = ["-Xptxas", "-v"] if ptxas_verbose else []
+        _run([nvcc, *NVCC_FLAGS, *extra, "-c", os.path.join(CSRC, f), "-o", o], verbose or ptxas_verbose)
+        objs.append(o)
+    tmp = LIB + ".tmp"
+    _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs, "-lm"], verbose)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    path = build(verbose=True, ptxas_verbose="-v" in sys.argv, force="-f" in sys.argv)
+    print(path)

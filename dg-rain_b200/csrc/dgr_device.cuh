@@ -1,0 +1,126 @@
+/*
+ * Device arithmetic of the DG-RAIN 2D step.
+ *
+ * Every function here evaluates the reference's expressions in the reference's order and
+ * parenthesisation, and the library is compiled with --fmad=false, so each multiply, add,
+ * divide and square root is one IEEE operation exactly as in the reference's C.  The only
+ * library call whose last bit may differ from the host is pow(H, 4/3) in the Manning term.
+ */
+#pragma once
+
+#include <cstdint>
+
+#define DGR_DEV __device__ __forceinline__
+
+namespace dgr {
+
+/* sign() of 2DCode/mathfunctions.c:4-12 */
+DGR_DEV int sgn(double a)
+{
+    if (a < 0) return -1;
+    if (a == 0) return 0;
+    return 1;
+}
+/* max()/min() macros of 2DCode/mathfunctions.h:8-14 (not fmax/fmin: NaN order matters) */
+DGR_DEV double rmax(double a, double b) { return (a > b) ? a : b; }
+DGR_DEV double rmin(double a, double b) { return (a < b) ? a : b; }
+
+/* Dense 3x3 times vector, summed from +0 in column order (2DCode/mathfunctions.c:24-35). */
+DGR_DEV void matvec3(const double m[3][3], const double v[3], double out[3])
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        double s = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) s += m[i][j] * v[j];
+        out[i] = s;
+    }
+}
+
+/* Roe flux with entropy fix, 2DCode/numericalFlux2D.c:6-108.  Returns max |lambda| of the
+ * two traces.  local_g scales the pressure term only; g sets the eigen-structure. */
+DGR_DEV double roe_flux(double fh[3], double zeta_in, double zeta_ex, double qx_in, double qx_ex,
+                        double qy_in, double qy_ex, double z_edge, double nx, double ny,
+                        double local_g, double g)
+{
+    const double h_in = zeta_in + z_edge;
+    const double h_ex = zeta_ex + z_edge;
+    const double u_in = qx_in / h_in, u_ex = qx_ex / h_ex;
+    const double v_in = qy_in / h_in, v_ex = qy_ex / h_ex;
+    const double jump[3] = {zeta_in - zeta_ex, qx_in - qx_ex, qy_in - qy_ex};
+
+    const double p_in = 0.5 * local_g * (h_in * h_in - z_edge * z_edge);
+    const double p_ex = 0.5 * local_g * (h_ex * h_ex - z_edge * z_edge);
+    const double huv_in = h_in * u_in * v_in, huv_ex = h_ex * u_ex * v_ex;
+    const double fn_in[3] = {h_in * u_in * nx + h_in * v_in * ny,
+                             (h_in * u_in * u_in + p_in) * nx + huv_in * ny,
+                             huv_in * nx + (h_in * v_in * v_in + p_in) * ny};
+    const double fn_ex[3] = {h_ex * u_ex * nx + h_ex * v_ex * ny,
+                             (h_ex * u_ex * u_ex + p_ex) * nx + huv_ex * ny,
+                             huv_ex * nx + (h_ex * v_ex * v_ex + p_ex) * ny};
+
+    const double s_in = sqrt(h_in), s_ex = sqrt(h_ex);
+    const double h_hat = 0.5 * (h_in + h_ex);
+    const double u_hat = (u_in * s_in + u_ex * s_ex) / (s_in + s_ex);
+    const double v_hat = (v_in * s_in + v_ex * s_ex) / (s_in + s_ex);
+    const double c = sqrt(g * h_hat);
+
+    const double r[3][3] = {{1, 0, 1}, {u_hat - c * nx, -ny, u_hat + c * nx}, {v_hat - c * ny, nx, v_hat + c * ny}};
+    const double den = -2 * c;
+    const double ri[3][3] = {{(-c - nx * u_hat - ny * v_hat) / den, nx / den, ny / den},
+                             {(-2 * c * ny * u_hat + 2 * c * nx * v_hat) / den, 2 * c * ny / den, -2 * c * nx / den},
+                             {(-c + nx * u_hat + ny * v_hat) / den, -nx / den, -ny / den}};
+
+    const double un_in = u_in * nx + v_in * ny, un_ex = u_ex * nx + v_ex * ny;
+    const double c_in = sqrt(g * h_in), c_ex = sqrt(g * h_ex);
+    const double l1_in = un_in - c_in, l2_in = un_in, l3_in = un_in + c_in;
+    const double l1_ex = un_ex - c_ex, l2_ex = un_ex, l3_ex = un_ex + c_ex;
+    const double un_hat = u_hat * nx + v_hat * ny;
+    double lh1 = un_hat - c, lh2 = un_hat, lh3 = un_hat + c;
+
+    double e1 = fmax(0.0, (lh1 - l1_in));
+    e1 = fmax(e1, (l1_ex - lh1));
+    lh1 = fmax(e1, fabs(lh1));
+    double e2 = fmax(0.0, (lh2 - l2_in));
+    e2 = fmax(e2, (l2_ex - lh2));
+    lh2 = fmax(e2, fabs(lh2));
+    double e3 = fmax(0.0, (lh3 - l3_in));
+    e3 = fmax(e3, (l3_ex - lh3));
+    lh3 = fmax(e3, fabs(lh3));
+
+    const double lam[3][3] = {{lh1, 0, 0}, {0, lh2, 0}, {0, 0, lh3}};
+    double p1[3], p2[3], p3[3];
+    matvec3(ri, jump, p1);
+    matvec3(lam, p1, p2);
+    matvec3(r, p2, p3);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) fh[k] = 0.5 * (fn_in[k] + fn_ex[k]) + 0.5 * p3[k];
+
+    double m = rmax(fabs(l1_in), fabs(l1_ex));
+    m = rmax(m, fabs(l2_in));
+    m = rmax(m, fabs(l2_ex));
+    m = rmax(m, fabs(l3_in));
+    m = rmax(m, fabs(l3_ex));
+    return m;
+}
+
+/* RT0 fit F = (a + b x, c + b y) through three normal-flux values (Cramer's rule of
+ * 2DCode/2DInnerProducts.c:134-146 and :507-519). */
+DGR_DEV void rt0_fit(double R1, double R2, double R3, double M11, double M12, double M13, double M21,
+                     double M22, double M23, double M31, double M32, double M33, double dM, double &a,
+                     double &b, double &c)
+{
+    a = (R3 * M13 * M22 - R3 * M12 * M23 - R2 * M13 * M32 + R1 * M23 * M32 + R2 * M12 * M33 - R1 * M22 * M33) / dM;
+    b = -(R3 * M13 * M21 - R3 * M11 * M23 - R2 * M13 * M31 + R1 * M23 * M31 + R2 * M11 * M33 - R1 * M21 * M33) / dM;
+    c = (R3 * M12 * M21 - R3 * M11 * M22 - R2 * M12 * M31 + R1 * M22 * M31 + R2 * M11 * M32 - R1 * M21 * M32) / dM;
+}
+
+/* Status key: earlier step, then earlier phase, then lower index wins under atomicMin,
+ * which is the failure the sequential reference would have stopped at. */
+DGR_DEV unsigned long long err_key(int step, int phase, int code, int index)
+{
+    return ((unsigned long long)(unsigned)step << 40) | ((unsigned long long)(phase & 15) << 36) |
+           ((unsigned long long)(code & 15) << 32) | (unsigned long long)(unsigned)index;
+}
+
+}  // namespace dgr

@@ -1,0 +1,175 @@
+"""Python mirror of the reference 2DCode call surface over the C ABI.
+
+Method names follow the reference functions they replace (2DCode/compute2DL.c:12,
+SlopeLimiter2D.c:10, wetDry2D.c:16 and :63, time_evolution.c:10 and :248,
+boundary_conditions.c:9); arrays use the reference layout [3*el+k].  Where the reference
+prints a message and exits, these methods raise StepError carrying the same code and the
+edge or element index the reference would have printed.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .mesh import Mesh, _dp, _ip
+
+
+class StepError(RuntimeError):
+    def __init__(self, code: int, index: int, step: int, where: str):
+        self.code, self.index, self.step = code, index, step
+        super().__init__(f"{where}: {_lib.status_string(code)} (code {code}) at index {index}, step {step}")
+
+
+def default_params(**overrides) -> _lib.DgrParams:
+    p = _lib.DgrParams()
+    _lib.check(_lib.load().dgr_params_default(C.byref(p)), "dgr_params_default")
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise KeyError(f"unknown parameter {k}")
+        setattr(p, k, v)
+    return p
+
+
+class Solver:
+    """One mesh on one GPU (a dgr_ctx)."""
+
+    def __init__(self, mesh: Mesh, params: _lib.DgrParams | None = None, **overrides):
+        self.lib = _lib.load()
+        self.mesh = mesh
+        self.params = params if params is not None else default_params(**overrides)
+        self._view = mesh.view()
+        h = C.c_void_p()
+        _lib.check(self.lib.dgr_create(C.byref(self._view), C.byref(self.params), C.byref(h)), "dgr_create")
+        self.ctx = h
+        self.ne = mesh.num_el
+        self.nf = mesh.num_edges
+
+    # ------------------------------------------------------------------ life ----
+    def close(self) -> None:
+        if self.ctx:
+            self.lib.dgr_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, **kw) -> None:
+        for k, v in kw.items():
+            setattr(self.params, k, v)
+        _lib.check(self.lib.dgr_set_params(self.ctx, C.byref(self.params)), "dgr_set_params")
+
+    def set_element_manning(self, n_el: np.ndarray | None) -> None:
+        if n_el is None:
+            _lib.check(self.lib.dgr_set_element_manning(self.ctx, None), "dgr_set_element_manning")
+            return
+        n_el = np.ascontiguousarray(n_el, dtype=np.float64)
+        assert n_el.shape == (self.ne,)
+        _lib.check(self.lib.dgr_set_element_manning(self.ctx, _dp(n_el)), "dgr_set_element_manning")
+
+    # ----------------------------------------------------------------- state ----
+    def upload_state(self, zeta, qx, qy, wd=None) -> None:
+        z = np.ascontiguousarray(zeta, dtype=np.float64)
+        x = np.ascontiguousarray(qx, dtype=np.float64)
+        y = np.ascontiguousarray(qy, dtype=np.float64)
+        assert z.shape == x.shape == y.shape == (3 * self.ne,)
+        w = None if wd is None else np.ascontiguousarray(wd, dtype=np.int32)
+        _lib.check(self.lib.dgr_upload_state(self.ctx, _dp(z), _dp(x), _dp(y), None if w is None else _ip(w)),
+                   "dgr_upload_state")
+
+    def download_state(self):
+        z = np.empty(3 * self.ne)
+        x = np.empty(3 * self.ne)
+        y = np.empty(3 * self.ne)
+        w = np.empty(self.ne, dtype=np.int32)
+        _lib.check(self.lib.dgr_download_state(self.ctx, _dp(z), _dp(x), _dp(y), _ip(w)), "dgr_download_state")
+        return z, x, y, w
+
+    def set_boundary(self, bzeta, bqn) -> None:
+        bz = np.ascontiguousarray(bzeta, dtype=np.float64)
+        bq = np.ascontiguousarray(bqn, dtype=np.float64)
+        _lib.check(self.lib.dgr_set_boundary(self.ctx, _dp(bz), _dp(bq)), "dgr_set_boundary")
+
+    def boundary_conditions(self, time: float = 0.0) -> None:
+        _lib.check(self.lib.dgr_boundary_conditions(self.ctx, time), "dgr_boundary_conditions")
+
+    # ------------------------------------------------------------- operators ----
+    def _status(self, rc: int, where: str) -> None:
+        if rc == _lib.DGR_OK:
+            return
+        if 1 <= rc <= 6:
+            code, index, step = C.c_int(), C.c_int(), C.c_int()
+            self.lib.dgr_last_error(self.ctx, C.byref(code), C.byref(index), C.byref(step))
+            raise StepError(code.value, index.value, step.value, where)
+        _lib.check(rc, where)
+
+    def compute2DL(self, time: float = 0.0):
+        rz = np.empty(3 * self.ne)
+        rx = np.empty(3 * self.ne)
+        ry = np.empty(3 * self.ne)
+        lam = C.c_double()
+        self._status(self.lib.dgr_compute_L(self.ctx, time, _dp(rz), _dp(rx), _dp(ry), C.byref(lam)), "compute2DL")
+        return rz, rx, ry, lam.value
+
+    def SlopeLimiter(self) -> None:  # noqa: N802 (reference name)
+        self._status(self.lib.dgr_slope_limiter(self.ctx), "SlopeLimiter")
+
+    def PDop2D(self) -> None:  # noqa: N802
+        self._status(self.lib.dgr_pdop(self.ctx), "PDop2D")
+
+    def wetDryStatus2D(self) -> None:  # noqa: N802
+        self._status(self.lib.dgr_wet_dry_status(self.ctx), "wetDryStatus2D")
+
+    def oneTimeStep2D(self, time: float, dt: float) -> float:  # noqa: N802
+        lam = C.c_double()
+        self._status(self.lib.dgr_step(self.ctx, time, dt, C.byref(lam)), "oneTimeStep2D")
+        return lam.value
+
+    def time_evolution(self, final_time: float, nsteps: int, time: float = -1.0, dt: float = 0.0):
+        """Device-resident loop; returns (time, next dt, steps done)."""
+        t = C.c_double(time)
+        d = C.c_double(dt)
+        n = C.c_int(0)
+        self._status(self.lib.dgr_run(self.ctx, nsteps, final_time, C.byref(t), C.byref(d), C.byref(n)),
+                     "time_evolution")
+        return t.value, d.value, n.value
+
+    # ------------------------------------------------------------ diagnostics ----
+    def last_error(self):
+        code, index, step = C.c_int(), C.c_int(), C.c_int()
+        _lib.check(self.lib.dgr_last_error(self.ctx, C.byref(code), C.byref(index), C.byref(step)),
+                   "dgr_last_error")
+        return code.value, index.value, step.value
+
+    def decisions(self, stage: int):
+        lim = np.empty(self.ne, dtype=np.int32)
+        pd = np.empty(self.ne, dtype=np.int32)
+        _lib.check(self.lib.dgr_get_decisions(self.ctx, stage, _ip(lim), _ip(pd)), "dgr_get_decisions")
+        return lim, pd
+
+    def fhat(self):
+        f = [np.empty(3 * self.ne) for _ in range(3)]
+        _lib.check(self.lib.dgr_get_fhat(self.ctx, *[_dp(a) for a in f]), "dgr_get_fhat")
+        return tuple(f)
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.dgr_kernel_launches(self.ctx))
+
+    def last_device_ms(self) -> float:
+        return float(self.lib.dgr_last_device_ms(self.ctx))
+
+    def profile_step(self, nsteps: int = 3):
+        """Average device ms per launch of (edge flux, element, node bounds, limiter)."""
+        out = (C.c_double * 4)()
+        self._status(self.lib.dgr_profile_step(self.ctx, nsteps, out, 4), "dgr_profile_step")
+        return list(out)

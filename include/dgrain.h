@@ -1,0 +1,221 @@
+/*
+ * dgrain.h — C ABI of the B200 DG-RAIN 2D shallow-water step.
+ *
+ * The reference (evalseth/DG-RAIN, 2DCode/) has no library interface: its step is a set
+ * of link-level C functions over process-wide globals (2DCode/MeshAttributes.h:5-42).
+ * This header replaces those functions one for one, with an explicit context instead of
+ * globals and an int status instead of exit():
+ *
+ *   reference (2DCode/)                                   this ABI
+ *   store_mesh(char*)            extract_mesh_attributes.c:39    dgr_read_fort14()
+ *   extract_mesh_attributes()    extract_mesh_attributes.c:143   dgr_build_connectivity()
+ *   initialize()                 initialize.c:29                 dgr_initial_state()
+ *   boundary_conditions()        boundary_conditions.c:9         dgr_set_boundary() / dgr_boundary_conditions()
+ *   compute2DL(double)           compute2DL.c:12                 dgr_compute_L()
+ *   SlopeLimiter()               SlopeLimiter2D.c:10             dgr_slope_limiter()
+ *   wetDryStatus2D()             wetDry2D.c:16                   dgr_wet_dry_status()
+ *   PDop2D()                     wetDry2D.c:63                   dgr_pdop()
+ *   oneTimeStep2D(double,double) time_evolution.c:10             dgr_step()
+ *   time_evolution(double)       time_evolution.c:248            dgr_run()
+ *   .dat writer                  time_evolution.c:324-390        dgr_write_dat()
+ *
+ * Data layout at this boundary is the reference's: state arrays are double[3*NumEl]
+ * indexed [3*el+k] with k the local edge (v_k, v_{(k+1)%3}); mesh arrays are the
+ * reference's EltoVert[3*NumEl], EdgtoEls[2*NumEdges], EdgtoVert[2*NumEdges],
+ * BdryPrescribed[NumEdges] with 0-based indices.  Ownership stays with the caller: every
+ * array passed in is copied before the call returns.
+ *
+ * Errors: every function returns DGR_OK (0) or a DGR_ERR_* code.  The numerical failures
+ * that make the reference print a message and exit (2DCode/compute2DL.c:245-302,
+ * 2DCode/wetDry2D.c:142-146,233-237) are returned as codes 1-5, and dgr_last_error()
+ * gives the edge or element index the reference would have printed.
+ *
+ * Threading: a context belongs to one host thread at a time and owns one CUDA stream.
+ * Separate contexts may be used from separate threads.
+ */
+#ifndef DGRAIN_H
+#define DGRAIN_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGR_ABI_VERSION 1
+
+/* Exported entry points keep default visibility in a library built with
+ * -fvisibility=hidden. */
+#if defined(__GNUC__)
+#define DGR_API __attribute__((visibility("default")))
+#else
+#define DGR_API
+#endif
+
+enum dgr_status {
+    DGR_OK = 0,
+    DGR_ERR_NAN_FLUX = 1,     /* 2DCode/compute2DL.c:245-249 and :298-302 */
+    DGR_ERR_NAN_FLUX_IN = 2,  /* 2DCode/compute2DL.c:262-266 */
+    DGR_ERR_NAN_FLUX_EX = 3,  /* 2DCode/compute2DL.c:281-285 */
+    DGR_ERR_NEG_DEPTH = 4,    /* 2DCode/wetDry2D.c:142-146 */
+    DGR_ERR_NAN_VELOCITY = 5, /* 2DCode/wetDry2D.c:233-237 */
+    DGR_ERR_EDGE_MATCH = 6,   /* 2DCode/compute2DL.c:51-67 */
+    DGR_ERR_INVALID = 10,     /* bad argument */
+    DGR_ERR_MESH = 11,        /* inconsistent mesh (edge count, uncovered element edge) */
+    DGR_ERR_IO = 12,          /* file cannot be read or written */
+    DGR_ERR_CUDA = 13,        /* a CUDA call failed; see dgr_last_cuda_error() */
+    DGR_ERR_NO_DEVICE = 14,   /* no CUDA device: this library has no CPU fallback */
+    DGR_ERR_TOO_LARGE = 15    /* size beyond a documented limit */
+};
+
+/* Run parameters.  dgr_params_default() fills the reference's constants. */
+typedef struct dgr_params {
+    double g;        /* 9.81   2DCode/initialize.c:22 */
+    double H0;       /* 1e-3   2DCode/initialize.c:26 */
+    double VELZERO;  /* 1e-2   2DCode/initialize.c:27 */
+    double cfl;      /* 0.1    2DCode/time_evolution.c:399 */
+    double dt0;      /* 1e-7   2DCode/time_evolution.c:255 */
+    int wet_dry;     /* 1: wet/dry on — compute2DL's WDON flux branch plus wetDryStatus2D and
+                        PDop2D in the order of ChanNet/time_evolution.c:218-427.
+                        0: the step exactly as 2DCode ships it. Default 1. */
+    int tide_on;     /* 1: type-2 (outflow-list) edges get zeta_b = tide_amp*sin(2*pi*t/tide_period)
+                        instead of 0.296 (extension; the reference has no tide). Default 0. */
+    double tide_amp;
+    double tide_period;
+    double rain;     /* m/s added to the elevation right-hand side (extension). Default 0. */
+    int device;      /* CUDA device ordinal. Default 0. */
+    int record_decisions; /* 1: keep per-element limiter/PDop decisions of the last step. */
+} dgr_params;
+
+/* Mesh in the reference's arrays (2DCode/MeshAttributes.h:5-20), 0-based. */
+typedef struct dgr_mesh_view {
+    int num_el, num_nodes, num_edges;
+    const double *x_coord, *y_coord; /* [num_nodes] */
+    const double *z;                 /* [num_nodes] depth, positive down */
+    const double *nFriction;         /* [num_nodes] Manning n */
+    const int *EltoVert;             /* [3*num_el] */
+    const int *EdgtoEls;             /* [2*num_edges]; boundary edges repeat the element */
+    const int *EdgtoVert;            /* [2*num_edges] */
+    const int *BdryPrescribed;       /* [num_edges] 0 land, 1 inflow, 2 outflow, 3 inflow-2 */
+    double minEdgLength;             /* 2DCode/extract_mesh_attributes.c:303 */
+} dgr_mesh_view;
+
+/* A mesh as read from a fort.14 file of the 2DCode dialect
+ * (2DCode/extract_mesh_attributes.c:39-141): node lines carry "id x y z n". */
+typedef struct dgr_fort14 {
+    int num_el, num_nodes;
+    double *x_coord, *y_coord, *z, *nFriction;
+    int *EltoVert;                        /* 0-based */
+    int num_inflow1, num_inflow2, num_outflow;
+    int *inflow1, *inflow2, *outflow;     /* node pairs, 0-based, 2 per edge */
+} dgr_fort14;
+
+typedef struct dgr_ctx dgr_ctx;
+
+DGR_API const char *dgr_status_string(int code);
+DGR_API int dgr_abi_version(void);
+
+/* ---- host-side mesh ingest (C, no GPU needed) ---------------------------------- */
+
+/* store_mesh (2DCode/extract_mesh_attributes.c:39-141).  *out is freed by
+ * dgr_fort14_free. */
+DGR_API int dgr_read_fort14(const char *path, dgr_fort14 **out);
+DGR_API void dgr_fort14_free(dgr_fort14 *m);
+
+/* extract_mesh_attributes (2DCode/extract_mesh_attributes.c:143-361) with hashing
+ * instead of the O(E*N) search; the outputs are identical, edge order and element slot
+ * order included.  Output arrays hold num_nodes+num_el-1 edges (Euler's relation, which
+ * the reference also requires, :218-257); DGR_ERR_MESH if the mesh breaks it.
+ * Boundary lists are node pairs, 0-based. */
+DGR_API int dgr_count_edges(int num_el, int num_nodes, const int *EltoVert, int *num_edges);
+DGR_API int dgr_build_connectivity(int num_el, int num_nodes, const int *EltoVert,
+                           const double *x_coord, const double *y_coord,
+                           int num_inflow1, const int *inflow1,
+                           int num_inflow2, const int *inflow2,
+                           int num_outflow, const int *outflow,
+                           int *EdgtoVert, int *EdgtoEls, int *BdryPrescribed,
+                           double *minEdgLength);
+
+/* initialize (2DCode/initialize.c:117-126): nodal elevations averaged onto the edge
+ * midpoints, zero discharge, WD = -1.  zeta_nodal == NULL gives the reference's 0.1. */
+DGR_API int dgr_initial_state(int num_el, const int *EltoVert, const double *zeta_nodal,
+                      double *zeta, double *Qx, double *Qy, int *WD);
+
+/* Writes one .dat file in the reference format (time_evolution.c:284-306,363-386):
+ * one element per line, its three values as "%1.15f\t\t". */
+DGR_API int dgr_write_dat(const char *path, int num_el, const double *values);
+
+/* Page-locked host memory for fast copies (cudaHostAlloc); NULL on failure. */
+DGR_API void *dgr_host_alloc(size_t bytes);
+DGR_API void dgr_host_free(void *p);
+
+/* ---- device context ------------------------------------------------------------- */
+
+DGR_API int dgr_params_default(dgr_params *p);
+DGR_API int dgr_create(const dgr_mesh_view *mesh, const dgr_params *params, dgr_ctx **out);
+DGR_API int dgr_destroy(dgr_ctx *ctx);
+DGR_API int dgr_get_params(const dgr_ctx *ctx, dgr_params *out);
+/* Only rain, tide_on, tide_amp, tide_period, cfl, dt0 and record_decisions may change. */
+DGR_API int dgr_set_params(dgr_ctx *ctx, const dgr_params *params);
+/* Per-element Manning n (extension); NULL restores the node average of
+ * 2DCode/2DInnerProducts.c:272-274. */
+DGR_API int dgr_set_element_manning(dgr_ctx *ctx, const double *n_el);
+
+/* State in the reference layout.  Upload clears the error word and marks the wet/dry
+ * flags stale, so the next step starts with wetDryStatus2D as the reference does. */
+DGR_API int dgr_upload_state(dgr_ctx *ctx, const double *zeta, const double *Qx, const double *Qy,
+                     const int *WD);
+DGR_API int dgr_download_state(dgr_ctx *ctx, double *zeta, double *Qx, double *Qy, int *WD);
+
+/* boundary_conditions(): the caller's bzeta/bQn arrays ([NumEdges], only prescribed
+ * edges are read) ... */
+DGR_API int dgr_set_boundary(dgr_ctx *ctx, const double *bzeta, const double *bQn);
+/* ... or the device fills them for time t from the reference constants and the tide. */
+DGR_API int dgr_boundary_conditions(dgr_ctx *ctx, double time);
+
+/* Single operators on the device state, for drop-in use and parity checks. */
+DGR_API int dgr_compute_L(dgr_ctx *ctx, double time, double *RHSZeta, double *RHSQx, double *RHSQy,
+                  double *max_lambda);
+DGR_API int dgr_slope_limiter(dgr_ctx *ctx);
+DGR_API int dgr_pdop(dgr_ctx *ctx);
+DGR_API int dgr_wet_dry_status(dgr_ctx *ctx);
+
+/* oneTimeStep2D(time, dt): one SSP-RK2 step of the device state with the current
+ * boundary values; returns the max wave speed of the second stage (the reference's
+ * max_lambda), from which the caller sets the next dt. */
+DGR_API int dgr_step(dgr_ctx *ctx, double time, double dt, double *max_lambda);
+
+/* time_evolution(): up to nsteps steps while time < final_time, entirely on the device
+ * (CFL dt, boundary forcing and clock stay on the GPU; one host sync at the end).
+ * *time_io < 0 starts a new run at t = 0 with dt = dt0; otherwise (*time_io, *dt_io)
+ * continue a previous run.  The steps of one call are replayed from a CUDA graph. */
+DGR_API int dgr_run(dgr_ctx *ctx, int nsteps, double final_time, double *time_io, double *dt_io,
+            int *steps_done);
+
+/* First failure since the last upload: status code, edge or element index, step. */
+DGR_API int dgr_last_error(dgr_ctx *ctx, int *code, int *index, int *step);
+DGR_API const char *dgr_last_cuda_error(void);
+
+/* Per-element decisions of the last step (needs record_decisions = 1).  stage 0 or 1.
+ * limit[el] = 1 when the limiter rewrote the element; pdop[el] = 4*mass + momentum
+ * branch (see oracle/dgr_oracle.h for the branch numbering). */
+DGR_API int dgr_get_decisions(dgr_ctx *ctx, int stage, int *limit, int *pdop);
+/* Numerical fluxes of the last L evaluation in the reference's Fhat{1,2,3}dotn layout. */
+DGR_API int dgr_get_fhat(dgr_ctx *ctx, double *F1, double *F2, double *F3);
+
+/* Number of kernels this context has launched since creation (all launches, graph
+ * replays included). */
+DGR_API long long dgr_kernel_launches(const dgr_ctx *ctx);
+/* Device time of the last dgr_run/dgr_step call in ms (CUDA events on the context's
+ * stream). */
+DGR_API double dgr_last_device_ms(const dgr_ctx *ctx);
+/* Runs nsteps steps with CUDA events around every launch; kernel_ms[0..3] (n >= 4)
+ * receive the average ms of one launch of: edge flux, element RHS + RK update, node
+ * bounds, limiter + PDop. */
+DGR_API int dgr_profile_step(dgr_ctx *ctx, int nsteps, double *kernel_ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

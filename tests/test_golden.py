@@ -1,0 +1,55 @@
+"""The oracle restatement against golden vectors that the unmodified reference wrote
+(tests/golden/make_golden.py).  Runs everywhere: no reference tree, no GPU needed."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import load_golden, mesh_from_golden
+
+
+@pytest.mark.parametrize("flag", [0, 1])
+def test_oracle_compute2DL_golden(dgrain, oracle_mod, flag):
+    g = load_golden("compute2DL_jittered576.npz")
+    m = mesh_from_golden(dgrain, g)
+    # the generator and the native connectivity builder still give the stored mesh
+    m2 = dgrain.rectangle(24, 12, jitter=0.1, seed=5)
+    for k in ("x", "y", "z", "el2v", "ed2v", "ed2el", "bdry"):
+        assert np.array_equal(getattr(m2, k), g[k]), k
+    orc = oracle_mod.Oracle(m)
+    wd = g["wd_rand"] if flag else np.full(m.num_el, -1, dtype=np.int32)
+    orc.set_state(g["zeta"], g["qx"], g["qy"], wd)
+    orc.set_bc(g["bzeta"], g["bqn"])
+    rc, rz, rx, ry, lam = orc.compute_L(flag)
+    assert rc == 0
+    assert np.array_equal(rz, g[f"wd{flag}_rhs_zeta"])
+    assert np.array_equal(rx, g[f"wd{flag}_rhs_qx"])
+    assert np.array_equal(ry, g[f"wd{flag}_rhs_qy"])
+    assert lam == float(g[f"wd{flag}_max_lambda"])
+    for a, k in zip(orc.fhat(), ("f1", "f2", "f3")):
+        assert np.array_equal(a, g[f"wd{flag}_{k}"])
+
+
+def test_oracle_run_golden(dgrain, oracle_mod):
+    g = load_golden("run120_wd_tide_rect1600.npz")
+    m = mesh_from_golden(dgrain, g)
+    orc = oracle_mod.Oracle(m)
+    orc.set_state(g["zeta0"], g["qx0"], g["qy0"], g["wd0"])
+    rc, t, dt, n, hist = orc.run(120, 1e9, 0.3, wet_dry=1, tide_on=1, amp=0.5, want_dt=True)
+    assert rc == 0 and n == 120
+    z, qx, qy, wd = orc.get_state()
+    assert np.array_equal(z, g["zeta"]) and np.array_equal(qx, g["qx"]) and np.array_equal(qy, g["qy"])
+    assert np.array_equal(wd, g["wd"])
+    assert t == float(g["time"]) and dt == float(g["dt_next"])
+    assert np.array_equal(hist, g["dt_hist"])
+
+
+def test_oracle_failure_golden(dgrain, oracle_mod):
+    g = load_golden("failure_film_h0_rect1600.npz")
+    m = mesh_from_golden(dgrain, g)
+    orc = oracle_mod.Oracle(m)
+    orc.set_state(g["zeta0"], g["qx0"], g["qy0"], g["wd0"])
+    rc, t, dt, n, _ = orc.run(50, 1e9, 0.3, wet_dry=1, tide_on=1, amp=0.5)
+    code, idx = orc.last_error()
+    assert rc == code == 1
+    assert idx == int(g["fail_edge"]) and n == int(g["steps_done"])

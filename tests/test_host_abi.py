@@ -1,0 +1,92 @@
+"""The C ABI without a GPU: the library loads, exports every entry point that
+include/dgrain.h declares, and its host-side functions (fort.14 reader, connectivity,
+initial state, .dat writer) behave like the reference's."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, has_gpu
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "dgrain.h")).read()
+    return sorted(set(re.findall(r"^DGR_API [^;(]*?\b(dgr_\w+)\(", text, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol(dgrain):
+    lib = dgrain.load()
+    names = declared_symbols()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(lib, n), n
+    bound = {n for n, _, _ in dgrain._lib.SIGNATURES}
+    assert set(names) == bound, set(names) ^ bound
+    assert lib.dgr_abi_version() == 1
+    assert dgrain._lib.status_string(1) == "numerical flux not a number"
+
+
+def test_fort14_roundtrip_and_connectivity(dgrain, tmp_path):
+    m = dgrain.rectangle(9, 5, jitter=0.1, seed=2)
+    p = str(tmp_path / "a.14")
+    dgrain.write_fort14(m, p)
+    m2 = dgrain.read_fort14(p)
+    for k in ("x", "y", "z", "nfric", "el2v", "outflow", "ed2v", "ed2el", "bdry"):
+        assert np.array_equal(getattr(m, k), getattr(m2, k)), k
+    assert m.min_edge == m2.min_edge
+    assert m.num_edges == m.num_nodes + m.num_el - 1
+    # boundary edges repeat their element; interior edges list the lower element first
+    bd = m.ed2el[:, 0] == m.ed2el[:, 1]
+    assert bd.sum() == 2 * (9 + 5)
+    assert np.all(m.ed2el[~bd, 0] < m.ed2el[~bd, 1])
+    assert (m.bdry == 2).sum() == 5
+
+
+def test_fort14_errors(dgrain, tmp_path):
+    p = tmp_path / "bad.14"
+    p.write_text("title\n2 3\n1 0 0 0 0.03\n")
+    with pytest.raises(dgrain.DgrError) as ei:
+        dgrain.read_fort14(str(p))
+    assert ei.value.code == dgrain._lib.DGR_ERR_IO
+    with pytest.raises(dgrain.DgrError):
+        dgrain.read_fort14(str(tmp_path / "missing.14"))
+
+
+def test_mesh_breaking_euler_relation_is_rejected(dgrain):
+    # two separate triangles: NumEdges (6) != NumNodes + NumEl - 1 (7)
+    m = dgrain.Mesh(x=np.array([0, 1, 0, 5, 6, 5.0]), y=np.array([0, 0, 1, 0, 0, 1.0]), z=np.zeros(6),
+                    nfric=np.zeros(6), el2v=np.array([[0, 1, 2], [3, 4, 5]], dtype=np.int32),
+                    inflow1=np.zeros((0, 2), np.int32), inflow2=np.zeros((0, 2), np.int32),
+                    outflow=np.zeros((0, 2), np.int32))
+    with pytest.raises(dgrain.DgrError) as ei:
+        dgrain.build_connectivity(m)
+    assert ei.value.code == dgrain._lib.DGR_ERR_MESH
+
+
+def test_initial_state_and_dat_writer(dgrain, tmp_path):
+    m = dgrain.rectangle(4, 2, seed=1)
+    z, qx, qy, wd = dgrain.initial_state(m, np.arange(m.num_nodes, dtype=np.float64))
+    el = 3
+    v = m.el2v[el]
+    assert z[3 * el] == 0.5 * (v[0] + v[1]) and z[3 * el + 2] == 0.5 * (v[2] + v[0])
+    assert not qx.any() and not qy.any() and (wd == -1).all()
+    lib = dgrain.load()
+    p = str(tmp_path / "001_H.dat")
+    assert lib.dgr_write_dat(p.encode(), m.num_el, z.ctypes.data_as(dgrain._lib.dptr)) == 0
+    lines = open(p).read().splitlines()
+    assert len(lines) == m.num_el
+    assert lines[0] == "\t\t".join("%1.15f" % x for x in z[:3]) + "\t\t"
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-GPU path")
+def test_device_calls_fail_loudly_without_gpu(dgrain):
+    m = dgrain.rectangle(4, 2, seed=1)
+    with pytest.raises(dgrain.DgrError) as ei:
+        dgrain.Solver(m)
+    assert ei.value.code == dgrain._lib.DGR_ERR_NO_DEVICE
+    p = dgrain.default_params()
+    assert p.g == 9.81 and p.H0 == 1e-3 and p.VELZERO == 1e-2 and p.cfl == 0.1 and p.dt0 == 1e-7
