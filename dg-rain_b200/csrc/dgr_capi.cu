@@ -55,7 +55,7 @@ struct dgr_ctx {
     int *bdry;
     double *e_geo, *geo;
     /* state and work */
-    double *U, *W, *flux, *avg, *bounds, *bzeta, *bqn;
+    double *U, *W, *flux, *avg, *bounds, *bzeta, *bqn, *bstage;
     int *wdA, *wdB;
     int *dec;  /* [4][ne]: limit s0, pdop s0, limit s1, pdop s1 */
     DevClock *clk;
@@ -153,7 +153,7 @@ static void release(dgr_ctx *c)
     if (c->graph) cudaGraphDestroy(c->graph);
     void *ptrs[] = {c->x, c->y, c->zn, c->nfric, c->n_el, c->el2v_aos, c->el2v, c->elem_edge, c->e_in,
                     c->e_ex, c->e_info, c->n2e_ptr, c->n2e, c->bnd_edges, c->bnd_type, c->bdry, c->e_geo,
-                    c->geo, c->U, c->W, c->flux, c->avg, c->bounds, c->bzeta, c->bqn, c->wdA, c->wdB,
+                    c->geo, c->U, c->W, c->flux, c->avg, c->bounds, c->bzeta, c->bqn, c->bstage, c->wdA, c->wdB,
                     c->dec, c->clk};
     for (void *q : ptrs)
         if (q) cudaFree(q);
@@ -341,6 +341,7 @@ extern "C" int dgr_create(const dgr_mesh_view *m, const dgr_params *params, dgr_
     TRY(dalloc(&c->n2e, 3 * ne));
     TRY(dalloc(&c->bnd_edges, be.size()));
     TRY(dalloc(&c->bnd_type, bt.size()));
+    TRY(dalloc(&c->bstage, 2 * be.size()));
     TRY(cudaHostAlloc((void **)&c->h_stage, sizeof(double) * 2 * (be.size() + 1), cudaHostAllocDefault) == cudaSuccess
             ? 0
             : DGR_ERR_CUDA);
@@ -489,7 +490,7 @@ extern "C" int dgr_set_boundary(dgr_ctx *c, const double *bzeta, const double *b
         c->h_stage[j] = bzeta[be[j]];
         c->h_stage[c->nbnd + j] = bQn[be[j]];
     }
-    double *tmp = c->avg; /* scratch: avg is rebuilt by every stage */
+    double *tmp = c->bstage;
     CK(cudaMemcpyAsync(tmp, c->h_stage, sizeof(double) * 2 * c->nbnd, cudaMemcpyHostToDevice, c->stream));
     k_scatter_bnd<<<blocks(c->nbnd, 256), 256, 0, c->stream>>>(c->nbnd, c->bnd_edges, tmp, c->bzeta, c->bqn);
     c->launches++;
