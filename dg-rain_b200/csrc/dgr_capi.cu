@@ -897,3 +897,22 @@ extern "C" int dgr_profile_step(dgr_ctx *c, int nsteps, double *kernel_ms, int n
     for (int k = 0; k < 4; ++k) kernel_ms[k] = acc[k] / (2.0 * nsteps);
     return DGR_OK;
 }
+
+extern "C" int dgr_pow43_batch(const double *x, double *y, int n, int device)
+{
+    if (!x || !y || n < 0) return DGR_ERR_INVALID;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return DGR_ERR_NO_DEVICE;
+    CK(cudaSetDevice(device));
+    double *d = nullptr;
+    CK(cudaMalloc((void **)&d, 2 * (size_t)(n ? n : 1) * sizeof(double)));
+    cudaMemcpy(d, x, (size_t)n * 8, cudaMemcpyHostToDevice);
+    if (n) k_pow43<<<blocks(n, 256), 256>>>(n, d, d + n);
+    cudaError_t e = cudaMemcpy(y, d + n, (size_t)n * 8, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        snprintf(g_cuda_err, sizeof g_cuda_err, "pow43: %s", cudaGetErrorString(e));
+        return DGR_ERR_CUDA;
+    }
+    return DGR_OK;
+}

@@ -3,8 +3,10 @@
  *
  * Every function here evaluates the reference's expressions in the reference's order and
  * parenthesisation, and the library is compiled with --fmad=false, so each multiply, add,
- * divide and square root is one IEEE operation exactly as in the reference's C.  The only
- * library call whose last bit may differ from the host is pow(H, 4/3) in the Manning term.
+ * divide and square root is one IEEE operation exactly as in the reference's C.  The one
+ * transcendental on the path, pow(H, 4/3) in the Manning term, is evaluated correctly
+ * rounded by pow43() below, which agrees with glibc's pow wherever glibc's is correctly
+ * rounded (all but ~0.1% of arguments).
  */
 #pragma once
 
@@ -102,6 +104,42 @@ DGR_DEV double roe_flux(double fh[3], double zeta_in, double zeta_ex, double qx_
     m = rmax(m, fabs(l3_in));
     m = rmax(m, fabs(l3_ex));
     return m;
+}
+
+/*
+ * x^p for p = 4./3 (the double nearest 4/3, used by the Manning term
+ * pow(H[e], 4./3) of 2DCode/2DInnerProducts.c:318), correctly rounded.
+ *
+ * Method.  p = 4/3 - 1/(3*2^52) exactly, so x^p = x * cbrt(x) * exp(eta) with
+ * eta = -ln(x)/(3*2^52), |eta| < 1e-15 for the depths that occur.
+ *   1. c0 = cbrt(x) (CUDA, <= 1 ulp), refined by one Newton step c = c0 - (c0^3 - x)/(3 c0^2)
+ *      whose residual is formed without rounding loss by FMA-based exact products
+ *      (Dekker's product; Sterbenz makes c0^3 - x exact): c is within ~2^-100 of cbrt(x).
+ *   2. x*c0 split exactly into hi + lo by FMA; exp(eta) = 1 + eta to 1e-30, where the
+ *      double log(x) gives eta far more accurately than needed.
+ *   3. y = hi + ((lo - x*d) + hi*eta) is within a few 2^-100 relative of x^p, so its final
+ *      rounding is the correctly rounded result unless x^p lies within that distance of a
+ *      rounding midpoint.
+ * glibc's pow is correctly rounded for all but ~0.1% of arguments, CUDA's pow for far
+ * fewer; this keeps the device friction term on the reference's bits.
+ * Zero, negative, non-finite and extreme arguments go to pow(), whose special-case
+ * results are the C standard's on both sides.
+ */
+DGR_DEV double pow43(double x)
+{
+    if (!(x >= 1e-200 && x <= 1e200)) return pow(x, 4. / 3);
+    const double c0 = cbrt(x);
+    const double a_h = c0 * c0;
+    const double a_l = __fma_rn(c0, c0, -a_h);
+    const double b_h = a_h * c0;
+    const double b_l = __fma_rn(a_h, c0, -b_h);
+    const double r = ((b_h - x) + b_l) + a_l * c0; /* c0^3 - x */
+    const double d = r / (3.0 * a_h);
+    const double p_h = x * c0;
+    const double p_l = __fma_rn(x, c0, -p_h);
+    const double eta = log(x) * -7.401486830834377e-17;
+    const double lo = (p_l - x * d) + p_h * eta;
+    return p_h + lo;
 }
 
 /* RT0 fit F = (a + b x, c + b y) through three normal-flux values (Cramer's rule of

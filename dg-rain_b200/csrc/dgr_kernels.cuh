@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(128) k_element(MeshDev m, const double *__rest
         H[e] = zr[e] + midz;
         const double u = qxr[e] / H[e];
         const double v = qyr[e] / H[e];
-        tau[e] = GEO(G_GNN + e) * sqrt(u * u + v * v) / (pow(H[e], 4. / 3));
+        tau[e] = GEO(G_GNN + e) * sqrt(u * u + v * v) / pow43(H[e]);
         const double pr = 0.5 * local_g * (H[e] * H[e] - midz * midz);
         const double qxy = qxr[e] * qyr[e] / H[e];
         R[0][e] = qxr[e] * nx[e] + qyr[e] * ny[e];
@@ -855,6 +855,13 @@ __global__ void k_element_setup(int ne, int ldE, const int *__restrict__ el2v_ao
     const double jv = x0v * (y1v - y2v) + x1v * (y2v - y0v) + x2v * (y0v - y1v);
     SETG(G_M11, 6 / fabs(jv));
 #undef SETG
+}
+
+/* the Manning power on n arguments (diagnostic entry point) */
+__global__ void k_pow43(int n, const double *__restrict__ x, double *__restrict__ y)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = pow43(x[i]);
 }
 
 /* reference layout [3*el+k] <-> planar [3*v+k][ld] */

@@ -214,6 +214,10 @@ DGR_API double dgr_last_device_ms(const dgr_ctx *ctx);
  * bounds, limiter + PDop. */
 DGR_API int dgr_profile_step(dgr_ctx *ctx, int nsteps, double *kernel_ms, int n);
 
+/* Diagnostic: y[i] = x[i]^(4./3) as the kernels evaluate the Manning term of
+ * 2DCode/2DInnerProducts.c:318 (correctly rounded; see dgr_device.cuh). */
+DGR_API int dgr_pow43_batch(const double *x, double *y, int n, int device);
+
 #ifdef __cplusplus
 }
 #endif

@@ -243,3 +243,19 @@ def test_large_mesh_one_step(dgrain, oracle_mod):
     assert same(gs[3], os_[3])
     for a, b in zip(gs[:3], os_[:3]):
         assert rel_err(a, b) <= RTOL_RUN
+
+
+def test_manning_power_correctly_rounded(dgrain):
+    """The device x^(4./3) against 60-digit decimal values rounded once to double."""
+    import ctypes as C
+
+    g = load_golden("pow43_cr.npz")
+    x = np.ascontiguousarray(g["x"])
+    y = np.empty_like(x)
+    lib = dgrain.load()
+    assert lib.dgr_pow43_batch(x.ctypes.data_as(dgrain._lib.dptr), y.ctypes.data_as(dgrain._lib.dptr),
+                               len(x), 0) == 0
+    assert np.array_equal(y, g["cr"])
+    # glibc's pow (the reference's) agrees wherever glibc is correctly rounded
+    agree = (y == g["glibc"]).mean()
+    assert agree > 0.998, agree
