@@ -27,7 +27,7 @@ NVCC_FLAGS = [
 ]
 CC_FLAGS = ["-std=c99", "-O2", "-ffp-contract=off", "-fPIC", "-Wall", "-Wextra", "-Wno-unused-parameter"]
 
-CU_SOURCES = ["dgr_capi.cu"]
+CU_SOURCES = ["dgr_capi.cu", "dgr_noalloc.cu"]
 C_SOURCES = ["dgr_host.c"]
 DEPS = ["dgr_kernels.cuh", "dgr_device.cuh", "dgr_forcing.h", os.path.join("..", "..", "include", "dgrain.h")]
 

@@ -118,6 +118,8 @@ SIGNATURES = [
     ("dgr_last_device_ms", C.c_double, [C.c_void_p]),
     ("dgr_profile_step", C.c_int, [C.c_void_p, C.c_int, dptr, C.c_int]),
     ("dgr_pow43_batch", C.c_int, [dptr, dptr, C.c_int, C.c_int]),
+    ("dgr_slope_limiter_noalloc", C.c_int,
+     [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
 ]
 
 _lib = None
