@@ -69,7 +69,7 @@ def measured_peak():
 def ncu_traffic(num_el: int):
     """DRAM bytes per launch of the element kernel from the committed ncu summary, scaled
     to this mesh by the number of elements (see the file for the capture)."""
-    p = os.path.join(ROOT, "profiles", "k_element_stage2_traffic.txt")
+    p = os.path.join(ROOT, "profiles", "k_element_traffic.txt")
     if not os.path.exists(p):
         return None
     vals = {}
