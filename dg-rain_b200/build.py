@@ -57,26 +57,31 @@ def _run(cmd: list[str], verbose: bool) -> None:
         sys.stderr.write(res.stdout + res.stderr)
 
 
-def build(verbose: bool = False, ptxas_verbose: bool = False, force: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build(verbose: bool = False, ptxas_verbose: bool = False, force: bool = False, out: str | None = None,
+          defines: list[str] | None = None) -> str:
+    """Build libdgrain.so (or `out`, with extra -D `defines`, for tuning sweeps)."""
+    lib = out or LIB
+    build_dir = BUILD if out is None else out + ".build"
+    os.makedirs(build_dir, exist_ok=True)
+    dflags = [f"-D{d}" for d in (defines or [])]
     nvcc = _nvcc()
     all_src = [os.path.join(CSRC, f) for f in CU_SOURCES + C_SOURCES + DEPS]
-    if not force and not _newer(LIB, all_src + [__file__]):
-        return LIB
+    if not force and not _newer(lib, all_src + [__file__]):
+        return lib
     objs = []
     for f in C_SOURCES:
-        o = os.path.join(BUILD, f + ".o")
+        o = os.path.join(build_dir, f + ".o")
         _run(["gcc", *CC_FLAGS, "-c", os.path.join(CSRC, f), "-o", o], verbose)
         objs.append(o)
     for f in CU_SOURCES:
-        o = os.path.join(BUILD, f + ".o")
+        o = os.path.join(build_dir, f + ".o")
         extra = ["-Xptxas", "-v"] if ptxas_verbose else []
-        _run([nvcc, *NVCC_FLAGS, *extra, "-c", os.path.join(CSRC, f), "-o", o], verbose or ptxas_verbose)
+        _run([nvcc, *NVCC_FLAGS, *dflags, *extra, "-c", os.path.join(CSRC, f), "-o", o], verbose or ptxas_verbose)
         objs.append(o)
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs, "-lm"], verbose)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":

@@ -69,9 +69,12 @@ DGR_DEV double roe_flux(double fh[3], double zeta_in, double zeta_ex, double qx_
 
     const double r[3][3] = {{1, 0, 1}, {u_hat - c * nx, -ny, u_hat + c * nx}, {v_hat - c * ny, nx, v_hat + c * ny}};
     const double den = -2 * c;
-    const double ri[3][3] = {{(-c - nx * u_hat - ny * v_hat) / den, nx / den, ny / den},
+    /* (-nx)/den is exactly -(nx/den): IEEE division is symmetric in sign, so the third
+     * row reuses the first row's quotients. */
+    const double nx_den = nx / den, ny_den = ny / den;
+    const double ri[3][3] = {{(-c - nx * u_hat - ny * v_hat) / den, nx_den, ny_den},
                              {(-2 * c * ny * u_hat + 2 * c * nx * v_hat) / den, 2 * c * ny / den, -2 * c * nx / den},
-                             {(-c + nx * u_hat + ny * v_hat) / den, -nx / den, -ny / den}};
+                             {(-c + nx * u_hat + ny * v_hat) / den, -nx_den, -ny_den}};
 
     const double un_in = u_in * nx + v_in * ny, un_ex = u_ex * nx + v_ex * ny;
     const double c_in = sqrt(g * h_in), c_ex = sqrt(g * h_ex);
@@ -140,6 +143,16 @@ DGR_DEV double pow43(double x)
     const double eta = log(x) * -7.401486830834377e-17;
     const double lo = (p_l - x * d) + p_h * eta;
     return p_h + lo;
+}
+
+/* x / d for the limiter's redistribution count d in {1, 2, 3} (as a double).  Division
+ * by 1 and by 2 are exact (x and x*0.5 are the correctly rounded x/d); only d = 3 needs
+ * the full IEEE division. */
+DGR_DEV double div_by_count(double x, double d)
+{
+    if (d == 1.0) return x;
+    if (d == 2.0) return x * 0.5;
+    return x / d;
 }
 
 /* RT0 fit F = (a + b x, c + b y) through three normal-flux values (Cramer's rule of

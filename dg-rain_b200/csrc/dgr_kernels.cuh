@@ -22,6 +22,19 @@
 #include "dgr_device.cuh"
 #include "dgr_forcing.h"
 
+/* Minimum resident blocks per SM requested from the compiler for the three step kernels
+ * (register caps: 65536 / (block size x blocks)).  Chosen by measurement; overridable at
+ * build time for tuning sweeps. */
+#ifndef DGR_MINB_EDGE
+#define DGR_MINB_EDGE 3
+#endif
+#ifndef DGR_MINB_ELEMENT
+#define DGR_MINB_ELEMENT 4
+#endif
+#ifndef DGR_MINB_LIMIT
+#define DGR_MINB_LIMIT 6
+#endif
+
 namespace dgr {
 
 /* element geometry planes */
@@ -81,7 +94,7 @@ struct PhysParams {
 /* One thread per edge: traces, ghost state, Roe flux(es), max wave speed
  * (2DCode/compute2DL.c:17-331). */
 template <bool WD>
-__global__ void __launch_bounds__(256) k_edge_flux(MeshDev m, const double *__restrict__ S,
+__global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, const double *__restrict__ S,
                                                    const int *__restrict__ wd,
                                                    const double *__restrict__ bzeta,
                                                    const double *__restrict__ bqn,
@@ -196,7 +209,7 @@ enum { MODE_RHS = 0, MODE_STAGE1 = 1, MODE_STAGE2 = 2 };
  * S is the stage input, U the step input (stage 2 only).  MODE_RHS writes the RHS.
  */
 template <int MODE>
-__global__ void __launch_bounds__(128) k_element(MeshDev m, const double *__restrict__ S,
+__global__ void __launch_bounds__(128, DGR_MINB_ELEMENT) k_element(MeshDev m, const double *__restrict__ S,
                                                  const double *__restrict__ U,
                                                  const int *__restrict__ wd,
                                                  const double *__restrict__ flux,
@@ -432,7 +445,7 @@ __global__ void __launch_bounds__(256) k_wd_status(MeshDev m, const double *__re
  * element had; the new status goes to wd_out.
  */
 template <bool LIMIT, bool PDOP, bool STATUS>
-__global__ void __launch_bounds__(128) k_limit(MeshDev m, double *__restrict__ S,
+__global__ void __launch_bounds__(128, DGR_MINB_LIMIT) k_limit(MeshDev m, double *__restrict__ S,
                                                const double *__restrict__ bounds,
                                                const int *__restrict__ wd_in, int *__restrict__ wd_out,
                                                DevClock *clk, double h0, double velzero, int phase,
@@ -484,7 +497,7 @@ __global__ void __launch_bounds__(128) k_limit(MeshDev m, double *__restrict__ S
                     const double div = fmax(1.0, kdp);
                     double redfac;
                     if (diff[k] > 0) {
-                        redfac = sumdiff * sdd / div;
+                        redfac = div_by_count(sumdiff * sdd, div);
                         kdp -= 1;
                     } else {
                         redfac = 0;
