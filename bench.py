@@ -37,7 +37,7 @@ for _p in (ROOT, PKG):
         sys.path.insert(0, _p)
 
 NX, NY, JITTER, CFL, AMP, PERIOD = 2000, 1000, 0.1, 0.3, 0.5, 44712.0
-LAND_FILM = 0.5e-3      # dry land holds H0/2 (a film of exactly H0 makes the reference stop)
+LAND_FILM = 0.5e-3      # dry land holds H0/2: with exactly H0 the reference wet/dry step stops on a NaN flux
 ALG_BYTES = 216         # algorithmic bytes per element-stage (state in, step input, state out)
 METRIC = "element-stage updates/s"
 

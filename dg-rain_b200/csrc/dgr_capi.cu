@@ -1,6 +1,11 @@
 /*
  * Device context and C ABI of include/dgrain.h (the part that needs CUDA).
  *
+ * A context holds S >= 1 scenarios: the disjoint union of their meshes, flattened into
+ * one mesh (elements, nodes and edges renumbered with per-scenario offsets), with a
+ * scenario id per element and per edge and one clock per scenario.  A single mesh is
+ * the case S = 1.  Each scenario's numbers are exactly those of running it alone.
+ *
  * Step orchestration (wet/dry on; the order of ChanNet/time_evolution.c:218-427 around
  * the 2DCode operators):
  *
@@ -11,9 +16,17 @@
  * The last status call is the one the reference makes at the start of the next step;
  * doing it here saves a launch.  The reference's global WD after a step is WB, which is
  * what dgr_download_state returns.
+ *
+ * Schedules of the device loop ("fusion depth"), chosen by dgr_autotune or
+ * dgr_set_schedule:
+ *   0: ten kernels per step (clock, 4 per stage, clock end), one thread per item;
+ *   1: one persistent cooperative kernel per RK stage between the clock kernels;
+ *   2: one persistent cooperative kernel per step, clock included;
+ * and the block size (elements per block) of the element and limiter work.
  */
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -41,34 +54,48 @@ extern "C" const char *dgr_last_cuda_error(void) { return g_cuda_err; }
 
 static int pad32(int n) { return (n + 31) & ~31; }
 
+static double bits_to_double(unsigned long long b)
+{
+    double d;
+    memcpy(&d, &b, sizeof d);
+    return d;
+}
+
+static unsigned blocks(int n, int t) { return (unsigned)((n + t - 1) / t); }
+
 struct dgr_ctx {
     dgr_params p;
     int device;
+    int nscen;
     int ne, nn, nf, nbnd;
     int ldE, ldF, ldN;
-    double min_edge;
+    std::vector<int> el_off, nd_off, ed_off; /* [nscen + 1] */
+    std::vector<int> h_bnd;                  /* prescribed edges (flattened ids) */
     cudaStream_t stream;
     cudaEvent_t ev0, ev1;
+    int num_sms;
     /* mesh */
     double *x, *y, *zn, *nfric, *n_el;
-    int *el2v_aos, *el2v, *elem_edge, *e_in, *e_ex, *e_info, *n2e_ptr, *n2e, *bnd_edges, *bnd_type;
-    int *bdry;
+    int *el2v_aos, *el2v, *elem_edge, *e_in, *e_ex, *e_info, *n2e_ptr, *n2e, *bnd_edges, *bnd_type, *bnd_sid;
+    int *bdry, *el_sid, *ed_sid;
     double *e_geo, *geo;
     /* state and work */
     double *U, *W, *flux, *avg, *bounds, *bzeta, *bqn, *bstage;
     int *wdA, *wdB;
-    int *dec;  /* [4][ne]: limit s0, pdop s0, limit s1, pdop s1 */
+    int *dec; /* [4][ne]: limit s0, pdop s0, limit s1, pdop s1 */
+    unsigned *bar;
     DevClock *clk;
-    DevClock *h_clk; /* pinned mirror */
-    double *h_stage; /* pinned staging for compact boundary values */
-    std::vector<int> *h_bnd; /* prescribed edge ids, host copy */
+    DevClock *h_clk; /* pinned mirror [nscen] */
+    double *h_stage;
     int wd_fresh;    /* WA already holds the status for the next step */
     int wd_cur_is_B; /* reference-semantic WD lives in WB */
     long long launches;
     double last_ms;
+    /* schedule of the device loop */
+    int bs;     /* block size of element/limiter work: 64, 128 or 256 */
+    int fusion; /* 0, 1 or 2 */
     cudaGraph_t graph;
     cudaGraphExec_t graph_exec;
-    int graph_kernels;
 };
 
 static MeshDev mesh_dev(const dgr_ctx *c)
@@ -90,7 +117,8 @@ static MeshDev mesh_dev(const dgr_ctx *c)
     m.n2e_ptr = c->n2e_ptr;
     m.n2e = c->n2e;
     m.zn = c->zn;
-    m.minlen_cfl_unused = nullptr;
+    m.el_sid = c->el_sid;
+    m.ed_sid = c->ed_sid;
     return m;
 }
 
@@ -100,24 +128,10 @@ static PhysParams phys(const dgr_ctx *c)
     q.g = c->p.g;
     q.h0 = c->p.H0;
     q.velzero = c->p.VELZERO;
-    q.rain = c->p.rain;
     q.cfl = c->p.cfl;
     q.dt0 = c->p.dt0;
-    q.min_edge = c->min_edge;
-    q.tide_amp = c->p.tide_amp;
-    q.tide_period = c->p.tide_period;
-    q.tide_on = c->p.tide_on;
     return q;
 }
-
-static double bits_to_double(unsigned long long b)
-{
-    double d;
-    memcpy(&d, &b, sizeof d);
-    return d;
-}
-
-static unsigned blocks(int n, int t) { return (unsigned)((n + t - 1) / t); }
 
 extern "C" int dgr_params_default(dgr_params *p)
 {
@@ -146,15 +160,22 @@ static int dalloc(T **p, size_t n)
     return DGR_OK;
 }
 
+static void drop_graph(dgr_ctx *c)
+{
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graph_exec = nullptr;
+    c->graph = nullptr;
+}
+
 static void release(dgr_ctx *c)
 {
     if (!c) return;
-    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
-    if (c->graph) cudaGraphDestroy(c->graph);
+    drop_graph(c);
     void *ptrs[] = {c->x, c->y, c->zn, c->nfric, c->n_el, c->el2v_aos, c->el2v, c->elem_edge, c->e_in,
-                    c->e_ex, c->e_info, c->n2e_ptr, c->n2e, c->bnd_edges, c->bnd_type, c->bdry, c->e_geo,
-                    c->geo, c->U, c->W, c->flux, c->avg, c->bounds, c->bzeta, c->bqn, c->bstage, c->wdA, c->wdB,
-                    c->dec, c->clk};
+                    c->e_ex, c->e_info, c->n2e_ptr, c->n2e, c->bnd_edges, c->bnd_type, c->bnd_sid, c->bdry,
+                    c->el_sid, c->ed_sid, c->e_geo, c->geo, c->U, c->W, c->flux, c->avg, c->bounds, c->bzeta,
+                    c->bqn, c->bstage, c->wdA, c->wdB, c->dec, c->bar, c->clk};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (c->h_clk) cudaFreeHost(c->h_clk);
@@ -162,15 +183,13 @@ static void release(dgr_ctx *c)
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
-    delete c->h_bnd;
     delete c;
 }
 
 static int upload_geometry(dgr_ctx *c)
 {
-    const dim3 t(128);
-    k_element_setup<<<blocks(c->ne, 128), t, 0, c->stream>>>(c->ne, c->ldE, c->el2v_aos, c->x, c->y, c->zn,
-                                                             c->nfric, c->n_el, c->p.g, c->el2v, c->geo);
+    k_element_setup<<<blocks(c->ne, 128), 128, 0, c->stream>>>(c->ne, c->ldE, c->el2v_aos, c->x, c->y, c->zn,
+                                                               c->nfric, c->n_el, c->p.g, c->el2v, c->geo);
     c->launches++;
     CK(cudaGetLastError());
     return DGR_OK;
@@ -182,7 +201,6 @@ static int check_mesh_view(const dgr_mesh_view *m)
     if (!m->x_coord || !m->y_coord || !m->z || !m->nFriction || !m->EltoVert || !m->EdgtoEls ||
         !m->EdgtoVert || !m->BdryPrescribed)
         return DGR_ERR_INVALID;
-    if ((long long)m->num_edges >= (1LL << 30) || (long long)m->num_el >= (1LL << 30)) return DGR_ERR_TOO_LARGE;
     for (long long i = 0; i < 3LL * m->num_el; ++i)
         if (m->EltoVert[i] < 0 || m->EltoVert[i] >= m->num_nodes) return DGR_ERR_MESH;
     for (long long i = 0; i < 2LL * m->num_edges; ++i) {
@@ -202,40 +220,88 @@ static int check_mesh_view(const dgr_mesh_view *m)
             return r_;      \
         }                   \
     } while (0)
+#define TRYC(x) TRY((x) == cudaSuccess ? DGR_OK : DGR_ERR_CUDA)
 
-extern "C" int dgr_create(const dgr_mesh_view *m, const dgr_params *params, dgr_ctx **out)
+/* Copies one host array per scenario into a flattened device array, adding `add[s]` to
+ * every entry of scenario s (connectivity renumbering); add == nullptr copies as is. */
+template <class T>
+static int upload_concat(cudaStream_t s, T *dst, int nscen, const T *const *src, const std::vector<int> &count,
+                         int mult, const std::vector<int> *add)
 {
-    if (!out) return DGR_ERR_INVALID;
+    size_t off = 0;
+    std::vector<T> tmp;
+    for (int k = 0; k < nscen; ++k) {
+        const size_t n = (size_t)count[k] * mult;
+        if (add && (*add)[k] != 0) {
+            tmp.assign(src[k], src[k] + n);
+            for (auto &v : tmp) v += (T)(*add)[k];
+            CK(cudaMemcpy(dst + off, tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+        } else {
+            CK(cudaMemcpyAsync(dst + off, src[k], n * sizeof(T), cudaMemcpyHostToDevice, s));
+        }
+        off += n;
+    }
+    CK(cudaStreamSynchronize(s));
+    return DGR_OK;
+}
+
+static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario_params *sp, const dgr_params *params,
+                       dgr_ctx **out)
+{
+    if (!out || nscen <= 0 || !views) return DGR_ERR_INVALID;
     *out = nullptr;
-    int rc = check_mesh_view(m);
-    if (rc) return rc;
+    long long tot_e = 0, tot_n = 0, tot_f = 0;
+    for (int k = 0; k < nscen; ++k) {
+        int rc = check_mesh_view(&views[k]);
+        if (rc) return rc;
+        tot_e += views[k].num_el;
+        tot_n += views[k].num_nodes;
+        tot_f += views[k].num_edges;
+    }
+    if (tot_f >= (1LL << 30) || tot_e >= (1LL << 30) || tot_n >= (1LL << 30)) return DGR_ERR_TOO_LARGE;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         snprintf(g_cuda_err, sizeof g_cuda_err, "no CUDA device visible");
         return DGR_ERR_NO_DEVICE;
     }
     dgr_ctx *c = new dgr_ctx();
-    memset((void *)c, 0, sizeof *c);
     if (params)
         c->p = *params;
     else
         dgr_params_default(&c->p);
     c->device = c->p.device;
+    c->bs = 128;
+    c->fusion = 0;
     if (c->device < 0 || c->device >= ndev) {
         release(c);
         return DGR_ERR_INVALID;
     }
-    TRY(cudaSetDevice(c->device) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    c->ne = m->num_el;
-    c->nn = m->num_nodes;
-    c->nf = m->num_edges;
+    TRYC(cudaSetDevice(c->device));
+    TRYC(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
+    c->nscen = nscen;
+    c->ne = (int)tot_e;
+    c->nn = (int)tot_n;
+    c->nf = (int)tot_f;
     c->ldE = pad32(c->ne);
     c->ldF = pad32(c->nf);
     c->ldN = pad32(c->nn);
-    c->min_edge = m->minEdgLength;
-    TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaEventCreate(&c->ev0) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaEventCreate(&c->ev1) == cudaSuccess ? 0 : DGR_ERR_CUDA);
+    std::vector<int> ne_s(nscen), nn_s(nscen), nf_s(nscen);
+    c->el_off.assign(nscen + 1, 0);
+    c->nd_off.assign(nscen + 1, 0);
+    c->ed_off.assign(nscen + 1, 0);
+    for (int k = 0; k < nscen; ++k) {
+        ne_s[k] = views[k].num_el;
+        nn_s[k] = views[k].num_nodes;
+        nf_s[k] = views[k].num_edges;
+        c->el_off[k + 1] = c->el_off[k] + ne_s[k];
+        c->nd_off[k + 1] = c->nd_off[k] + nn_s[k];
+        c->ed_off[k + 1] = c->ed_off[k] + nf_s[k];
+    }
+    std::vector<int> el_add(c->el_off.begin(), c->el_off.end() - 1), nd_add(c->nd_off.begin(), c->nd_off.end() - 1);
+
+    TRYC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    TRYC(cudaEventCreate(&c->ev0));
+    TRYC(cudaEventCreate(&c->ev1));
 
     const size_t ne = c->ne, nn = c->nn, nf = c->nf, lE = c->ldE, lF = c->ldF, lN = c->ldN;
     TRY(dalloc(&c->x, nn));
@@ -261,31 +327,81 @@ extern "C" int dgr_create(const dgr_mesh_view *m, const dgr_params *params, dgr_
     TRY(dalloc(&c->wdA, ne));
     TRY(dalloc(&c->wdB, ne));
     TRY(dalloc(&c->dec, 4 * ne));
-    TRY(dalloc(&c->clk, 1));
-    TRY(cudaHostAlloc((void **)&c->h_clk, sizeof(DevClock), cudaHostAllocDefault) == cudaSuccess ? 0 : DGR_ERR_CUDA);
+    TRY(dalloc(&c->bar, 4));
+    TRY(dalloc(&c->clk, nscen));
+    TRYC(cudaHostAlloc((void **)&c->h_clk, sizeof(DevClock) * nscen, cudaHostAllocDefault));
 
     cudaStream_t s = c->stream;
-    TRY(cudaMemcpyAsync(c->x, m->x_coord, nn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemcpyAsync(c->y, m->y_coord, nn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemcpyAsync(c->zn, m->z, nn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemcpyAsync(c->nfric, m->nFriction, nn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemcpyAsync(c->el2v_aos, m->EltoVert, 3 * ne * 4, cudaMemcpyHostToDevice, s) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemcpyAsync(c->bdry, m->BdryPrescribed, nf * 4, cudaMemcpyHostToDevice, s) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemsetAsync(c->elem_edge, 0xff, 3 * lE * 4, s) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemsetAsync(c->bzeta, 0, nf * 8, s) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemsetAsync(c->bqn, 0, nf * 8, s) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemsetAsync(c->U, 0, 9 * lE * 8, s) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemsetAsync(c->W, 0, 9 * lE * 8, s) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemsetAsync(c->dec, 0, 4 * ne * 4, s) == cudaSuccess ? 0 : DGR_ERR_CUDA);
+    {
+        std::vector<const double *> px(nscen), py(nscen), pz(nscen), pn(nscen);
+        std::vector<const int *> pev(nscen), pbd(nscen);
+        for (int k = 0; k < nscen; ++k) {
+            px[k] = views[k].x_coord;
+            py[k] = views[k].y_coord;
+            pz[k] = views[k].z;
+            pn[k] = views[k].nFriction;
+            pev[k] = views[k].EltoVert;
+            pbd[k] = views[k].BdryPrescribed;
+        }
+        TRY(upload_concat(s, c->x, nscen, px.data(), nn_s, 1, nullptr));
+        TRY(upload_concat(s, c->y, nscen, py.data(), nn_s, 1, nullptr));
+        TRY(upload_concat(s, c->zn, nscen, pz.data(), nn_s, 1, nullptr));
+        TRY(upload_concat(s, c->nfric, nscen, pn.data(), nn_s, 1, nullptr));
+        TRY(upload_concat(s, c->el2v_aos, nscen, pev.data(), ne_s, 3, &nd_add));
+        TRY(upload_concat(s, c->bdry, nscen, pbd.data(), nf_s, 1, nullptr));
+    }
+    TRYC(cudaMemsetAsync(c->elem_edge, 0xff, 3 * lE * 4, s));
+    TRYC(cudaMemsetAsync(c->bzeta, 0, nf * 8, s));
+    TRYC(cudaMemsetAsync(c->bqn, 0, nf * 8, s));
+    TRYC(cudaMemsetAsync(c->U, 0, 9 * lE * 8, s));
+    TRYC(cudaMemsetAsync(c->W, 0, 9 * lE * 8, s));
+    TRYC(cudaMemsetAsync(c->dec, 0, 4 * ne * 4, s));
+    TRYC(cudaMemsetAsync(c->bar, 0, 16, s));
 
-    /* connectivity arrays go through a temporary device copy */
+    /* per-element Manning n of the scenarios that give one (negative: node average) */
+    bool any_nel = false;
+    for (int k = 0; k < nscen; ++k) any_nel |= (sp && sp[k].n_el);
+    if (any_nel) {
+        std::vector<double> nel(ne, -1.0);
+        for (int k = 0; k < nscen; ++k)
+            if (sp[k].n_el) std::copy(sp[k].n_el, sp[k].n_el + ne_s[k], nel.begin() + c->el_off[k]);
+        TRY(dalloc(&c->n_el, ne));
+        TRYC(cudaMemcpy(c->n_el, nel.data(), ne * 8, cudaMemcpyHostToDevice));
+    }
+    if (nscen > 1) {
+        std::vector<int> esid(ne), fsid(nf);
+        for (int k = 0; k < nscen; ++k) {
+            std::fill(esid.begin() + c->el_off[k], esid.begin() + c->el_off[k + 1], k);
+            std::fill(fsid.begin() + c->ed_off[k], fsid.begin() + c->ed_off[k + 1], k);
+        }
+        TRY(dalloc(&c->el_sid, ne));
+        TRY(dalloc(&c->ed_sid, nf));
+        TRYC(cudaMemcpy(c->el_sid, esid.data(), ne * 4, cudaMemcpyHostToDevice));
+        TRYC(cudaMemcpy(c->ed_sid, fsid.data(), nf * 4, cudaMemcpyHostToDevice));
+    }
+
+    /* connectivity goes through a temporary device copy */
     int *d_ed2el = nullptr, *d_ed2v = nullptr, *d_bad = nullptr;
     TRY(dalloc(&d_ed2el, 2 * nf));
     TRY(dalloc(&d_ed2v, 2 * nf));
     TRY(dalloc(&d_bad, 1));
-    int big = 0x7fffffff;
-    cudaMemcpyAsync(d_ed2el, m->EdgtoEls, 2 * nf * 4, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(d_ed2v, m->EdgtoVert, 2 * nf * 4, cudaMemcpyHostToDevice, s);
+    {
+        std::vector<const int *> pe(nscen), pv(nscen);
+        for (int k = 0; k < nscen; ++k) {
+            pe[k] = views[k].EdgtoEls;
+            pv[k] = views[k].EdgtoVert;
+        }
+        int r1 = upload_concat(s, d_ed2el, nscen, pe.data(), nf_s, 2, &el_add);
+        int r2 = upload_concat(s, d_ed2v, nscen, pv.data(), nf_s, 2, &nd_add);
+        if (r1 || r2) {
+            cudaFree(d_ed2el);
+            cudaFree(d_ed2v);
+            cudaFree(d_bad);
+            release(c);
+            return r1 ? r1 : r2;
+        }
+    }
+    const int big = 0x7fffffff;
     cudaMemcpyAsync(d_bad, &big, 4, cudaMemcpyHostToDevice, s);
     k_edge_setup<<<blocks(c->nf, 256), 256, 0, s>>>(c->nf, c->ldE, c->ldF, d_ed2el, d_ed2v, c->el2v_aos, c->bdry,
                                                      c->x, c->y, c->zn, c->e_in, c->e_ex, c->e_info, c->e_geo,
@@ -316,55 +432,79 @@ extern "C" int dgr_create(const dgr_mesh_view *m, const dgr_params *params, dgr_
                 return DGR_ERR_MESH; /* an element edge that no EdgtoEls entry covers */
             }
 
-    /* node -> element lists, ascending element order */
-    std::vector<int> ptr(nn + 1, 0), lst(3 * ne);
-    for (size_t i = 0; i < 3 * ne; ++i) ptr[m->EltoVert[i] + 1]++;
+    /* node -> element lists (ascending element order) and prescribed edges */
+    std::vector<int> ptr(nn + 1, 0), lst(3 * ne), be, bt, bsid;
+    for (int k = 0; k < nscen; ++k)
+        for (long long i = 0; i < 3LL * ne_s[k]; ++i) ptr[views[k].EltoVert[i] + c->nd_off[k] + 1]++;
     for (size_t n = 0; n < nn; ++n) ptr[n + 1] += ptr[n];
     {
         std::vector<int> fill(nn, 0);
-        for (size_t el = 0; el < ne; ++el)
-            for (int k = 0; k < 3; ++k) {
-                int v = m->EltoVert[3 * el + k];
-                lst[ptr[v] + fill[v]++] = (int)el;
-            }
+        for (int k = 0; k < nscen; ++k)
+            for (int el = 0; el < ne_s[k]; ++el)
+                for (int j = 0; j < 3; ++j) {
+                    const int v = views[k].EltoVert[3 * el + j] + c->nd_off[k];
+                    lst[ptr[v] + fill[v]++] = el + c->el_off[k];
+                }
     }
-    /* prescribed boundary edges */
-    std::vector<int> be, bt;
-    for (size_t i = 0; i < nf; ++i)
-        if (m->BdryPrescribed[i]) {
-            be.push_back((int)i);
-            bt.push_back(m->BdryPrescribed[i]);
-        }
+    for (int k = 0; k < nscen; ++k)
+        for (int i = 0; i < nf_s[k]; ++i)
+            if (views[k].BdryPrescribed[i]) {
+                be.push_back(i + c->ed_off[k]);
+                bt.push_back(views[k].BdryPrescribed[i]);
+                bsid.push_back(k);
+            }
     c->nbnd = (int)be.size();
-    c->h_bnd = new std::vector<int>(be);
+    c->h_bnd = be;
     TRY(dalloc(&c->n2e_ptr, nn + 1));
     TRY(dalloc(&c->n2e, 3 * ne));
     TRY(dalloc(&c->bnd_edges, be.size()));
     TRY(dalloc(&c->bnd_type, bt.size()));
+    TRY(dalloc(&c->bnd_sid, bsid.size()));
     TRY(dalloc(&c->bstage, 2 * be.size()));
-    TRY(cudaHostAlloc((void **)&c->h_stage, sizeof(double) * 2 * (be.size() + 1), cudaHostAllocDefault) == cudaSuccess
-            ? 0
-            : DGR_ERR_CUDA);
-    TRY(cudaMemcpy(c->n2e_ptr, ptr.data(), (nn + 1) * 4, cudaMemcpyHostToDevice) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemcpy(c->n2e, lst.data(), 3 * ne * 4, cudaMemcpyHostToDevice) == cudaSuccess ? 0 : DGR_ERR_CUDA);
+    TRYC(cudaHostAlloc((void **)&c->h_stage, sizeof(double) * 2 * (be.size() + 1), cudaHostAllocDefault));
+    TRYC(cudaMemcpy(c->n2e_ptr, ptr.data(), (nn + 1) * 4, cudaMemcpyHostToDevice));
+    TRYC(cudaMemcpy(c->n2e, lst.data(), 3 * ne * 4, cudaMemcpyHostToDevice));
     if (!be.empty()) {
-        TRY(cudaMemcpy(c->bnd_edges, be.data(), be.size() * 4, cudaMemcpyHostToDevice) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-        TRY(cudaMemcpy(c->bnd_type, bt.data(), bt.size() * 4, cudaMemcpyHostToDevice) == cudaSuccess ? 0 : DGR_ERR_CUDA);
+        TRYC(cudaMemcpy(c->bnd_edges, be.data(), be.size() * 4, cudaMemcpyHostToDevice));
+        TRYC(cudaMemcpy(c->bnd_type, bt.data(), bt.size() * 4, cudaMemcpyHostToDevice));
+        TRYC(cudaMemcpy(c->bnd_sid, bsid.data(), bsid.size() * 4, cudaMemcpyHostToDevice));
     }
-    /* clock and flags */
-    DevClock hc;
-    memset(&hc, 0, sizeof hc);
-    hc.err = ~0ull;
-    hc.final_time = 1e300;
-    TRY(cudaMemcpy(c->clk, &hc, sizeof hc, cudaMemcpyHostToDevice) == cudaSuccess ? 0 : DGR_ERR_CUDA);
+    /* clocks */
+    for (int k = 0; k < nscen; ++k) {
+        DevClock &h = c->h_clk[k];
+        memset(&h, 0, sizeof h);
+        h.err = ~0ull;
+        h.final_time = 1e300;
+        h.min_edge = views[k].minEdgLength;
+        h.rain = sp ? sp[k].rain : c->p.rain;
+        h.tide_on = sp ? sp[k].tide_on : c->p.tide_on;
+        h.tide_amp = sp ? sp[k].tide_amp : c->p.tide_amp;
+        h.tide_period = sp ? sp[k].tide_period : c->p.tide_period;
+        h.el_off = c->el_off[k];
+        h.ed_off = c->ed_off[k];
+    }
+    TRYC(cudaMemcpy(c->clk, c->h_clk, sizeof(DevClock) * nscen, cudaMemcpyHostToDevice));
     std::vector<int> wd(ne, -1);
-    TRY(cudaMemcpy(c->wdA, wd.data(), ne * 4, cudaMemcpyHostToDevice) == cudaSuccess ? 0 : DGR_ERR_CUDA);
-    TRY(cudaMemcpy(c->wdB, wd.data(), ne * 4, cudaMemcpyHostToDevice) == cudaSuccess ? 0 : DGR_ERR_CUDA);
+    TRYC(cudaMemcpy(c->wdA, wd.data(), ne * 4, cudaMemcpyHostToDevice));
+    TRYC(cudaMemcpy(c->wdB, wd.data(), ne * 4, cudaMemcpyHostToDevice));
     c->wd_fresh = 0;
     c->wd_cur_is_B = 0;
     *out = c;
     return DGR_OK;
 }
+
+extern "C" int dgr_create(const dgr_mesh_view *m, const dgr_params *params, dgr_ctx **out)
+{
+    return create_impl(1, m, nullptr, params, out);
+}
+
+extern "C" int dgr_ensemble_create(int nscen, const dgr_mesh_view *meshes, const dgr_scenario_params *sp,
+                                   const dgr_params *params, dgr_ctx **out)
+{
+    return create_impl(nscen, meshes, sp, params, out);
+}
+
+extern "C" int dgr_ensemble_size(const dgr_ctx *c) { return c ? c->nscen : -1; }
 
 extern "C" int dgr_destroy(dgr_ctx *c)
 {
@@ -375,18 +515,24 @@ extern "C" int dgr_destroy(dgr_ctx *c)
     return DGR_OK;
 }
 
-static void drop_graph(dgr_ctx *c)
-{
-    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
-    if (c->graph) cudaGraphDestroy(c->graph);
-    c->graph_exec = nullptr;
-    c->graph = nullptr;
-}
-
 extern "C" int dgr_get_params(const dgr_ctx *c, dgr_params *out)
 {
     if (!c || !out) return DGR_ERR_INVALID;
     *out = c->p;
+    return DGR_OK;
+}
+
+static int read_clock(dgr_ctx *c)
+{
+    CK(cudaMemcpyAsync(c->h_clk, c->clk, sizeof(DevClock) * c->nscen, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DGR_OK;
+}
+
+static int write_clock(dgr_ctx *c)
+{
+    CK(cudaMemcpyAsync(c->clk, c->h_clk, sizeof(DevClock) * c->nscen, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return DGR_OK;
 }
 
@@ -396,6 +542,7 @@ extern "C" int dgr_set_params(dgr_ctx *c, const dgr_params *p)
     if (p->g != c->p.g || p->H0 != c->p.H0 || p->VELZERO != c->p.VELZERO || p->wet_dry != c->p.wet_dry ||
         p->device != c->p.device)
         return DGR_ERR_INVALID;
+    CK(cudaSetDevice(c->device));
     c->p.rain = p->rain;
     c->p.tide_on = p->tide_on;
     c->p.tide_amp = p->tide_amp;
@@ -403,6 +550,16 @@ extern "C" int dgr_set_params(dgr_ctx *c, const dgr_params *p)
     c->p.cfl = p->cfl;
     c->p.dt0 = p->dt0;
     c->p.record_decisions = p->record_decisions;
+    if (c->nscen == 1) { /* a single mesh takes its forcing from the run parameters */
+        int r = read_clock(c);
+        if (r) return r;
+        c->h_clk[0].rain = p->rain;
+        c->h_clk[0].tide_on = p->tide_on;
+        c->h_clk[0].tide_amp = p->tide_amp;
+        c->h_clk[0].tide_period = p->tide_period;
+        r = write_clock(c);
+        if (r) return r;
+    }
     drop_graph(c);
     return DGR_OK;
 }
@@ -430,43 +587,82 @@ extern "C" int dgr_set_element_manning(dgr_ctx *c, const double *n_el)
 
 /* ------------------------------------------------------------------ state ---- */
 
-extern "C" int dgr_upload_state(dgr_ctx *c, const double *zeta, const double *Qx, const double *Qy, const int *WD)
+static int upload_slice(dgr_ctx *c, int sc, const double *zeta, const double *Qx, const double *Qy, const int *WD)
 {
-    if (!c || !zeta || !Qx || !Qy) return DGR_ERR_INVALID;
+    if (!zeta || !Qx || !Qy || sc < 0 || sc >= c->nscen) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
-    const size_t n3 = 3 * (size_t)c->ne;
+    const int n = c->el_off[sc + 1] - c->el_off[sc];
+    const size_t n3 = 3 * (size_t)n;
     double *st = c->W; /* staging: W is free between steps */
     cudaStream_t s = c->stream;
     CK(cudaMemcpyAsync(st, zeta, n3 * 8, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(st + n3, Qx, n3 * 8, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(st + 2 * n3, Qy, n3 * 8, cudaMemcpyHostToDevice, s));
-    k_aos_to_planar<<<blocks(c->ne, 256), 256, 0, s>>>(c->ne, c->ldE, st, st + n3, st + 2 * n3, c->U);
+    k_aos_to_planar<<<blocks(n, 256), 256, 0, s>>>(n, c->ldE, st, st + n3, st + 2 * n3, c->U + c->el_off[sc]);
     c->launches++;
-    if (WD) CK(cudaMemcpyAsync(c->wdA, WD, (size_t)c->ne * 4, cudaMemcpyHostToDevice, s));
-    /* clear the error word */
-    const unsigned long long none = ~0ull;
-    CK(cudaMemcpyAsync(&c->clk->err, &none, 8, cudaMemcpyHostToDevice, s));
+    /* the other scenarios' current flags must sit in WA as well before WA is marked current */
+    if (c->wd_cur_is_B && c->nscen > 1)
+        for (int k = 0; k < c->nscen; ++k)
+            if (k != sc)
+                CK(cudaMemcpyAsync(c->wdA + c->el_off[k], c->wdB + c->el_off[k],
+                                   (size_t)(c->el_off[k + 1] - c->el_off[k]) * 4, cudaMemcpyDeviceToDevice, s));
+    if (WD) CK(cudaMemcpyAsync(c->wdA + c->el_off[sc], WD, (size_t)n * 4, cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
+    /* clear the scenario's error word and run state */
+    int r = read_clock(c);
+    if (r) return r;
+    c->h_clk[sc].err = ~0ull;
+    c->h_clk[sc].done = 0;
+    r = write_clock(c);
+    if (r) return r;
     c->wd_fresh = 0;
     c->wd_cur_is_B = 0;
     return DGR_OK;
 }
 
-extern "C" int dgr_download_state(dgr_ctx *c, double *zeta, double *Qx, double *Qy, int *WD)
+static int download_slice(dgr_ctx *c, int sc, double *zeta, double *Qx, double *Qy, int *WD)
 {
-    if (!c || !zeta || !Qx || !Qy) return DGR_ERR_INVALID;
+    if (!zeta || !Qx || !Qy || sc < 0 || sc >= c->nscen) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
-    const size_t n3 = 3 * (size_t)c->ne;
+    const int n = c->el_off[sc + 1] - c->el_off[sc];
+    const size_t n3 = 3 * (size_t)n;
     double *st = c->W;
     cudaStream_t s = c->stream;
-    k_planar_to_aos<<<blocks(c->ne, 256), 256, 0, s>>>(c->ne, c->ldE, c->U, st, st + n3, st + 2 * n3);
+    k_planar_to_aos<<<blocks(n, 256), 256, 0, s>>>(n, c->ldE, c->U + c->el_off[sc], st, st + n3, st + 2 * n3);
     c->launches++;
     CK(cudaMemcpyAsync(zeta, st, n3 * 8, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(Qx, st + n3, n3 * 8, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(Qy, st + 2 * n3, n3 * 8, cudaMemcpyDeviceToHost, s));
-    if (WD) CK(cudaMemcpyAsync(WD, c->wd_cur_is_B ? c->wdB : c->wdA, (size_t)c->ne * 4, cudaMemcpyDeviceToHost, s));
+    if (WD)
+        CK(cudaMemcpyAsync(WD, (c->wd_cur_is_B ? c->wdB : c->wdA) + c->el_off[sc], (size_t)n * 4,
+                           cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return DGR_OK;
+}
+
+extern "C" int dgr_upload_state(dgr_ctx *c, const double *zeta, const double *Qx, const double *Qy, const int *WD)
+{
+    if (!c || c->nscen != 1) return DGR_ERR_INVALID;
+    return upload_slice(c, 0, zeta, Qx, Qy, WD);
+}
+
+extern "C" int dgr_download_state(dgr_ctx *c, double *zeta, double *Qx, double *Qy, int *WD)
+{
+    if (!c || c->nscen != 1) return DGR_ERR_INVALID;
+    return download_slice(c, 0, zeta, Qx, Qy, WD);
+}
+
+extern "C" int dgr_ensemble_upload_state(dgr_ctx *c, int scenario, const double *zeta, const double *Qx,
+                                         const double *Qy, const int *WD)
+{
+    if (!c) return DGR_ERR_INVALID;
+    return upload_slice(c, scenario, zeta, Qx, Qy, WD);
+}
+
+extern "C" int dgr_ensemble_download_state(dgr_ctx *c, int scenario, double *zeta, double *Qx, double *Qy, int *WD)
+{
+    if (!c) return DGR_ERR_INVALID;
+    return download_slice(c, scenario, zeta, Qx, Qy, WD);
 }
 
 __global__ void k_scatter_bnd(int nb, const int *be, const double *vals, double *bzeta, double *bqn)
@@ -479,20 +675,19 @@ __global__ void k_scatter_bnd(int nb, const int *be, const double *vals, double 
 
 extern "C" int dgr_set_boundary(dgr_ctx *c, const double *bzeta, const double *bQn)
 {
-    if (!c || !bzeta || !bQn) return DGR_ERR_INVALID;
+    if (!c || !bzeta || !bQn || c->nscen != 1) return DGR_ERR_INVALID;
     if (c->nbnd == 0) return DGR_OK;
     CK(cudaSetDevice(c->device));
     /* only prescribed edges are read by the flux; copy those through a compact stage
      * (the pinned stage may still feed the previous copy: wait for the stream first) */
     CK(cudaStreamSynchronize(c->stream));
-    const std::vector<int> &be = *c->h_bnd;
+    const std::vector<int> &be = c->h_bnd;
     for (int j = 0; j < c->nbnd; ++j) {
         c->h_stage[j] = bzeta[be[j]];
         c->h_stage[c->nbnd + j] = bQn[be[j]];
     }
-    double *tmp = c->bstage;
-    CK(cudaMemcpyAsync(tmp, c->h_stage, sizeof(double) * 2 * c->nbnd, cudaMemcpyHostToDevice, c->stream));
-    k_scatter_bnd<<<blocks(c->nbnd, 256), 256, 0, c->stream>>>(c->nbnd, c->bnd_edges, tmp, c->bzeta, c->bqn);
+    CK(cudaMemcpyAsync(c->bstage, c->h_stage, sizeof(double) * 2 * c->nbnd, cudaMemcpyHostToDevice, c->stream));
+    k_scatter_bnd<<<blocks(c->nbnd, 256), 256, 0, c->stream>>>(c->nbnd, c->bnd_edges, c->bstage, c->bzeta, c->bqn);
     c->launches++;
     CK(cudaGetLastError());
     return DGR_OK;
@@ -503,8 +698,8 @@ extern "C" int dgr_boundary_conditions(dgr_ctx *c, double time)
     if (!c) return DGR_ERR_INVALID;
     if (c->nbnd == 0) return DGR_OK;
     CK(cudaSetDevice(c->device));
-    k_forcing<<<blocks(c->nbnd, 256), 256, 0, c->stream>>>(phys(c), time, c->bnd_edges, c->bnd_type, c->nbnd,
-                                                           c->bzeta, c->bqn);
+    k_forcing<<<blocks(c->nbnd, 256), 256, 0, c->stream>>>(c->clk, time, c->bnd_edges, c->bnd_type, c->bnd_sid,
+                                                           c->nbnd, c->bzeta, c->bqn);
     c->launches++;
     CK(cudaGetLastError());
     return DGR_OK;
@@ -514,40 +709,75 @@ extern "C" int dgr_boundary_conditions(dgr_ctx *c, double time)
 
 static const int *wd_current(const dgr_ctx *c) { return c->wd_cur_is_B ? c->wdB : c->wdA; }
 
-/* one RK stage; stage 0 reads U writes W, stage 1 reads W and U writes U */
-static void launch_stage(dgr_ctx *c, int stage, int phase_base, bool count)
+template <int MODE>
+static void launch_element(dgr_ctx *c, const double *S, const int *wd, double *OUT)
 {
     const MeshDev m = mesh_dev(c);
     cudaStream_t s = c->stream;
+    switch (c->bs) {
+    case 64:
+        k_element<MODE, 64><<<blocks(c->ne, 64), 64, 0, s>>>(m, S, c->U, wd, c->flux, OUT, c->avg, c->clk, c->p.g);
+        break;
+    case 256:
+        k_element<MODE, 256><<<blocks(c->ne, 256), 256, 0, s>>>(m, S, c->U, wd, c->flux, OUT, c->avg, c->clk, c->p.g);
+        break;
+    default:
+        k_element<MODE, 128><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, c->U, wd, c->flux, OUT, c->avg, c->clk, c->p.g);
+    }
+}
+
+template <bool L, bool P, bool ST>
+static void launch_limit(dgr_ctx *c, double *S, const int *wd_in, int *wd_out, int phase, int *dl, int *dp)
+{
+    const MeshDev m = mesh_dev(c);
+    cudaStream_t s = c->stream;
+    const double h0 = c->p.H0, vz = c->p.VELZERO;
+    switch (c->bs) {
+    case 64:
+        k_limit<L, P, ST, 64><<<blocks(c->ne, 64), 64, 0, s>>>(m, S, c->bounds, wd_in, wd_out, c->clk, h0, vz, phase,
+                                                               dl, dp);
+        break;
+    case 256:
+        k_limit<L, P, ST, 256><<<blocks(c->ne, 256), 256, 0, s>>>(m, S, c->bounds, wd_in, wd_out, c->clk, h0, vz,
+                                                                  phase, dl, dp);
+        break;
+    default:
+        k_limit<L, P, ST, 128><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, c->bounds, wd_in, wd_out, c->clk, h0, vz,
+                                                                  phase, dl, dp);
+    }
+}
+
+static void launch_edge(dgr_ctx *c, const double *S, const int *wd, int lam_slot, int phase)
+{
+    const MeshDev m = mesh_dev(c);
+    if (c->p.wet_dry)
+        k_edge_flux<true><<<blocks(c->nf, 256), 256, 0, c->stream>>>(m, S, wd, c->bzeta, c->bqn, c->flux, c->clk,
+                                                                     lam_slot, phase, c->p.g);
+    else
+        k_edge_flux<false><<<blocks(c->nf, 256), 256, 0, c->stream>>>(m, S, wd, c->bzeta, c->bqn, c->flux, c->clk,
+                                                                      lam_slot, phase, c->p.g);
+}
+
+/* one RK stage as four kernels; stage 0 reads U writes W, stage 1 reads W and U writes U */
+static void launch_stage(dgr_ctx *c, int stage, bool count)
+{
     const bool wd = c->p.wet_dry != 0;
-    const double g = c->p.g;
     const double *S = stage == 0 ? c->U : c->W;
     double *OUT = stage == 0 ? c->W : c->U;
-    const int *wd_in = stage == 0 ? c->wdA : c->wdB;
+    const int *wd_in = (stage == 0 || !wd) ? c->wdA : c->wdB;
     int *wd_out = stage == 0 ? c->wdB : c->wdA;
-    if (!wd) wd_in = c->wdA;
     int *dl = c->p.record_decisions ? c->dec + (size_t)(2 * stage) * c->ne : nullptr;
     int *dp = c->p.record_decisions ? c->dec + (size_t)(2 * stage + 1) * c->ne : nullptr;
-
-    if (wd)
-        k_edge_flux<true><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, c->flux, c->clk, stage,
-                                                             phase_base, g);
-    else
-        k_edge_flux<false><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, c->flux, c->clk, stage,
-                                                              phase_base, g);
+    launch_edge(c, S, wd_in, stage, 2 * stage);
     if (stage == 0)
-        k_element<MODE_STAGE1><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, c->U, wd_in, c->flux, OUT, c->avg, c->clk, g,
-                                                                  c->p.rain);
+        launch_element<MODE_STAGE1>(c, S, wd_in, OUT);
     else
-        k_element<MODE_STAGE2><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, c->U, wd_in, c->flux, OUT, c->avg, c->clk, g,
-                                                                  c->p.rain);
-    k_node_bounds<<<blocks(c->nn, 256), 256, 0, s>>>(m, c->avg, c->bounds, c->clk);
+        launch_element<MODE_STAGE2>(c, S, wd_in, OUT);
+    k_node_bounds<<<blocks(c->nn, 256), 256, 0, c->stream>>>(mesh_dev(c), c->avg, c->bounds);
     if (wd)
-        k_limit<true, true, true><<<blocks(c->ne, 128), 128, 0, s>>>(m, OUT, c->bounds, wd_in, wd_out, c->clk,
-                                                                     c->p.H0, c->p.VELZERO, phase_base + 1, dl, dp);
+        launch_limit<true, true, true>(c, OUT, wd_in, wd_out, 2 * stage + 1, dl, dp);
     else
-        k_limit<true, false, false><<<blocks(c->ne, 128), 128, 0, s>>>(m, OUT, c->bounds, wd_in, wd_out, c->clk,
-                                                                       c->p.H0, c->p.VELZERO, phase_base + 1, dl, dp);
+        launch_limit<true, false, false>(c, OUT, wd_in, wd_out, 2 * stage + 1, dl, dp);
     if (count) c->launches += 4;
 }
 
@@ -563,12 +793,95 @@ static void launch_wd_refresh(dgr_ctx *c)
     }
 }
 
-static int read_clock(dgr_ctx *c)
+/* persistent fused kernel: grid of co-resident blocks, cooperative launch */
+static FusedArgs fused_args(dgr_ctx *c)
 {
-    CK(cudaMemcpyAsync(c->h_clk, c->clk, sizeof(DevClock), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    return DGR_OK;
+    FusedArgs a;
+    a.m = mesh_dev(c);
+    a.U = c->U;
+    a.W = c->W;
+    a.flux = c->flux;
+    a.avg = c->avg;
+    a.bounds = c->bounds;
+    a.bzeta = c->bzeta;
+    a.bqn = c->bqn;
+    a.wdA = c->wdA;
+    a.wdB = c->wdB;
+    a.clk = c->clk;
+    a.nscen = c->nscen;
+    a.bnd_edges = c->bnd_edges;
+    a.bnd_type = c->bnd_type;
+    a.bnd_sid = c->bnd_sid;
+    a.nbnd = c->nbnd;
+    a.p = phys(c);
+    a.dec = c->p.record_decisions ? c->dec : nullptr;
+    a.bar = c->bar;
+    return a;
 }
+
+template <bool WD, int BS>
+static cudaError_t launch_fused_bs(dgr_ctx *c, int stage_begin, int stage_end, int with_clock)
+{
+    auto fn = k_step_fused<WD, BS>;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, BS, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const int need = (int)blocks(std::max(std::max(c->ne, c->nf), c->nn), BS);
+    const int grid = std::max(1, std::min(per_sm * c->num_sms, need));
+    FusedArgs a = fused_args(c);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(BS);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaMemsetAsync(c->bar, 0, 16, c->stream);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchKernelEx(&cfg, fn, a, stage_begin, stage_end, with_clock);
+}
+
+static cudaError_t launch_fused(dgr_ctx *c, int stage_begin, int stage_end, int with_clock)
+{
+    const bool wd = c->p.wet_dry != 0;
+    switch (c->bs) {
+    case 64:
+        return wd ? launch_fused_bs<true, 64>(c, stage_begin, stage_end, with_clock)
+                  : launch_fused_bs<false, 64>(c, stage_begin, stage_end, with_clock);
+    case 256:
+        return wd ? launch_fused_bs<true, 256>(c, stage_begin, stage_end, with_clock)
+                  : launch_fused_bs<false, 256>(c, stage_begin, stage_end, with_clock);
+    default:
+        return wd ? launch_fused_bs<true, 128>(c, stage_begin, stage_end, with_clock)
+                  : launch_fused_bs<false, 128>(c, stage_begin, stage_end, with_clock);
+    }
+}
+
+/* One step of the device loop with the current schedule. */
+static cudaError_t launch_step(dgr_ctx *c)
+{
+    cudaStream_t s = c->stream;
+    const PhysParams p = phys(c);
+    if (c->fusion == 2) return launch_fused(c, 0, 2, 1);
+    k_clock_begin<<<1, 256, 0, s>>>(c->clk, c->nscen, p, c->bnd_edges, c->bnd_type, c->bnd_sid, c->nbnd, c->bzeta,
+                                    c->bqn);
+    if (c->fusion == 1) {
+        cudaError_t e = launch_fused(c, 0, 1, 0);
+        if (e != cudaSuccess) return e;
+        e = launch_fused(c, 1, 2, 0);
+        if (e != cudaSuccess) return e;
+    } else {
+        launch_stage(c, 0, false);
+        launch_stage(c, 1, false);
+    }
+    k_clock_end<<<blocks(c->nscen, 256), 256, 0, s>>>(c->clk, c->nscen);
+    return cudaGetLastError();
+}
+
+static int kernels_per_step(const dgr_ctx *c) { return c->fusion == 2 ? 1 : (c->fusion == 1 ? 4 : 10); }
 
 static int decode_err(unsigned long long key, int *code, int *index, int *step)
 {
@@ -585,17 +898,34 @@ static int decode_err(unsigned long long key, int *code, int *index, int *step)
     return cd;
 }
 
+static int first_error(const dgr_ctx *c)
+{
+    for (int k = 0; k < c->nscen; ++k) {
+        const int cd = decode_err(c->h_clk[k].err, nullptr, nullptr, nullptr);
+        if (cd) return cd;
+    }
+    return DGR_OK;
+}
+
+static int check_barrier(dgr_ctx *c)
+{
+    if (c->fusion == 0) return DGR_OK;
+    unsigned flag = 0;
+    CK(cudaMemcpy(&flag, c->bar + 2, 4, cudaMemcpyDeviceToHost));
+    return flag ? DGR_ERR_TIMEOUT : DGR_OK;
+}
+
 extern "C" int dgr_step(dgr_ctx *c, double time, double dt, double *max_lambda)
 {
-    if (!c) return DGR_ERR_INVALID;
+    if (!c || c->nscen != 1) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     CK(cudaEventRecord(c->ev0, s));
     k_clock_set<<<1, 1, 0, s>>>(c->clk, time, dt);
     c->launches++;
     launch_wd_refresh(c);
-    launch_stage(c, 0, 0, true);
-    launch_stage(c, 1, 2, true);
+    launch_stage(c, 0, true);
+    launch_stage(c, 1, true);
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev1, s));
     if (c->p.wet_dry) {
@@ -607,27 +937,21 @@ extern "C" int dgr_step(dgr_ctx *c, double time, double dt, double *max_lambda)
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     c->last_ms = ms;
-    if (max_lambda) *max_lambda = bits_to_double(c->h_clk->lam_bits[1]);
-    return decode_err(c->h_clk->err, nullptr, nullptr, nullptr);
+    if (max_lambda) *max_lambda = bits_to_double(c->h_clk[0].lam_bits[1]);
+    return decode_err(c->h_clk[0].err, nullptr, nullptr, nullptr);
 }
 
 extern "C" int dgr_compute_L(dgr_ctx *c, double time, double *rz, double *rqx, double *rqy, double *max_lambda)
 {
     (void)time;
-    if (!c) return DGR_ERR_INVALID;
+    if (!c || c->nscen != 1) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
-    const MeshDev m = mesh_dev(c);
     k_clock_set<<<1, 1, 0, s>>>(c->clk, 0.0, 0.0);
     const int *wd = wd_current(c);
-    if (c->p.wet_dry)
-        k_edge_flux<true><<<blocks(c->nf, 256), 256, 0, s>>>(m, c->U, wd, c->bzeta, c->bqn, c->flux, c->clk, 0, 0,
-                                                             c->p.g);
-    else
-        k_edge_flux<false><<<blocks(c->nf, 256), 256, 0, s>>>(m, c->U, wd, c->bzeta, c->bqn, c->flux, c->clk, 0, 0,
-                                                              c->p.g);
-    k_element<MODE_RHS><<<blocks(c->ne, 128), 128, 0, s>>>(m, c->U, c->U, wd, c->flux, c->W, c->avg, c->clk, c->p.g,
-                                                           c->p.rain);
+    launch_edge(c, c->U, wd, 0, 0);
+    k_element<MODE_RHS, 128><<<blocks(c->ne, 128), 128, 0, s>>>(mesh_dev(c), c->U, c->U, wd, c->flux, c->W, c->avg,
+                                                                c->clk, c->p.g);
     c->launches += 3;
     CK(cudaGetLastError());
     if (rz && rqx && rqy) {
@@ -643,13 +967,13 @@ extern "C" int dgr_compute_L(dgr_ctx *c, double time, double *rz, double *rqx, d
     }
     int r = read_clock(c);
     if (r) return r;
-    if (max_lambda) *max_lambda = bits_to_double(c->h_clk->lam_bits[0]);
-    return decode_err(c->h_clk->err, nullptr, nullptr, nullptr);
+    if (max_lambda) *max_lambda = bits_to_double(c->h_clk[0].lam_bits[0]);
+    return decode_err(c->h_clk[0].err, nullptr, nullptr, nullptr);
 }
 
 extern "C" int dgr_get_fhat(dgr_ctx *c, double *f1, double *f2, double *f3)
 {
-    if (!c || !f1 || !f2 || !f3) return DGR_ERR_INVALID;
+    if (!c || !f1 || !f2 || !f3 || c->nscen != 1) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     const size_t n3 = 3 * (size_t)c->ne;
     double *tmp = nullptr;
@@ -666,16 +990,16 @@ extern "C" int dgr_get_fhat(dgr_ctx *c, double *f1, double *f2, double *f3)
 
 extern "C" int dgr_slope_limiter(dgr_ctx *c)
 {
-    if (!c) return DGR_ERR_INVALID;
+    if (!c || c->nscen != 1) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     const MeshDev m = mesh_dev(c);
     k_clock_set<<<1, 1, 0, s>>>(c->clk, 0.0, 0.0);
     k_avg<<<blocks(c->ne, 256), 256, 0, s>>>(m, c->U, c->avg);
-    k_node_bounds<<<blocks(c->nn, 256), 256, 0, s>>>(m, c->avg, c->bounds, c->clk);
+    k_node_bounds<<<blocks(c->nn, 256), 256, 0, s>>>(m, c->avg, c->bounds);
     int *dl = c->p.record_decisions ? c->dec : nullptr;
-    k_limit<true, false, false><<<blocks(c->ne, 128), 128, 0, s>>>(m, c->U, c->bounds, c->wdA, c->wdA, c->clk,
-                                                                   c->p.H0, c->p.VELZERO, 0, dl, nullptr);
+    k_limit<true, false, false, 128><<<blocks(c->ne, 128), 128, 0, s>>>(m, c->U, c->bounds, c->wdA, c->wdA, c->clk,
+                                                                         c->p.H0, c->p.VELZERO, 0, dl, nullptr);
     c->launches += 4;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
@@ -685,24 +1009,25 @@ extern "C" int dgr_slope_limiter(dgr_ctx *c)
 
 extern "C" int dgr_pdop(dgr_ctx *c)
 {
-    if (!c) return DGR_ERR_INVALID;
+    if (!c || c->nscen != 1) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     k_clock_set<<<1, 1, 0, s>>>(c->clk, 0.0, 0.0);
     int *dp = c->p.record_decisions ? c->dec + c->ne : nullptr;
-    k_limit<false, true, false><<<blocks(c->ne, 128), 128, 0, s>>>(mesh_dev(c), c->U, c->bounds, c->wdA, c->wdA,
-                                                                   c->clk, c->p.H0, c->p.VELZERO, 1, nullptr, dp);
+    k_limit<false, true, false, 128><<<blocks(c->ne, 128), 128, 0, s>>>(mesh_dev(c), c->U, c->bounds, c->wdA,
+                                                                         c->wdA, c->clk, c->p.H0, c->p.VELZERO, 1,
+                                                                         nullptr, dp);
     c->launches += 2;
     CK(cudaGetLastError());
     int r = read_clock(c);
     if (r) return r;
     c->wd_fresh = 0;
-    return decode_err(c->h_clk->err, nullptr, nullptr, nullptr);
+    return decode_err(c->h_clk[0].err, nullptr, nullptr, nullptr);
 }
 
 extern "C" int dgr_wet_dry_status(dgr_ctx *c)
 {
-    if (!c) return DGR_ERR_INVALID;
+    if (!c || c->nscen != 1) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     int *wd = c->wd_cur_is_B ? c->wdB : c->wdA;
@@ -717,86 +1042,213 @@ extern "C" int dgr_wet_dry_status(dgr_ctx *c)
 
 /* ---------------------------------------------------------- device loop ---- */
 
-/* Capture one step (clock, two stages, clock end) into a graph. */
+/* Capture one step with the current schedule into a graph (eager launches when the
+ * schedule cannot be captured). */
 static int build_graph(dgr_ctx *c)
 {
     drop_graph(c);
     cudaStream_t s = c->stream;
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    k_clock_begin<<<1, 256, 0, s>>>(c->clk, phys(c), c->bnd_edges, c->bnd_type, c->nbnd, c->bzeta, c->bqn);
-    /* the stage launches below see wd roles of a fresh step */
-    launch_stage(c, 0, 0, false);
-    launch_stage(c, 1, 2, false);
-    k_clock_end<<<1, 1, 0, s>>>(c->clk);
-    cudaError_t e = cudaStreamEndCapture(s, &c->graph);
-    if (e != cudaSuccess) {
-        snprintf(g_cuda_err, sizeof g_cuda_err, "capture: %s", cudaGetErrorString(e));
-        return DGR_ERR_CUDA;
+    cudaError_t e = launch_step(c);
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(s, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return DGR_OK; /* run eagerly */
     }
-    CK(cudaGraphInstantiate(&c->graph_exec, c->graph, 0));
-    c->graph_kernels = 10;
+    c->graph = g;
+    if (cudaGraphInstantiate(&c->graph_exec, c->graph, 0) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphDestroy(c->graph);
+        c->graph = nullptr;
+        c->graph_exec = nullptr;
+    }
     return DGR_OK;
 }
 
-__global__ void k_clock_init(DevClock *clk, double time, double dt, double final_time, int nsteps)
+/* Device loop for all scenarios: per scenario start clock (time_io[s] < 0 starts at t = 0
+ * with dt0), final time, and the common step limit. */
+static int run_impl(dgr_ctx *c, int nsteps, const double *final_time, double *time_io, double *dt_io,
+                    int *steps_done)
 {
-    clk->time = time;
-    clk->dt = dt;
-    clk->final_time = final_time;
-    clk->step = 0;
-    clk->nsteps = nsteps;
-    clk->done = 0;
-    clk->dt_pending = 0;
-}
-
-extern "C" int dgr_run(dgr_ctx *c, int nsteps, double final_time, double *time_io, double *dt_io, int *steps_done)
-{
-    if (!c || !time_io || !dt_io || nsteps < 0) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
-    double t0 = *time_io, dt = *dt_io;
-    const bool fresh_run = t0 < 0;
-    if (fresh_run) {
-        t0 = 0.0;
-        dt = c->p.dt0;
+    int r = read_clock(c);
+    if (r) return r;
+    for (int k = 0; k < c->nscen; ++k) {
+        DevClock &h = c->h_clk[k];
+        double t0 = time_io[k], dt = dt_io[k];
+        if (t0 < 0) {
+            t0 = 0.0;
+            dt = c->p.dt0;
+        }
+        h.time = t0;
+        h.dt = dt;
+        h.final_time = final_time[k];
+        h.step = 0;
+        h.nsteps = nsteps;
+        h.done = 0;
+        h.dt_pending = 0;
     }
+    r = write_clock(c);
+    if (r) return r;
     if (!c->graph_exec) {
-        int r = build_graph(c);
+        r = build_graph(c);
         if (r) return r;
     }
     CK(cudaEventRecord(c->ev0, s));
-    k_clock_init<<<1, 1, 0, s>>>(c->clk, t0, dt, final_time, nsteps);
-    c->launches++;
     launch_wd_refresh(c);
-    for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(c->graph_exec, s));
-    c->launches += (long long)nsteps * c->graph_kernels;
-    k_clock_finish<<<1, 1, 0, s>>>(c->clk, phys(c));
+    for (int i = 0; i < nsteps; ++i) {
+        if (c->graph_exec)
+            CK(cudaGraphLaunch(c->graph_exec, s));
+        else
+            CK(launch_step(c));
+    }
+    c->launches += (long long)nsteps * kernels_per_step(c);
+    k_clock_finish<<<blocks(c->nscen, 256), 256, 0, s>>>(c->clk, c->nscen, phys(c));
     c->launches++;
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev1, s));
-    int r = read_clock(c);
+    r = read_clock(c);
     if (r) return r;
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     c->last_ms = ms;
-    if (c->p.wet_dry && c->h_clk->step > 0) {
+    int any_step = 0;
+    for (int k = 0; k < c->nscen; ++k) {
+        time_io[k] = c->h_clk[k].time;
+        dt_io[k] = c->h_clk[k].dt;
+        if (steps_done) steps_done[k] = c->h_clk[k].step;
+        any_step |= c->h_clk[k].step > 0;
+    }
+    if (c->p.wet_dry && any_step) {
         c->wd_fresh = 1;
         c->wd_cur_is_B = 1;
     }
-    *time_io = c->h_clk->time;
-    *dt_io = c->h_clk->dt;
-    if (steps_done) *steps_done = c->h_clk->step;
-    return decode_err(c->h_clk->err, nullptr, nullptr, nullptr);
+    r = check_barrier(c);
+    if (r) return r;
+    return first_error(c);
+}
+
+extern "C" int dgr_run(dgr_ctx *c, int nsteps, double final_time, double *time_io, double *dt_io, int *steps_done)
+{
+    if (!c || !time_io || !dt_io || nsteps < 0 || c->nscen != 1) return DGR_ERR_INVALID;
+    return run_impl(c, nsteps, &final_time, time_io, dt_io, steps_done);
+}
+
+extern "C" int dgr_ensemble_run(dgr_ctx *c, int nsteps, const double *final_time, double *time_io, double *dt_io,
+                                int *steps_done)
+{
+    if (!c || !final_time || !time_io || !dt_io || nsteps < 0) return DGR_ERR_INVALID;
+    return run_impl(c, nsteps, final_time, time_io, dt_io, steps_done);
+}
+
+extern "C" int dgr_ensemble_last_error(dgr_ctx *c, int scenario, int *code, int *index, int *step)
+{
+    if (!c || scenario < 0 || scenario >= c->nscen) return DGR_ERR_INVALID;
+    CK(cudaSetDevice(c->device));
+    int r = read_clock(c);
+    if (r) return r;
+    decode_err(c->h_clk[scenario].err, code, index, step);
+    return DGR_OK;
 }
 
 extern "C" int dgr_last_error(dgr_ctx *c, int *code, int *index, int *step)
 {
+    return dgr_ensemble_last_error(c, 0, code, index, step);
+}
+
+extern "C" int dgr_set_schedule(dgr_ctx *c, int block_size, int fusion)
+{
+    if (!c || (block_size != 64 && block_size != 128 && block_size != 256) || fusion < 0 || fusion > 2)
+        return DGR_ERR_INVALID;
+    c->bs = block_size;
+    c->fusion = fusion;
+    drop_graph(c);
+    return DGR_OK;
+}
+
+extern "C" int dgr_get_schedule(const dgr_ctx *c, int *block_size, int *fusion)
+{
     if (!c) return DGR_ERR_INVALID;
+    if (block_size) *block_size = c->bs;
+    if (fusion) *fusion = c->fusion;
+    return DGR_OK;
+}
+
+/*
+ * Autotuner: times trial_steps steps of the device loop for every schedule (block size
+ * 64/128/256 x fusion depth 0/1/2) from the current state, restoring state, flags and
+ * clocks after each trial, and keeps the fastest.  Results do not depend on the schedule
+ * (same items, same arithmetic); only the time does.  ms_out (9 entries, or NULL)
+ * receives the ms per step of each trial at index 3*b + f (b: 64, 128, 256; f: fusion),
+ * -1 where the schedule could not run.
+ */
+extern "C" int dgr_autotune(dgr_ctx *c, int trial_steps, int *block_size, int *fusion, double *ms_out)
+{
+    if (!c || trial_steps <= 0) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    const size_t nU = 9 * (size_t)c->ldE;
+    double *saveU = nullptr;
+    int *saveWD = nullptr;
+    CK(cudaMallocAsync((void **)&saveU, nU * 8, s));
+    CK(cudaMallocAsync((void **)&saveWD, 2 * (size_t)c->ne * 4, s));
+    CK(cudaMemcpyAsync(saveU, c->U, nU * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(saveWD, c->wdA, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(saveWD + c->ne, c->wdB, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, s));
     int r = read_clock(c);
     if (r) return r;
-    decode_err(c->h_clk->err, code, index, step);
-    return DGR_OK;
+    const std::vector<DevClock> clk0(c->h_clk, c->h_clk + c->nscen);
+    const int fresh0 = c->wd_fresh, curB0 = c->wd_cur_is_B;
+    const int bss[3] = {64, 128, 256};
+    double best = 1e300;
+    int best_bs = c->bs, best_f = c->fusion;
+    std::vector<double> t(c->nscen), d(c->nscen), fin(c->nscen, 1e300);
+    for (int b = 0; b < 3; ++b)
+        for (int f = 0; f < 3; ++f) {
+            c->bs = bss[b];
+            c->fusion = f;
+            drop_graph(c);
+            for (int k = 0; k < c->nscen; ++k) {
+                t[k] = clk0[k].time;
+                d[k] = clk0[k].dt > 0 ? clk0[k].dt : c->p.dt0;
+            }
+            /* one untimed step builds the graph and warms the caches */
+            int rc = run_impl(c, 1, fin.data(), t.data(), d.data(), nullptr);
+            double ms = -1.0;
+            if (rc == DGR_OK) {
+                rc = run_impl(c, trial_steps, fin.data(), t.data(), d.data(), nullptr);
+                if (rc == DGR_OK) ms = c->last_ms / trial_steps;
+            }
+            cudaGetLastError();
+            if (ms_out) ms_out[3 * b + f] = ms;
+            if (ms > 0 && ms < best) {
+                best = ms;
+                best_bs = bss[b];
+                best_f = f;
+            }
+            /* restore */
+            CK(cudaMemcpyAsync(c->U, saveU, nU * 8, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(c->wdA, saveWD, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(c->wdB, saveWD + c->ne, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, s));
+            std::copy(clk0.begin(), clk0.end(), c->h_clk);
+            r = write_clock(c);
+            if (r) return r;
+            CK(cudaMemsetAsync(c->bar, 0, 16, s));
+            c->wd_fresh = fresh0;
+            c->wd_cur_is_B = curB0;
+        }
+    CK(cudaFreeAsync(saveU, s));
+    CK(cudaFreeAsync(saveWD, s));
+    CK(cudaStreamSynchronize(s));
+    c->bs = best_bs;
+    c->fusion = best_f;
+    drop_graph(c);
+    if (block_size) *block_size = best_bs;
+    if (fusion) *fusion = best_f;
+    return best < 1e300 ? DGR_OK : DGR_ERR_CUDA;
 }
 
 extern "C" int dgr_get_decisions(dgr_ctx *c, int stage, int *limit, int *pdop)
@@ -826,25 +1278,30 @@ extern "C" void dgr_host_free(void *p)
 }
 
 /*
- * Per-kernel device timing of whole steps: CUDA events around every launch of
- * nsteps host-driven steps (dt of the last run, or dt0).  kernel_ms[0..3] receive the
- * average ms of one launch of: edge flux, element RHS+RK, node bounds, limiter+PDop.
+ * Per-kernel device timing of whole steps: CUDA events around every launch of nsteps
+ * steps (dt of the last run, or dt0) with the four-kernel schedule.  kernel_ms[0..3]
+ * receive the average ms of one launch of: edge flux, element RHS+RK, node bounds,
+ * limiter+PDop.
  */
 extern "C" int dgr_profile_step(dgr_ctx *c, int nsteps, double *kernel_ms, int n)
 {
     if (!c || nsteps <= 0 || !kernel_ms || n < 4) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
-    const MeshDev m = mesh_dev(c);
     const bool wd = c->p.wet_dry != 0;
-    const double g = c->p.g;
-    cudaEvent_t ev[9];
-    for (int i = 0; i < 9; ++i) CK(cudaEventCreate(&ev[i]));
+    cudaEvent_t ev[5];
+    for (int i = 0; i < 5; ++i) CK(cudaEventCreate(&ev[i]));
     double acc[4] = {0, 0, 0, 0};
-    const double dt = (c->h_clk->dt > 0) ? c->h_clk->dt : c->p.dt0;
+    int r = read_clock(c);
+    if (r) return r;
+    for (int k = 0; k < c->nscen; ++k) {
+        if (!(c->h_clk[k].dt > 0)) c->h_clk[k].dt = c->p.dt0;
+        c->h_clk[k].done = 0;
+    }
+    r = write_clock(c);
+    if (r) return r;
     int rc = DGR_OK;
     for (int it = 0; it < nsteps && rc == DGR_OK; ++it) {
-        k_clock_set<<<1, 1, 0, s>>>(c->clk, 0.0, dt);
         launch_wd_refresh(c);
         for (int stage = 0; stage < 2; ++stage) {
             const double *S = stage == 0 ? c->U : c->W;
@@ -852,28 +1309,19 @@ extern "C" int dgr_profile_step(dgr_ctx *c, int nsteps, double *kernel_ms, int n
             const int *wd_in = (stage == 0 || !wd) ? c->wdA : c->wdB;
             int *wd_out = stage == 0 ? c->wdB : c->wdA;
             cudaEventRecord(ev[0], s);
-            if (wd)
-                k_edge_flux<true><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, c->flux, c->clk,
-                                                                     stage, 2 * stage, g);
-            else
-                k_edge_flux<false><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, c->flux, c->clk,
-                                                                      stage, 2 * stage, g);
+            launch_edge(c, S, wd_in, stage, 2 * stage);
             cudaEventRecord(ev[1], s);
             if (stage == 0)
-                k_element<MODE_STAGE1><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, c->U, wd_in, c->flux, OUT, c->avg,
-                                                                          c->clk, g, c->p.rain);
+                launch_element<MODE_STAGE1>(c, S, wd_in, OUT);
             else
-                k_element<MODE_STAGE2><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, c->U, wd_in, c->flux, OUT, c->avg,
-                                                                          c->clk, g, c->p.rain);
+                launch_element<MODE_STAGE2>(c, S, wd_in, OUT);
             cudaEventRecord(ev[2], s);
-            k_node_bounds<<<blocks(c->nn, 256), 256, 0, s>>>(m, c->avg, c->bounds, c->clk);
+            k_node_bounds<<<blocks(c->nn, 256), 256, 0, s>>>(mesh_dev(c), c->avg, c->bounds);
             cudaEventRecord(ev[3], s);
             if (wd)
-                k_limit<true, true, true><<<blocks(c->ne, 128), 128, 0, s>>>(
-                    m, OUT, c->bounds, wd_in, wd_out, c->clk, c->p.H0, c->p.VELZERO, 2 * stage + 1, nullptr, nullptr);
+                launch_limit<true, true, true>(c, OUT, wd_in, wd_out, 2 * stage + 1, nullptr, nullptr);
             else
-                k_limit<true, false, false><<<blocks(c->ne, 128), 128, 0, s>>>(
-                    m, OUT, c->bounds, wd_in, wd_out, c->clk, c->p.H0, c->p.VELZERO, 2 * stage + 1, nullptr, nullptr);
+                launch_limit<true, false, false>(c, OUT, wd_in, wd_out, 2 * stage + 1, nullptr, nullptr);
             cudaEventRecord(ev[4], s);
             c->launches += 4;
             if (cudaEventSynchronize(ev[4]) != cudaSuccess) {
@@ -891,7 +1339,7 @@ extern "C" int dgr_profile_step(dgr_ctx *c, int nsteps, double *kernel_ms, int n
             c->wd_cur_is_B = 1;
         }
     }
-    for (int i = 0; i < 9; ++i) cudaEventDestroy(ev[i]);
+    for (int i = 0; i < 5; ++i) cudaEventDestroy(ev[i]);
     if (rc) return rc;
     CK(cudaGetLastError());
     for (int k = 0; k < 4; ++k) kernel_ms[k] = acc[k] / (2.0 * nsteps);

@@ -433,6 +433,7 @@ const char *dgr_status_string(int code)
     case DGR_ERR_CUDA: return "CUDA error";
     case DGR_ERR_NO_DEVICE: return "no CUDA device";
     case DGR_ERR_TOO_LARGE: return "size beyond limit";
+    case DGR_ERR_TIMEOUT: return "device-side wait timed out";
     default: return "unknown status";
     }
 }

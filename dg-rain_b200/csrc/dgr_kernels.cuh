@@ -22,20 +22,25 @@
 #include "dgr_device.cuh"
 #include "dgr_forcing.h"
 
-/* Minimum resident blocks per SM requested from the compiler for the three step kernels
- * (register caps: 65536 / (block size x blocks)).  Chosen by measurement; overridable at
- * build time for tuning sweeps. */
+/* Minimum resident blocks per SM requested from the compiler for the edge kernel
+ * (register cap 65536 / (256 x blocks)); chosen by measurement, overridable at build time.
+ * The element kernels are capped at 128 registers and the limiter kernels at 85
+ * (launch bounds 512/BS and 768/BS blocks of BS threads). */
 #ifndef DGR_MINB_EDGE
 #define DGR_MINB_EDGE 3
 #endif
-#ifndef DGR_MINB_ELEMENT
-#define DGR_MINB_ELEMENT 4
-#endif
-#ifndef DGR_MINB_LIMIT
-#define DGR_MINB_LIMIT 6
-#endif
 
 namespace dgr {
+
+/* Loads of data that the same launch may have written on another SM (used by the
+ * persistent fused kernel, COH = true): served from L2, never from a stale L1 line or the
+ * read-only path.  The one-item-per-thread kernels use plain loads (COH = false). */
+template <bool COH, class T>
+DGR_DEV T ldm(const T *p)
+{
+    if (COH) return __ldcg(p);
+    return *p;
+}
 
 /* element geometry planes */
 enum {
@@ -58,6 +63,8 @@ enum {
     NG = 63
 };
 
+/* Clock and forcing of one scenario (one mesh of an ensemble; a single mesh is an
+ * ensemble of one).  Every scenario advances with its own CFL dt. */
 struct DevClock {
     double time;        /* current time */
     double dt;          /* dt of the step in progress, then of the next step */
@@ -69,6 +76,13 @@ struct DevClock {
     int nsteps;         /* step limit of the current run */
     int done;           /* 1: the run has finished, later kernels do nothing */
     int dt_pending;     /* 1: dt of the next step is still to be derived from lam_bits[1] */
+    /* per-scenario constants */
+    double min_edge;    /* minEdgLength of this scenario's mesh */
+    double rain;        /* m/s on the elevation equation (extension) */
+    double tide_amp, tide_period;
+    int tide_on;
+    int el_off, ed_off; /* first element / edge of the scenario in the flattened mesh */
+    int pad_;
 };
 
 struct MeshDev {
@@ -81,39 +95,36 @@ struct MeshDev {
     const double *geo;    /* [NG][ldE] */
     const int *n2e_ptr, *n2e;
     const double *zn;     /* node depth [nn] */
-    const double *minlen_cfl_unused;
+    const int *el_sid;    /* scenario of each element, NULL for a single mesh */
+    const int *ed_sid;    /* scenario of each edge, NULL for a single mesh */
 };
 
 struct PhysParams {
-    double g, h0, velzero, rain, cfl, dt0, min_edge, tide_amp, tide_period;
-    int tide_on;
+    double g, h0, velzero, cfl, dt0;
 };
 
 /* ------------------------------------------------------------------ edges ---- */
 
-/* One thread per edge: traces, ghost state, Roe flux(es), max wave speed
- * (2DCode/compute2DL.c:17-331). */
-template <bool WD>
-__global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, const double *__restrict__ S,
-                                                   const int *__restrict__ wd,
-                                                   const double *__restrict__ bzeta,
-                                                   const double *__restrict__ bqn,
-                                                   double *__restrict__ flux, DevClock *clk,
-                                                   int lam_slot, int phase, double g)
+/* One edge (2DCode/compute2DL.c:17-331): traces, ghost state, Roe flux(es); stores Fhat.n
+ * for both sides and returns the edge's max wave speed (0 for a finished scenario). */
+template <bool WD, bool COH = false>
+DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, const double *bzeta,
+                              const double *bqn, double *flux, DevClock *clk, int phase, double g, int i)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double lam = 0.0;
-    if (i < m.nf && !clk->done) {
+    DevClock *ck = clk + (m.ed_sid ? m.ed_sid[i] : 0);
+    if (!ldm<COH>(&ck->done)) {
         const int el_in = m.e_in[i], el_ex = m.e_ex[i], info = m.e_info[i];
         const int k_in = info & 3, k_ex = (info >> 2) & 3, bd = (info >> 4) & 7;
         const double nx = m.e_geo[i], ny = m.e_geo[m.ldF + i], z_edge = m.e_geo[2 * m.ldF + i];
         const double tx = -ny, ty = nx;
         const int ld = m.ldE;
-        const double zi = S[k_in * ld + el_in], qxi = S[(3 + k_in) * ld + el_in], qyi = S[(6 + k_in) * ld + el_in];
+        const double zi = ldm<COH>(&S[k_in * ld + el_in]), qxi = ldm<COH>(&S[(3 + k_in) * ld + el_in]),
+                     qyi = ldm<COH>(&S[(6 + k_in) * ld + el_in]);
         double ze, qxe, qye;
         if (bd) { /* :149-164 */
-            ze = bzeta[i];
-            double qn_ex = bqn[i];
+            ze = ldm<COH>(&bzeta[i]);
+            double qn_ex = ldm<COH>(&bqn[i]);
             if (ze < 0) ze = zi;
             if (qn_ex > 1000) qn_ex = qxi * nx + qyi * ny;
             const double qt_ex = qxi * tx + qyi * ty;
@@ -121,7 +132,7 @@ __global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, con
             qxe = (ty * qn_ex - ny * qt_ex) * d;
             qye = (-tx * qn_ex + nx * qt_ex) * d;
         } else if (el_in == el_ex) { /* land: reflect the normal discharge, :175-191 */
-            ze = S[k_ex * ld + el_ex];
+            ze = ldm<COH>(&S[k_ex * ld + el_ex]);
             const double qn_in = qxi * nx + qyi * ny;
             const double qt_in = qxi * tx + qyi * ty;
             const double qn_ex = -qn_in, qt_ex = qt_in;
@@ -129,14 +140,15 @@ __global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, con
             qxe = (ty * qn_ex - ny * qt_ex) * d;
             qye = (-tx * qn_ex + nx * qt_ex) * d;
         } else {
-            ze = S[k_ex * ld + el_ex];
-            qxe = S[(3 + k_ex) * ld + el_ex];
-            qye = S[(6 + k_ex) * ld + el_ex];
+            ze = ldm<COH>(&S[k_ex * ld + el_ex]);
+            qxe = ldm<COH>(&S[(3 + k_ex) * ld + el_ex]);
+            qye = ldm<COH>(&S[(6 + k_ex) * ld + el_ex]);
         }
 
         double fin[3], fex[3];
         int code = 0;
-        if (WD && wd[el_in] == 0 && wd[el_ex] == 0) { /* both dry, :203-239 */
+        const int wdi = WD ? ldm<COH>(&wd[el_in]) : 1, wde = WD ? ldm<COH>(&wd[el_ex]) : 1;
+        if (WD && wdi == 0 && wde == 0) { /* both dry, :203-239 */
             double qn_in = qxi * nx + qyi * ny;
             double qt_in = qxi * tx + qyi * ty;
             double qn_ex = -qn_in, qt_ex = qt_in;
@@ -156,14 +168,14 @@ __global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, con
             double fh[3];
             lam = roe_flux(fh, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, g, g);
             if (isnan(fh[0]) || isnan(fh[1]) || isnan(fh[2])) code = 1;
-            if (!WD || wd[el_in] == 1) {
+            if (!WD || wdi == 1) {
                 fin[0] = fh[0]; fin[1] = fh[1]; fin[2] = fh[2];
             } else {
                 const double l2 = roe_flux(fin, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g);
                 if (!code && (isnan(fin[0]) || isnan(fin[1]) || isnan(fin[2]))) code = 2;
                 lam = rmax(lam, l2);
             }
-            if (!WD || wd[el_ex] == 1) {
+            if (!WD || wde == 1) {
                 fex[0] = fh[0]; fex[1] = fh[1]; fex[2] = fh[2];
             } else {
                 const double l2 = roe_flux(fex, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g);
@@ -171,7 +183,7 @@ __global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, con
                 lam = rmax(lam, l2);
             }
         }
-        if (code) atomicMin(&clk->err, err_key(clk->step, phase, code, i));
+        if (code) atomicMin(&ck->err, err_key(ldm<COH>(&ck->step), phase, code, i - ck->ed_off));
         const int lf = m.ldF;
         flux[i] = fin[0];
         flux[lf + i] = fin[1];
@@ -180,44 +192,69 @@ __global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, con
         flux[4 * lf + i] = fex[1];
         flux[5 * lf + i] = fex[2];
         if (!(lam >= 0.0)) lam = 0.0; /* NaN speeds are reported through the flux check */
-    }
-    /* block max of the wave speed, then one atomic per block */
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, o));
+        }
+    return lam;
+}
+
+/* Max of the wave speed per scenario: one atomic per block when the block's edges all
+ * belong to one scenario (always for a single mesh), else one per lane. */
+DGR_DEV void block_max_speed(double lam, int sid, bool valid, DevClock *clk, int lam_slot)
+{
     __shared__ double red[32];
+    __shared__ int s_sid0;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) red[wid] = lam;
+    if (threadIdx.x == 0) s_sid0 = sid;
     __syncthreads();
-    if (wid == 0) {
-        lam = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
+    const int one_scenario = __syncthreads_and(!valid || sid == s_sid0);
+    if (one_scenario) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, o));
-        if (lane == 0 && lam > 0.0)
-            atomicMax(&clk->lam_bits[lam_slot], (unsigned long long)__double_as_longlong(lam));
+        if (lane == 0) red[wid] = lam;
+        __syncthreads();
+        if (wid == 0) {
+            lam = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, o));
+            if (lane == 0 && lam > 0.0)
+                atomicMax(&clk[s_sid0].lam_bits[lam_slot], (unsigned long long)__double_as_longlong(lam));
+        }
+        __syncthreads();
+    } else if (valid && lam > 0.0) {
+        atomicMax(&clk[sid].lam_bits[lam_slot], (unsigned long long)__double_as_longlong(lam));
     }
+}
+
+template <bool WD>
+__global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, const double *__restrict__ S,
+                                                                  const int *__restrict__ wd,
+                                                                  const double *__restrict__ bzeta,
+                                                                  const double *__restrict__ bqn,
+                                                                  double *__restrict__ flux, DevClock *clk,
+                                                                  int lam_slot, int phase, double g)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < m.nf;
+    const int sid = (valid && m.ed_sid) ? m.ed_sid[i] : 0;
+    const double lam = valid ? edge_flux_item<WD>(m, S, wd, bzeta, bqn, flux, clk, phase, g, i) : 0.0;
+    block_max_speed(lam, sid, valid, clk, lam_slot);
 }
 
 /* ---------------------------------------------------------------- elements ---- */
 
 enum { MODE_RHS = 0, MODE_STAGE1 = 1, MODE_STAGE2 = 2 };
 
-/*
- * One thread per element: surface and volume integrals of
- * 2DCode/2DInnerProducts.c:8-570, the right-hand side of 2DCode/compute2DL.c:338-411,
- * and the SSP-RK2 combination of 2DCode/time_evolution.c:76-88 (stage 1:
- * w1 = w + RHS*dt) or :176-217 (stage 2: w = (w1 + w)*0.5 + RHS*(dt/2)).
- * S is the stage input, U the step input (stage 2 only).  MODE_RHS writes the RHS.
- */
-template <int MODE>
-__global__ void __launch_bounds__(128, DGR_MINB_ELEMENT) k_element(MeshDev m, const double *__restrict__ S,
-                                                 const double *__restrict__ U,
-                                                 const int *__restrict__ wd,
-                                                 const double *__restrict__ flux,
-                                                 double *__restrict__ out, double *__restrict__ avg,
-                                                 const DevClock *clk, double g, double rain)
+/* One element: surface and volume integrals of 2DCode/2DInnerProducts.c:8-570, the
+ * right-hand side of 2DCode/compute2DL.c:338-411 and the SSP-RK2 combination of
+ * 2DCode/time_evolution.c:76-88 (stage 1: w1 = w + RHS*dt) or :176-217 (stage 2:
+ * w = (w1 + w)*0.5 + RHS*(dt/2)).  S is the stage input, U the step input (stage 2 only).
+ * MODE_RHS writes the RHS. */
+template <int MODE, bool COH = false>
+DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, const int *wd, const double *flux,
+                          double *out, double *avg, const DevClock *clk, double g, int el)
 {
-    const int el = blockIdx.x * blockDim.x + threadIdx.x;
-    if (el >= m.ne || clk->done) return;
+    const DevClock *ck = clk + (m.el_sid ? m.el_sid[el] : 0);
+    if (ldm<COH>(&ck->done)) return;
+    const double rain = ck->rain;
     const int ld = m.ldE;
     const double *G = m.geo + el;
 #define GEO(j) G[(size_t)(j) * ld]
@@ -231,7 +268,7 @@ __global__ void __launch_bounds__(128, DGR_MINB_ELEMENT) k_element(MeshDev m, co
         const int side = ee & 1;
 #pragma unroll
         for (int v = 0; v < 3; ++v) {
-            const double f = flux[(3 * side + v) * m.ldF + e];
+            const double f = ldm<COH>(&flux[(3 * side + v) * m.ldF + e]);
             F[v][k] = side ? -f : f;
         }
     }
@@ -269,11 +306,11 @@ __global__ void __launch_bounds__(128, DGR_MINB_ELEMENT) k_element(MeshDev m, co
     double zr[3], qxr[3], qyr[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        zr[k] = S[k * ld + el];
-        qxr[k] = S[(3 + k) * ld + el];
-        qyr[k] = S[(6 + k) * ld + el];
+        zr[k] = ldm<COH>(&S[k * ld + el]);
+        qxr[k] = ldm<COH>(&S[(3 + k) * ld + el]);
+        qyr[k] = ldm<COH>(&S[(6 + k) * ld + el]);
     }
-    const double local_g = (wd[el] == 0) ? 0.0 : g;
+    const double local_g = (ldm<COH>(&wd[el]) == 0) ? 0.0 : g;
     double H[3], tau[3], R[3][3]; /* R[variable][edge] = volume flux . n */
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
@@ -333,7 +370,7 @@ __global__ void __launch_bounds__(128, DGR_MINB_ELEMENT) k_element(MeshDev m, co
             for (int k = 0; k < 3; ++k) out[(3 * v + k) * ld + el] = rhs[v][k];
         return;
     }
-    const double dt = clk->dt;
+    const double dt = ldm<COH>(&ck->dt);
     double w[3][3];
     if (MODE == MODE_STAGE1) {
         w[0][0] = zr[0] + rhs[0][0] * dt;
@@ -351,7 +388,7 @@ __global__ void __launch_bounds__(128, DGR_MINB_ELEMENT) k_element(MeshDev m, co
 #pragma unroll
         for (int v = 0; v < 3; ++v)
 #pragma unroll
-            for (int k = 0; k < 3; ++k) w[v][k] = (s[v][k] + U[(3 * v + k) * ld + el]) * 0.5 + rhs[v][k] * hdt;
+            for (int k = 0; k < 3; ++k) w[v][k] = (s[v][k] + ldm<COH>(&U[(3 * v + k) * ld + el])) * 0.5 + rhs[v][k] * hdt;
     }
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
@@ -361,20 +398,28 @@ __global__ void __launch_bounds__(128, DGR_MINB_ELEMENT) k_element(MeshDev m, co
     }
 }
 
+template <int MODE, int BS>
+__global__ void __launch_bounds__(BS, 512 / BS) k_element(MeshDev m, const double *__restrict__ S,
+                                                          const double *__restrict__ U, const int *__restrict__ wd,
+                                                          const double *__restrict__ flux, double *__restrict__ out,
+                                                          double *__restrict__ avg, const DevClock *clk, double g)
+{
+    const int el = blockIdx.x * BS + threadIdx.x;
+    if (el < m.ne) element_item<MODE>(m, S, U, wd, flux, out, avg, clk, g, el);
+}
+
 /* ------------------------------------------------------------------ nodes ---- */
 
 /* Node max/min of element averages, 2DCode/SlopeLimiter2D.c:105-153 (the reference's
  * +-99999 starting values included). */
-__global__ void __launch_bounds__(256) k_node_bounds(MeshDev m, const double *__restrict__ avg,
-                                                     double *__restrict__ bounds, const DevClock *clk)
+template <bool COH = false>
+DGR_DEV void node_item(const MeshDev &m, const double *avg, double *bounds, int n)
 {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= m.nn || clk->done) return;
     double mx0 = -99999, mx1 = -99999, mx2 = -99999, mn0 = 99999, mn1 = 99999, mn2 = 99999;
     const int b = m.n2e_ptr[n], e = m.n2e_ptr[n + 1];
     for (int j = b; j < e; ++j) {
         const int el = m.n2e[j];
-        const double a0 = avg[el], a1 = avg[m.ldE + el], a2 = avg[2 * m.ldE + el];
+        const double a0 = ldm<COH>(&avg[el]), a1 = ldm<COH>(&avg[m.ldE + el]), a2 = ldm<COH>(&avg[2 * m.ldE + el]);
         if (a0 < mn0) mn0 = a0;
         if (a0 > mx0) mx0 = a0;
         if (a1 < mn1) mn1 = a1;
@@ -389,6 +434,13 @@ __global__ void __launch_bounds__(256) k_node_bounds(MeshDev m, const double *__
     bounds[3 * l + n] = mn0;
     bounds[4 * l + n] = mn1;
     bounds[5 * l + n] = mn2;
+}
+
+__global__ void __launch_bounds__(256) k_node_bounds(MeshDev m, const double *__restrict__ avg,
+                                                     double *__restrict__ bounds)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n < m.nn) node_item(m, avg, bounds, n);
 }
 
 /* Element means of a state (used by the stand-alone limiter call). */
@@ -429,7 +481,8 @@ __global__ void __launch_bounds__(256) k_wd_status(MeshDev m, const double *__re
                                                    const DevClock *clk, double h0)
 {
     const int el = blockIdx.x * blockDim.x + threadIdx.x;
-    if (el >= m.ne || clk->done) return;
+    if (el >= m.ne) return;
+    if (clk[m.el_sid ? m.el_sid[el] : 0].done) return;
     const int ld = m.ldE;
     const double mz[3] = {S[el], S[ld + el], S[2 * ld + el]};
     const double zn[3] = {m.zn[m.el2v[el]], m.zn[m.el2v[ld + el]], m.zn[m.el2v[2 * ld + el]]};
@@ -439,20 +492,17 @@ __global__ void __launch_bounds__(256) k_wd_status(MeshDev m, const double *__re
 /* ---------------------------------------------------------- limit + PDop ---- */
 
 /*
- * One thread per element: vertex-based limiter (2DCode/SlopeLimiter2D.c:157-343), then
- * the positive-depth operator (2DCode/wetDry2D.c:63-260), then the wet/dry status
+ * One element: vertex-based limiter (2DCode/SlopeLimiter2D.c:157-343), then the
+ * positive-depth operator (2DCode/wetDry2D.c:63-260), then the wet/dry status
  * (2DCode/wetDry2D.c:16-60) that the reference calls next.  wd_in is the status the
  * element had; the new status goes to wd_out.
  */
-template <bool LIMIT, bool PDOP, bool STATUS>
-__global__ void __launch_bounds__(128, DGR_MINB_LIMIT) k_limit(MeshDev m, double *__restrict__ S,
-                                               const double *__restrict__ bounds,
-                                               const int *__restrict__ wd_in, int *__restrict__ wd_out,
-                                               DevClock *clk, double h0, double velzero, int phase,
-                                               int *__restrict__ dec_limit, int *__restrict__ dec_pdop)
+template <bool LIMIT, bool PDOP, bool STATUS, bool COH = false>
+DGR_DEV void limit_item(const MeshDev &m, double *S, const double *bounds, const int *wd_in, int *wd_out,
+                        DevClock *clk, double h0, double velzero, int phase, int *dec_limit, int *dec_pdop, int el)
 {
-    const int el = blockIdx.x * blockDim.x + threadIdx.x;
-    if (el >= m.ne || clk->done) return;
+    DevClock *ck = clk + (m.el_sid ? m.el_sid[el] : 0);
+    if (ldm<COH>(&ck->done)) return;
     const int ld = m.ldE;
     const int nd[3] = {m.el2v[el], m.el2v[ld + el], m.el2v[2 * ld + el]};
     const double zn[3] = {m.zn[nd[0]], m.zn[nd[1]], m.zn[nd[2]]};
@@ -460,7 +510,7 @@ __global__ void __launch_bounds__(128, DGR_MINB_LIMIT) k_limit(MeshDev m, double
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) w[v][k] = S[(3 * v + k) * ld + el];
+        for (int k = 0; k < 3; ++k) w[v][k] = ldm<COH>(&S[(3 * v + k) * ld + el]);
 
     int modify = 0;
     if (LIMIT) {
@@ -473,8 +523,8 @@ __global__ void __launch_bounds__(128, DGR_MINB_LIMIT) k_limit(MeshDev m, double
             double vmax[3], vmin[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                vmax[k] = bounds[v * lb + nd[k]];
-                vmin[k] = bounds[(3 + v) * lb + nd[k]];
+                vmax[k] = ldm<COH>(&bounds[v * lb + nd[k]]);
+                vmin[k] = ldm<COH>(&bounds[(3 + v) * lb + nd[k]]);
             }
             const double avg = (w1 + w2 + w3) / 3;
             if (v == 0) { /* :189-200 */
@@ -616,7 +666,7 @@ __global__ void __launch_bounds__(128, DGR_MINB_LIMIT) k_limit(MeshDev m, double
                 w[2][2] = 0.5 * (qye[2] + qye[0]);
             }
         }
-        if (code) atomicMin(&clk->err, err_key(clk->step, phase, code, el));
+        if (code) atomicMin(&ck->err, err_key(ldm<COH>(&ck->step), phase, code, el - ck->el_off));
         if (dec_pdop) dec_pdop[el] = 4 * mass_branch + mom_branch;
     }
 
@@ -624,80 +674,114 @@ __global__ void __launch_bounds__(128, DGR_MINB_LIMIT) k_limit(MeshDev m, double
     for (int v = 0; v < 3; ++v)
 #pragma unroll
         for (int k = 0; k < 3; ++k) S[(3 * v + k) * ld + el] = w[v][k];
-    if (STATUS) wd_out[el] = wd_status(w[0], zn, wd_in[el], h0);
+    if (STATUS) wd_out[el] = wd_status(w[0], zn, ldm<COH>(&wd_in[el]), h0);
+}
+
+template <bool LIMIT, bool PDOP, bool STATUS, int BS>
+__global__ void __launch_bounds__(BS, 768 / BS) k_limit(MeshDev m, double *__restrict__ S,
+                                                        const double *__restrict__ bounds,
+                                                        const int *__restrict__ wd_in, int *__restrict__ wd_out,
+                                                        DevClock *clk, double h0, double velzero, int phase,
+                                                        int *__restrict__ dec_limit, int *__restrict__ dec_pdop)
+{
+    const int el = blockIdx.x * BS + threadIdx.x;
+    if (el < m.ne)
+        limit_item<LIMIT, PDOP, STATUS>(m, S, bounds, wd_in, wd_out, clk, h0, velzero, phase, dec_limit, dec_pdop,
+                                        el);
 }
 
 /* ------------------------------------------------------------------ clock ---- */
 
 /*
- * Start of one step of the device time loop (2DCode/time_evolution.c:311-401):
- * finish the CFL dt of the previous step, stop when time has reached final_time, write
- * the boundary values for this step (boundary_conditions() at the current time), then
- * advance the clock.  One block; thread 0 owns the clock.
+ * Start of one step of the device time loop (2DCode/time_evolution.c:311-401), for every
+ * scenario: finish the CFL dt of the previous step, stop when time has reached
+ * final_time, evaluate the boundary values for this step (boundary_conditions() at the
+ * current time), then advance the clock.  One block; thread s owns scenario s's clock,
+ * then all threads write the prescribed edges.
  */
-__global__ void __launch_bounds__(256) k_clock_begin(DevClock *clk, PhysParams p, const int *__restrict__ bnd_edges,
-                                                     const int *__restrict__ bnd_type, int nbnd,
-                                                     double *__restrict__ bzeta, double *__restrict__ bqn)
+DGR_DEV void clock_begin_body(DevClock *clk, int nscen, const PhysParams &p, const int *__restrict__ bnd_edges,
+                              const int *__restrict__ bnd_type, const int *__restrict__ bnd_sid, int nbnd,
+                              double *__restrict__ bzeta, double *__restrict__ bqn)
 {
-    __shared__ int s_go;
-    __shared__ double s_zb2;
-    if (threadIdx.x == 0) {
-        int go = !clk->done;
-        if (go && clk->dt_pending) {
-            const double lam = __longlong_as_double((long long)clk->lam_bits[1]);
-            double dt = p.cfl * p.min_edge / lam;
-            if ((clk->time + dt) > clk->final_time) dt = clk->final_time - clk->time;
-            clk->dt = dt;
-            clk->dt_pending = 0;
+    for (int s = threadIdx.x; s < nscen; s += blockDim.x) {
+        DevClock *c = clk + s;
+        if (c->done) continue;
+        if (c->dt_pending) {
+            const double lam = __longlong_as_double((long long)c->lam_bits[1]);
+            double dt = p.cfl * c->min_edge / lam;
+            if ((c->time + dt) > c->final_time) dt = c->final_time - c->time;
+            c->dt = dt;
+            c->dt_pending = 0;
         }
-        if (go && (clk->step >= clk->nsteps || !(clk->time < clk->final_time) || clk->err != ~0ull)) {
-            clk->done = 1;
-            go = 0;
+        if (c->step >= c->nsteps || !(c->time < c->final_time) || c->err != ~0ull) {
+            c->done = 1;
+            continue;
         }
-        if (go) {
-            s_zb2 = dgr_outflow_zeta(clk->time, p.tide_on, p.tide_amp, p.tide_period);
-            clk->bc2_zeta = s_zb2;
-            clk->time = clk->time + clk->dt;
-            clk->lam_bits[0] = 0;
-            clk->lam_bits[1] = 0;
-        }
-        s_go = go;
+        c->bc2_zeta = dgr_outflow_zeta(c->time, c->tide_on, c->tide_amp, c->tide_period);
+        c->time = c->time + c->dt;
+        c->lam_bits[0] = 0;
+        c->lam_bits[1] = 0;
     }
     __syncthreads();
-    if (!s_go) return;
     for (int j = threadIdx.x; j < nbnd; j += blockDim.x) {
+        const DevClock *c = clk + (bnd_sid ? bnd_sid[j] : 0);
+        if (c->done) continue;
         const int e = bnd_edges[j];
         const int t = bnd_type[j];
         double zb = 0, qn = 0;
         if (t == 1) { zb = DGR_BC1_ZETA; qn = DGR_BC1_QN; }
-        else if (t == 2) { zb = s_zb2; qn = DGR_BC2_QN; }
+        else if (t == 2) { zb = c->bc2_zeta; qn = DGR_BC2_QN; }
         else if (t == 3) { zb = DGR_BC3_ZETA; qn = DGR_BC3_QN; }
         bzeta[e] = zb;
         bqn[e] = qn;
     }
 }
 
-/* End of a step: the step counter and the pending CFL update. */
-__global__ void k_clock_end(DevClock *clk)
+__global__ void __launch_bounds__(256) k_clock_begin(DevClock *clk, int nscen, PhysParams p,
+                                                     const int *__restrict__ bnd_edges,
+                                                     const int *__restrict__ bnd_type,
+                                                     const int *__restrict__ bnd_sid, int nbnd,
+                                                     double *__restrict__ bzeta, double *__restrict__ bqn)
 {
-    if (clk->done) return;
-    clk->step += 1;
-    clk->dt_pending = 1;
+    clock_begin_body(clk, nscen, p, bnd_edges, bnd_type, bnd_sid, nbnd, bzeta, bqn);
 }
 
-/* After a run: derive the dt of the next step so the host sees it. */
-__global__ void k_clock_finish(DevClock *clk, PhysParams p)
+/* End of a step: step counters and the pending CFL updates.  A scenario whose step just
+ * failed stops here, so its step count is the number of steps that completed. */
+template <bool COH = false>
+DGR_DEV void clock_end_item(DevClock *clk, int s)
 {
-    if (clk->dt_pending) {
-        const double lam = __longlong_as_double((long long)clk->lam_bits[1]);
-        double dt = p.cfl * p.min_edge / lam;
-        if ((clk->time + dt) > clk->final_time) dt = clk->final_time - clk->time;
-        clk->dt = dt;
-        clk->dt_pending = 0;
+    if (clk[s].done) return;
+    if (ldm<COH>(&clk[s].err) != ~0ull) {
+        clk[s].done = 1;
+        return;
+    }
+    clk[s].step += 1;
+    clk[s].dt_pending = 1;
+}
+
+__global__ void k_clock_end(DevClock *clk, int nscen)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nscen) clock_end_item(clk, s);
+}
+
+/* After a run: derive each scenario's next dt so the host sees it. */
+__global__ void k_clock_finish(DevClock *clk, int nscen, PhysParams p)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nscen) return;
+    DevClock *c = clk + s;
+    if (c->dt_pending) {
+        const double lam = __longlong_as_double((long long)c->lam_bits[1]);
+        double dt = p.cfl * c->min_edge / lam;
+        if ((c->time + dt) > c->final_time) dt = c->final_time - c->time;
+        c->dt = dt;
+        c->dt_pending = 0;
     }
 }
 
-/* Host-driven step (oneTimeStep2D): set the step's dt and clear the per-step words. */
+/* Host-driven step (oneTimeStep2D, single mesh): set the step's dt, clear per-step words. */
 __global__ void k_clock_set(DevClock *clk, double time, double dt)
 {
     clk->time = time;
@@ -708,12 +792,14 @@ __global__ void k_clock_set(DevClock *clk, double time, double dt)
 }
 
 /* Device-side boundary_conditions() at time t for the stand-alone call. */
-__global__ void k_forcing(PhysParams p, double t, const int *__restrict__ bnd_edges, const int *__restrict__ bnd_type,
-                          int nbnd, double *__restrict__ bzeta, double *__restrict__ bqn)
+__global__ void k_forcing(const DevClock *clk, double t, const int *__restrict__ bnd_edges,
+                          const int *__restrict__ bnd_type, const int *__restrict__ bnd_sid, int nbnd,
+                          double *__restrict__ bzeta, double *__restrict__ bqn)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nbnd) return;
-    const double zb2 = dgr_outflow_zeta(t, p.tide_on, p.tide_amp, p.tide_period);
+    const DevClock *c = clk + (bnd_sid ? bnd_sid[j] : 0);
+    const double zb2 = dgr_outflow_zeta(t, c->tide_on, c->tide_amp, c->tide_period);
     const int e = bnd_edges[j];
     const int tt = bnd_type[j];
     double zb = 0, qn = 0;
@@ -722,6 +808,110 @@ __global__ void k_forcing(PhysParams p, double t, const int *__restrict__ bnd_ed
     else if (tt == 3) { zb = DGR_BC3_ZETA; qn = DGR_BC3_QN; }
     bzeta[e] = zb;
     bqn[e] = qn;
+}
+
+/* ------------------------------------------------------ persistent fused kernel ---- */
+
+struct FusedArgs {
+    MeshDev m;
+    double *U, *W, *flux, *avg, *bounds, *bzeta, *bqn;
+    int *wdA, *wdB;
+    DevClock *clk;
+    int nscen;
+    const int *bnd_edges, *bnd_type, *bnd_sid;
+    int nbnd;
+    PhysParams p;
+    int *dec;         /* [4][ne] decisions, or nullptr */
+    unsigned *bar;    /* [0] arrivals, [1] generation, [2] time-out flag */
+};
+
+/* Polls of a grid-barrier wait before it gives up (about a second with the 64 ns sleeps). */
+constexpr unsigned kBarrierSpins = 1u << 24;
+
+/* Grid-wide barrier of a cooperative launch (every block resident).  The wait is bounded:
+ * a block that polls kBarrierSpins times records a time-out, and every block leaves the
+ * kernel at its next barrier check, so a broken invariant ends the launch with an error
+ * flag instead of hanging the GPU.  Returns false once a time-out is recorded. */
+DGR_DEV bool grid_barrier(unsigned *bar)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *vgen = bar + 1;
+        const unsigned gen = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned spins = 0;
+            while (*vgen == gen) {
+                if (++spins > kBarrierSpins) {
+                    atomicExch(bar + 2, 1u);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile unsigned *)(bar + 2) == 0u;
+}
+
+/*
+ * One persistent cooperative kernel for RK stages stage_begin..stage_end-1 (and, with
+ * with_clock, the clock and boundary values of the step): the edge, element, node and
+ * limiter phases of the one-item-per-thread kernels, each a grid-stride loop, separated by
+ * grid barriers.  Arrays written by one phase and read by a later one are read through L2
+ * (COH loads).  Same items, same arithmetic: results are identical to the separate kernels.
+ */
+template <bool WD, int BS>
+__global__ void __launch_bounds__(BS, 512 / BS) k_step_fused(FusedArgs a, int stage_begin, int stage_end,
+                                                             int with_clock)
+{
+    if (with_clock) {
+        if (blockIdx.x == 0)
+            clock_begin_body(a.clk, a.nscen, a.p, a.bnd_edges, a.bnd_type, a.bnd_sid, a.nbnd, a.bzeta, a.bqn);
+        if (!grid_barrier(a.bar)) return;
+    }
+    const int stride = gridDim.x * BS;
+    const int ne = a.m.ne;
+    for (int stage = stage_begin; stage < stage_end; ++stage) {
+        const double *S = stage == 0 ? a.U : a.W;
+        double *OUT = stage == 0 ? a.W : a.U;
+        const int *wd_in = (stage == 0 || !WD) ? a.wdA : a.wdB;
+        int *wd_out = stage == 0 ? a.wdB : a.wdA;
+        int *dl = a.dec ? a.dec + (size_t)(2 * stage) * ne : nullptr;
+        int *dp = a.dec ? a.dec + (size_t)(2 * stage + 1) * ne : nullptr;
+        for (int base = blockIdx.x * BS; base < a.m.nf; base += stride) {
+            const int i = base + threadIdx.x;
+            const bool valid = i < a.m.nf;
+            const int sid = (valid && a.m.ed_sid) ? a.m.ed_sid[i] : 0;
+            const double lam =
+                valid ? edge_flux_item<WD, true>(a.m, S, wd_in, a.bzeta, a.bqn, a.flux, a.clk, 2 * stage, a.p.g, i)
+                      : 0.0;
+            block_max_speed(lam, sid, valid, a.clk, stage);
+        }
+        if (!grid_barrier(a.bar)) return;
+        for (int el = blockIdx.x * BS + threadIdx.x; el < ne; el += stride) {
+            if (stage == 0)
+                element_item<MODE_STAGE1, true>(a.m, S, a.U, wd_in, a.flux, OUT, a.avg, a.clk, a.p.g, el);
+            else
+                element_item<MODE_STAGE2, true>(a.m, S, a.U, wd_in, a.flux, OUT, a.avg, a.clk, a.p.g, el);
+        }
+        if (!grid_barrier(a.bar)) return;
+        for (int n = blockIdx.x * BS + threadIdx.x; n < a.m.nn; n += stride) node_item<true>(a.m, a.avg, a.bounds, n);
+        if (!grid_barrier(a.bar)) return;
+        for (int el = blockIdx.x * BS + threadIdx.x; el < ne; el += stride)
+            limit_item<true, WD, WD, true>(a.m, OUT, a.bounds, wd_in, wd_out, a.clk, a.p.h0, a.p.velzero,
+                                           2 * stage + 1, dl, dp, el);
+        if (stage + 1 < stage_end || with_clock)
+            if (!grid_barrier(a.bar)) return;
+    }
+    if (with_clock && blockIdx.x == 0)
+        for (int sc = threadIdx.x; sc < a.nscen; sc += BS) clock_end_item<true>(a.clk, sc);
 }
 
 /* ---------------------------------------------------------------- set-up ---- */
@@ -837,7 +1027,7 @@ __global__ void k_element_setup(int ne, int ldE, const int *__restrict__ el2v_ao
                    M11 * M22 * M33);
     const double midz[3] = {0.5 * (z[v0] + z[v1]), 0.5 * (z[v1] + z[v2]), 0.5 * (z[v2] + z[v0])};
     double midn[3];
-    if (n_el) {
+    if (n_el && n_el[i] >= 0.0) {
         midn[0] = midn[1] = midn[2] = n_el[i];
     } else {
         midn[0] = 0.5 * (nfric[v0] + nfric[v1]);

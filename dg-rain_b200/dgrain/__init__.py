@@ -5,9 +5,9 @@ from . import _lib
 from ._lib import DgrError, load
 from .mesh import (Mesh, build_connectivity, initial_state, read_fort14, rectangle,
                    rectangle_with_elements, write_fort14)
-from .solver import Solver, StepError, default_params
+from .solver import Ensemble, Solver, StepError, default_params
 
 __all__ = [
     "_lib", "DgrError", "load", "Mesh", "build_connectivity", "initial_state", "read_fort14",
-    "rectangle", "rectangle_with_elements", "write_fort14", "Solver", "StepError", "default_params",
+    "rectangle", "rectangle_with_elements", "write_fort14", "Ensemble", "Solver", "StepError", "default_params",
 ]

@@ -24,6 +24,7 @@ DGR_ERR_IO = 12
 DGR_ERR_CUDA = 13
 DGR_ERR_NO_DEVICE = 14
 DGR_ERR_TOO_LARGE = 15
+DGR_ERR_TIMEOUT = 16
 
 dptr = C.POINTER(C.c_double)
 iptr = C.POINTER(C.c_int)
@@ -60,6 +61,16 @@ class DgrMeshView(C.Structure):
         ("EdgtoVert", iptr),
         ("BdryPrescribed", iptr),
         ("minEdgLength", C.c_double),
+    ]
+
+
+class DgrScenarioParams(C.Structure):
+    _fields_ = [
+        ("tide_amp", C.c_double),
+        ("tide_period", C.c_double),
+        ("rain", C.c_double),
+        ("tide_on", C.c_int),
+        ("n_el", dptr),
     ]
 
 
@@ -118,6 +129,16 @@ SIGNATURES = [
     ("dgr_last_device_ms", C.c_double, [C.c_void_p]),
     ("dgr_profile_step", C.c_int, [C.c_void_p, C.c_int, dptr, C.c_int]),
     ("dgr_pow43_batch", C.c_int, [dptr, dptr, C.c_int, C.c_int]),
+    ("dgr_ensemble_create", C.c_int, [C.c_int, C.POINTER(DgrMeshView), C.POINTER(DgrScenarioParams),
+                                      C.POINTER(DgrParams), C.POINTER(C.c_void_p)]),
+    ("dgr_ensemble_size", C.c_int, [C.c_void_p]),
+    ("dgr_ensemble_upload_state", C.c_int, [C.c_void_p, C.c_int, dptr, dptr, dptr, iptr]),
+    ("dgr_ensemble_download_state", C.c_int, [C.c_void_p, C.c_int, dptr, dptr, dptr, iptr]),
+    ("dgr_ensemble_run", C.c_int, [C.c_void_p, C.c_int, dptr, dptr, dptr, iptr]),
+    ("dgr_ensemble_last_error", C.c_int, [C.c_void_p, C.c_int, iptr, iptr, iptr]),
+    ("dgr_set_schedule", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("dgr_get_schedule", C.c_int, [C.c_void_p, iptr, iptr]),
+    ("dgr_autotune", C.c_int, [C.c_void_p, C.c_int, iptr, iptr, dptr]),
     ("dgr_slope_limiter_noalloc", C.c_int,
      [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
 ]

@@ -83,7 +83,10 @@ def _pairs(a) -> np.ndarray:
 
 
 def rectangle(nx: int, ny: int, lx: float = 10000.0, ly: float = 5000.0, jitter: float = 0.0,
-              seed: int = 0, n_bumps: int = 8, manning: float = 0.03, connect: bool = True) -> Mesh:
+              seed: int = 0, n_bumps: int = 8, manning: float = 0.03, connect: bool = True,
+              datum: float = 0.0) -> Mesh:
+    """The synthetic coastal rectangle; `datum` lowers the whole land surface by that many
+    metres (datum = 3 gives a basin that is under water everywhere)."""
     rng = np.random.default_rng(seed)
     amp = rng.uniform(-0.5, 0.5, n_bumps)
     sig = rng.uniform(300.0, 800.0, n_bumps)
@@ -104,7 +107,7 @@ def rectangle(nx: int, ny: int, lx: float = 10000.0, ly: float = 5000.0, jitter:
         y = y + jy
     x = x.ravel()
     y = y.ravel()
-    elev = -5.0 + 7.0 * x / lx
+    elev = -5.0 + 7.0 * x / lx - datum
     for k in range(n_bumps):
         elev = elev + amp[k] * np.exp(-((x - cx[k]) ** 2 + (y - cy[k]) ** 2) / (2.0 * sig[k] ** 2))
     z = -elev
@@ -210,8 +213,13 @@ def log_uniform_sizes(n: int, lo: int, hi: int, seed: int) -> np.ndarray:
     return np.exp(rng.uniform(np.log(lo), np.log(hi), n))
 
 
-def rectangle_with_elements(n_el: float, seed: int, jitter: float = 0.1, **kw) -> Mesh:
-    """Rectangle mesh with about n_el triangles: nx = round(sqrt(n_el)), ny = nx // 2."""
+def rectangle_with_elements(n_el: float, seed: int, jitter: float = 0.1, cell: float | None = None, **kw) -> Mesh:
+    """Rectangle mesh with about n_el triangles: nx = round(sqrt(n_el)), ny = nx // 2.
+    With `cell` (metres) the domain is nx*cell by ny*cell instead of 10 km x 5 km, so the
+    resolution, and with it the CFL time step, stays that of the large workload."""
     nx = max(2, int(round(np.sqrt(n_el))))
     ny = max(1, nx // 2)
+    if cell is not None:
+        kw.setdefault("lx", nx * cell)
+        kw.setdefault("ly", ny * cell)
     return rectangle(nx, ny, jitter=jitter, seed=seed, **kw)

@@ -173,3 +173,125 @@ class Solver:
         out = (C.c_double * 4)()
         self._status(self.lib.dgr_profile_step(self.ctx, nsteps, out, 4), "dgr_profile_step")
         return list(out)
+
+
+def _schedule_methods(cls):
+    """Schedule controls shared by Solver and Ensemble (dgr_set_schedule / dgr_autotune)."""
+
+    def set_schedule(self, block_size: int = 128, fusion: int = 0) -> None:
+        _lib.check(self.lib.dgr_set_schedule(self.ctx, block_size, fusion), "dgr_set_schedule")
+
+    def get_schedule(self):
+        b, f = C.c_int(), C.c_int()
+        _lib.check(self.lib.dgr_get_schedule(self.ctx, C.byref(b), C.byref(f)), "dgr_get_schedule")
+        return b.value, f.value
+
+    def autotune(self, trial_steps: int = 5):
+        """Times every schedule from the current state (restored afterwards) and keeps the
+        fastest; returns (block_size, fusion, {(block_size, fusion): ms per step})."""
+        b, f = C.c_int(), C.c_int()
+        ms = (C.c_double * 9)()
+        _lib.check(self.lib.dgr_autotune(self.ctx, trial_steps, C.byref(b), C.byref(f), ms), "dgr_autotune")
+        table = {(bs, fu): ms[3 * i + fu] for i, bs in enumerate((64, 128, 256)) for fu in range(3)}
+        return b.value, f.value, table
+
+    cls.set_schedule = set_schedule
+    cls.get_schedule = get_schedule
+    cls.autotune = autotune
+    return cls
+
+
+_schedule_methods(Solver)
+
+
+@_schedule_methods
+class Ensemble:
+    """Many meshes advanced together by one context (dgr_ensemble_*): each scenario with
+    its own CFL dt, forcing and results, identical to running it alone."""
+
+    def __init__(self, meshes, scenarios=None, **common):
+        self.lib = _lib.load()
+        self.meshes = list(meshes)
+        n = len(self.meshes)
+        self.params = default_params(**common)
+        self._views = (_lib.DgrMeshView * n)(*[m.view() for m in self.meshes])
+        sp = (_lib.DgrScenarioParams * n)()
+        self._keep = []
+        for k in range(n):
+            d = dict(tide_on=self.params.tide_on, tide_amp=self.params.tide_amp,
+                     tide_period=self.params.tide_period, rain=self.params.rain, n_el=None)
+            if scenarios is not None:
+                d.update(scenarios[k])
+            sp[k].tide_on, sp[k].tide_amp = int(d["tide_on"]), float(d["tide_amp"])
+            sp[k].tide_period, sp[k].rain = float(d["tide_period"]), float(d["rain"])
+            if d["n_el"] is not None:
+                a = np.ascontiguousarray(d["n_el"], dtype=np.float64)
+                assert a.shape == (self.meshes[k].num_el,)
+                self._keep.append(a)
+                sp[k].n_el = _dp(a)
+        h = C.c_void_p()
+        _lib.check(self.lib.dgr_ensemble_create(n, self._views, sp, C.byref(self.params), C.byref(h)),
+                   "dgr_ensemble_create")
+        self.ctx = h
+        self.n = n
+
+    def close(self) -> None:
+        if self.ctx:
+            self.lib.dgr_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload_state(self, s: int, zeta, qx, qy, wd=None) -> None:
+        ne = self.meshes[s].num_el
+        z, x, y = (np.ascontiguousarray(a, dtype=np.float64) for a in (zeta, qx, qy))
+        assert z.shape == x.shape == y.shape == (3 * ne,)
+        w = None if wd is None else np.ascontiguousarray(wd, dtype=np.int32)
+        _lib.check(self.lib.dgr_ensemble_upload_state(self.ctx, s, _dp(z), _dp(x), _dp(y),
+                                                      None if w is None else _ip(w)), "dgr_ensemble_upload_state")
+
+    def download_state(self, s: int):
+        ne = self.meshes[s].num_el
+        z, x, y = np.empty(3 * ne), np.empty(3 * ne), np.empty(3 * ne)
+        w = np.empty(ne, dtype=np.int32)
+        _lib.check(self.lib.dgr_ensemble_download_state(self.ctx, s, _dp(z), _dp(x), _dp(y), _ip(w)),
+                   "dgr_ensemble_download_state")
+        return z, x, y, w
+
+    def run(self, nsteps: int, final_time=1e300, time=None, dt=None, check=True):
+        """Advances every scenario up to nsteps steps; returns (time[], dt[], steps[])."""
+        fin = np.ascontiguousarray(np.broadcast_to(np.asarray(final_time, dtype=np.float64), (self.n,)))
+        t = np.full(self.n, -1.0) if time is None else np.ascontiguousarray(time, dtype=np.float64).copy()
+        d = np.zeros(self.n) if dt is None else np.ascontiguousarray(dt, dtype=np.float64).copy()
+        steps = np.zeros(self.n, dtype=np.int32)
+        rc = self.lib.dgr_ensemble_run(self.ctx, nsteps, _dp(fin), _dp(t), _dp(d), _ip(steps))
+        if rc != _lib.DGR_OK and (check or not 1 <= rc <= 6):
+            if 1 <= rc <= 6:
+                for s in range(self.n):
+                    code, index, step = self.last_error(s)
+                    if code:
+                        raise StepError(code, index, step, f"ensemble scenario {s}")
+            _lib.check(rc, "dgr_ensemble_run")
+        return t, d, steps
+
+    def last_error(self, s: int):
+        code, index, step = C.c_int(), C.c_int(), C.c_int()
+        _lib.check(self.lib.dgr_ensemble_last_error(self.ctx, s, C.byref(code), C.byref(index), C.byref(step)),
+                   "dgr_ensemble_last_error")
+        return code.value, index.value, step.value
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.dgr_kernel_launches(self.ctx))
+
+    def last_device_ms(self) -> float:
+        return float(self.lib.dgr_last_device_ms(self.ctx))

@@ -65,7 +65,8 @@ enum dgr_status {
     DGR_ERR_IO = 12,          /* file cannot be read or written */
     DGR_ERR_CUDA = 13,        /* a CUDA call failed; see dgr_last_cuda_error() */
     DGR_ERR_NO_DEVICE = 14,   /* no CUDA device: this library has no CPU fallback */
-    DGR_ERR_TOO_LARGE = 15    /* size beyond a documented limit */
+    DGR_ERR_TOO_LARGE = 15,   /* size beyond a documented limit */
+    DGR_ERR_TIMEOUT = 16      /* a bounded device-side wait gave up (persistent kernel barrier) */
 };
 
 /* Run parameters.  dgr_params_default() fills the reference's constants. */
@@ -109,6 +110,15 @@ typedef struct dgr_fort14 {
     int num_inflow1, num_inflow2, num_outflow;
     int *inflow1, *inflow2, *outflow;     /* node pairs, 0-based, 2 per edge */
 } dgr_fort14;
+
+/* Forcing of one ensemble scenario (extensions: the reference has one mesh and no
+ * time-dependent forcing).  n_el: per-element Manning n ([num_el], copied), or NULL for
+ * the node average of 2DCode/2DInnerProducts.c:272-274. */
+typedef struct dgr_scenario_params {
+    double tide_amp, tide_period, rain;
+    int tide_on;
+    const double *n_el;
+} dgr_scenario_params;
 
 typedef struct dgr_ctx dgr_ctx;
 
@@ -191,6 +201,36 @@ DGR_API int dgr_step(dgr_ctx *ctx, double time, double dt, double *max_lambda);
  * continue a previous run.  The steps of one call are replayed from a CUDA graph. */
 DGR_API int dgr_run(dgr_ctx *ctx, int nsteps, double final_time, double *time_io, double *dt_io,
             int *steps_done);
+
+/* ---- batched ensemble: many meshes advanced together ---------------------------- */
+
+/* One context over nscen scenarios of uneven size.  The meshes are flattened into one
+ * (disjoint union); every kernel launch advances all of them, each scenario with its own
+ * CFL dt, clock, forcing, error word and results (identical to running it alone).
+ * Single-mesh calls (dgr_step, dgr_upload_state, ...) require nscen == 1. */
+DGR_API int dgr_ensemble_create(int nscen, const dgr_mesh_view *meshes, const dgr_scenario_params *sp,
+                                const dgr_params *common, dgr_ctx **out);
+DGR_API int dgr_ensemble_size(const dgr_ctx *ctx);
+DGR_API int dgr_ensemble_upload_state(dgr_ctx *ctx, int scenario, const double *zeta, const double *Qx,
+                                      const double *Qy, const int *WD);
+DGR_API int dgr_ensemble_download_state(dgr_ctx *ctx, int scenario, double *zeta, double *Qx, double *Qy,
+                                        int *WD);
+/* All scenarios advance up to nsteps steps; arrays are [nscen]; time_io[s] < 0 starts
+ * scenario s at t = 0 with dt0.  Returns the first scenario's failure code, if any
+ * (per-scenario detail: dgr_ensemble_last_error). */
+DGR_API int dgr_ensemble_run(dgr_ctx *ctx, int nsteps, const double *final_time, double *time_io,
+                             double *dt_io, int *steps_done);
+DGR_API int dgr_ensemble_last_error(dgr_ctx *ctx, int scenario, int *code, int *index, int *step);
+
+/* Schedule of the device loop: block size (elements per block of the element and limiter
+ * work: 64, 128, 256) and fusion depth (0: ten kernels per step; 1: one persistent
+ * cooperative kernel per RK stage; 2: one per step, clock included).  dgr_autotune times
+ * trial_steps steps of every schedule from the current state (restored afterwards),
+ * keeps the fastest and reports it; ms_out (9 entries or NULL) gets ms per step at index
+ * 3*b + f, b = 0,1,2 for 64,128,256.  Results do not depend on the schedule. */
+DGR_API int dgr_set_schedule(dgr_ctx *ctx, int block_size, int fusion);
+DGR_API int dgr_get_schedule(const dgr_ctx *ctx, int *block_size, int *fusion);
+DGR_API int dgr_autotune(dgr_ctx *ctx, int trial_steps, int *block_size, int *fusion, double *ms_out);
 
 /* First failure since the last upload: status code, edge or element index, step. */
 DGR_API int dgr_last_error(dgr_ctx *ctx, int *code, int *index, int *step);
