@@ -2,7 +2,7 @@
 device loop (block size x fusion depth).  Every scenario of an ensemble must give the
 bits it gives alone, under every schedule; a failing scenario stops alone.
 
-Scenarios are submerged basins at 5 m resolution (the ensemble workload): the reference
+Scenarios are basins at 5 m resolution under water everywhere (the ensemble workload): the reference
 wet/dry scheme runs them for thousands of steps with rain, whereas rain on dry land makes
 it stop on a NaN flux within tens of steps."""
 from __future__ import annotations
@@ -19,7 +19,7 @@ def scenarios(dgrain, sizes=(600, 1900, 350, 4100, 1200), seed=0):
     rng = np.random.default_rng(seed)
     meshes, params, states = [], [], []
     for k, n in enumerate(sizes):
-        m = dgrain.rectangle_with_elements(n, seed=100 + k, cell=5.0, datum=3.0)
+        m = dgrain.rectangle_with_elements(n, seed=100 + k, cell=5.0, datum=7.0)
         n_el = rng.uniform(0.02, 0.06, m.num_el) if k % 2 == 0 else None
         p = dict(tide_on=1, tide_amp=float(rng.uniform(0.2, 1.5)), tide_period=44712.0,
                  rain=float(rng.uniform(0, 100) / 3.6e6), n_el=n_el)
