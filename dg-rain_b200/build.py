@@ -29,7 +29,7 @@ CC_FLAGS = ["-std=c99", "-O2", "-ffp-contract=off", "-fPIC", "-Wall", "-Wextra",
 
 CU_SOURCES = ["dgr_capi.cu", "dgr_noalloc.cu"]
 C_SOURCES = ["dgr_host.c"]
-DEPS = ["dgr_kernels.cuh", "dgr_device.cuh", "dgr_forcing.h", os.path.join("..", "..", "include", "dgrain.h")]
+DEPS = ["dgr_kernels.cuh", "dgr_device.cuh", "dgr_forcing.h", "dgr_internal.cuh", os.path.join("..", "..", "include", "dgrain.h")]
 
 
 def _nvcc() -> str:

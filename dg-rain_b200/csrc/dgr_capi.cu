@@ -33,105 +33,14 @@
 #include <cstring>
 #include <vector>
 
-#include "../../include/dgrain.h"
-#include "dgr_kernels.cuh"
+#include "dgr_internal.cuh"
 
 using namespace dgr;
 
 static thread_local char g_cuda_err[256] = "";
-
-#define CK(call)                                                                              \
-    do {                                                                                      \
-        cudaError_t e_ = (call);                                                              \
-        if (e_ != cudaSuccess) {                                                              \
-            snprintf(g_cuda_err, sizeof g_cuda_err, "%s:%d %s: %s", __FILE__, __LINE__, #call, \
-                     cudaGetErrorString(e_));                                                 \
-            return DGR_ERR_CUDA;                                                              \
-        }                                                                                     \
-    } while (0)
+char *dgr_cuda_err_buffer() { return g_cuda_err; }
 
 extern "C" const char *dgr_last_cuda_error(void) { return g_cuda_err; }
-
-static int pad32(int n) { return (n + 31) & ~31; }
-
-static double bits_to_double(unsigned long long b)
-{
-    double d;
-    memcpy(&d, &b, sizeof d);
-    return d;
-}
-
-static unsigned blocks(int n, int t) { return (unsigned)((n + t - 1) / t); }
-
-struct dgr_ctx {
-    dgr_params p;
-    int device;
-    int nscen;
-    int ne, nn, nf, nbnd;
-    int ldE, ldF, ldN;
-    std::vector<int> el_off, nd_off, ed_off; /* [nscen + 1] */
-    std::vector<int> h_bnd;                  /* prescribed edges (flattened ids) */
-    cudaStream_t stream;
-    cudaEvent_t ev0, ev1;
-    int num_sms;
-    /* mesh */
-    double *x, *y, *zn, *nfric, *n_el;
-    int *el2v_aos, *el2v, *elem_edge, *e_in, *e_ex, *e_info, *n2e_ptr, *n2e, *bnd_edges, *bnd_type, *bnd_sid;
-    int *bdry, *el_sid, *ed_sid;
-    double *e_geo, *geo;
-    /* state and work */
-    double *U, *W, *flux, *avg, *bounds, *bzeta, *bqn, *bstage;
-    int *wdA, *wdB;
-    int *dec; /* [4][ne]: limit s0, pdop s0, limit s1, pdop s1 */
-    unsigned *bar;
-    DevClock *clk;
-    DevClock *h_clk; /* pinned mirror [nscen] */
-    double *h_stage;
-    int wd_fresh;    /* WA already holds the status for the next step */
-    int wd_cur_is_B; /* reference-semantic WD lives in WB */
-    long long launches;
-    double last_ms;
-    /* schedule of the device loop */
-    int bs;     /* block size of element/limiter work: 64, 128 or 256 */
-    int fusion; /* 0, 1 or 2 */
-    cudaGraph_t graph;
-    cudaGraphExec_t graph_exec;
-};
-
-static MeshDev mesh_dev(const dgr_ctx *c)
-{
-    MeshDev m;
-    m.ne = c->ne;
-    m.nn = c->nn;
-    m.nf = c->nf;
-    m.ldE = c->ldE;
-    m.ldF = c->ldF;
-    m.ldN = c->ldN;
-    m.el2v = c->el2v;
-    m.elem_edge = c->elem_edge;
-    m.e_in = c->e_in;
-    m.e_ex = c->e_ex;
-    m.e_info = c->e_info;
-    m.e_geo = c->e_geo;
-    m.geo = c->geo;
-    m.n2e_ptr = c->n2e_ptr;
-    m.n2e = c->n2e;
-    m.zn = c->zn;
-    m.el_sid = c->el_sid;
-    m.ed_sid = c->ed_sid;
-    return m;
-}
-
-static PhysParams phys(const dgr_ctx *c)
-{
-    PhysParams q;
-    q.g = c->p.g;
-    q.h0 = c->p.H0;
-    q.velzero = c->p.VELZERO;
-    q.cfl = c->p.cfl;
-    q.dt0 = c->p.dt0;
-    return q;
-}
 
 extern "C" int dgr_params_default(dgr_params *p)
 {
@@ -261,7 +170,7 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     if (tot_f >= (1LL << 30) || tot_e >= (1LL << 30) || tot_n >= (1LL << 30)) return DGR_ERR_TOO_LARGE;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-        snprintf(g_cuda_err, sizeof g_cuda_err, "no CUDA device visible");
+        snprintf(dgr_cuda_err_buffer(), 256, "no CUDA device visible");
         return DGR_ERR_NO_DEVICE;
     }
     dgr_ctx *c = new dgr_ctx();
@@ -417,7 +326,7 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     cudaFree(d_ed2v);
     cudaFree(d_bad);
     if (e1 != cudaSuccess) {
-        snprintf(g_cuda_err, sizeof g_cuda_err, "setup: %s", cudaGetErrorString(e1));
+        snprintf(dgr_cuda_err_buffer(), 256, "setup: %s", cudaGetErrorString(e1));
         release(c);
         return DGR_ERR_CUDA;
     }
@@ -1359,7 +1268,7 @@ extern "C" int dgr_pow43_batch(const double *x, double *y, int n, int device)
     cudaError_t e = cudaMemcpy(y, d + n, (size_t)n * 8, cudaMemcpyDeviceToHost);
     cudaFree(d);
     if (e != cudaSuccess) {
-        snprintf(g_cuda_err, sizeof g_cuda_err, "pow43: %s", cudaGetErrorString(e));
+        snprintf(dgr_cuda_err_buffer(), 256, "pow43: %s", cudaGetErrorString(e));
         return DGR_ERR_CUDA;
     }
     return DGR_OK;

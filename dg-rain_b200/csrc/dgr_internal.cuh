@@ -1,0 +1,115 @@
+/*
+ * Context of the device step shared by the C-ABI translation units (dgr_capi.cu: forward
+ * step, ensemble, schedules; dgr_adjoint.cu: discrete adjoint).  Internal: not part of the
+ * public header.
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/dgrain.h"
+#include "dgr_kernels.cuh"
+
+namespace dgr {
+struct AdjointState; /* dgr_adjoint.cu */
+}
+
+/* last CUDA error text, per host thread (dgr_last_cuda_error) */
+char *dgr_cuda_err_buffer();
+
+#define CK(call)                                                                                     \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess) {                                                                     \
+            snprintf(dgr_cuda_err_buffer(), 256, "%s:%d %s: %s", __FILE__, __LINE__, #call,          \
+                     cudaGetErrorString(e_));                                                        \
+            return DGR_ERR_CUDA;                                                                     \
+        }                                                                                            \
+    } while (0)
+
+static inline int pad32(int n) { return (n + 31) & ~31; }
+
+static inline double bits_to_double(unsigned long long b)
+{
+    double d;
+    memcpy(&d, &b, sizeof d);
+    return d;
+}
+
+static inline unsigned blocks(int n, int t) { return (unsigned)((n + t - 1) / t); }
+
+struct dgr_ctx {
+    dgr_params p;
+    int device;
+    int nscen;
+    int ne, nn, nf, nbnd;
+    int ldE, ldF, ldN;
+    std::vector<int> el_off, nd_off, ed_off; /* [nscen + 1] */
+    std::vector<int> h_bnd;                  /* prescribed edges (flattened ids) */
+    cudaStream_t stream;
+    cudaEvent_t ev0, ev1;
+    int num_sms;
+    /* mesh */
+    double *x, *y, *zn, *nfric, *n_el;
+    int *el2v_aos, *el2v, *elem_edge, *e_in, *e_ex, *e_info, *n2e_ptr, *n2e, *bnd_edges, *bnd_type, *bnd_sid;
+    int *bdry, *el_sid, *ed_sid;
+    double *e_geo, *geo;
+    /* state and work */
+    double *U, *W, *flux, *avg, *bounds, *bzeta, *bqn, *bstage;
+    int *wdA, *wdB;
+    int *dec; /* [4][ne]: limit s0, pdop s0, limit s1, pdop s1 */
+    unsigned *bar;
+    dgr::DevClock *clk;
+    dgr::DevClock *h_clk; /* pinned mirror [nscen] */
+    double *h_stage;
+    int wd_fresh;    /* WA already holds the status for the next step */
+    int wd_cur_is_B; /* reference-semantic WD lives in WB */
+    long long launches;
+    double last_ms;
+    /* schedule of the device loop */
+    int bs;     /* block size of element/limiter work: 64, 128 or 256 */
+    int fusion; /* 0, 1 or 2 */
+    cudaGraph_t graph;
+    cudaGraphExec_t graph_exec;
+    dgr::AdjointState *adj; /* discrete adjoint storage, created on first use */
+};
+
+static inline dgr::MeshDev mesh_dev(const dgr_ctx *c)
+{
+    dgr::MeshDev m;
+    m.ne = c->ne;
+    m.nn = c->nn;
+    m.nf = c->nf;
+    m.ldE = c->ldE;
+    m.ldF = c->ldF;
+    m.ldN = c->ldN;
+    m.el2v = c->el2v;
+    m.elem_edge = c->elem_edge;
+    m.e_in = c->e_in;
+    m.e_ex = c->e_ex;
+    m.e_info = c->e_info;
+    m.e_geo = c->e_geo;
+    m.geo = c->geo;
+    m.n2e_ptr = c->n2e_ptr;
+    m.n2e = c->n2e;
+    m.zn = c->zn;
+    m.el_sid = c->el_sid;
+    m.ed_sid = c->ed_sid;
+    return m;
+}
+
+static inline dgr::PhysParams phys(const dgr_ctx *c)
+{
+    dgr::PhysParams q;
+    q.g = c->p.g;
+    q.h0 = c->p.H0;
+    q.velzero = c->p.VELZERO;
+    q.cfl = c->p.cfl;
+    q.dt0 = c->p.dt0;
+    return q;
+}
+
