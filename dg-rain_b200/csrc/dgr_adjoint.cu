@@ -1,0 +1,556 @@
+/*
+ * Discrete adjoint and tangent-linear model of the device time loop (single mesh).
+ *
+ * Objective: J = sum over steps n and gauges g of (zeta_g(u^{n+1}) - target[n][g])^2, with
+ * zeta_g a fixed linear functional of one element's three midpoint elevations (e.g. the
+ * Crouzeix-Raviart interpolation at the gauge point).  Parameters: per-element Manning n,
+ * node depth z, and the initial state.
+ *
+ * Forward (dgr_adjoint_forward): the plain step (same kernels, same bits as dgr_run), the
+ * per-step CFL dt and boundary time recorded, gauge residuals stored, and a checkpoint
+ * (state, wet/dry status, clock) every K steps.
+ *
+ * Backward (dgr_adjoint_backward), per segment of K steps from the last:
+ *   1. recompute the segment from its checkpoint with the recorded dt, keeping per step and
+ *      stage the stage inputs, the pre-limiter outputs, element means, node bounds and the
+ *      wet/dry flags (the decisions are recomputed bit for bit, i.e. frozen);
+ *   2. reverse each step: misfit, then per stage (2 then 1) limiter+PDop, node bounds,
+ *      element, edge reverse kernels (dgr_tlm.cuh).
+ * Memory: checkpoints 72 B per element per K steps; segment store about 390 B per element
+ * and step, times K.
+ *
+ * TLM (dgr_tlm): the same steps in dual numbers with the recorded dt (frozen), giving J and
+ * its directional derivative; its primal part is the forward bit for bit.
+ */
+#include <algorithm>
+
+#include "dgr_internal.cuh"
+#include "dgr_tlm.cuh"
+
+using namespace dgr;
+
+namespace dgr {
+
+struct AdjointState {
+    int nsteps = 0, K = 0, nseg = 0, ng = 0;
+    int have_forward = 0;
+    int *g_el = nullptr;
+    double *g_w = nullptr, *target = nullptr, *resid = nullptr, *sums = nullptr;
+    double *dt_hist = nullptr, *time_hist = nullptr;
+    double *ckU = nullptr;
+    int *ckWd = nullptr;
+    DevClock *ckClk = nullptr;
+    /* segment store */
+    double *segU = nullptr, *segW = nullptr, *segR = nullptr, *segAvg = nullptr, *segB = nullptr;
+    int *segWd = nullptr;
+    /* adjoint work */
+    double *lamU = nullptr, *lamW = nullptr, *Rbar = nullptr, *bbar = nullptr, *bnode = nullptr, *fbar = nullptr;
+    double *zvb = nullptr, *zeb = nullptr, *nbar = nullptr, *zbar = nullptr;
+    int *barg = nullptr;
+    /* tangent work */
+    double *Ud = nullptr, *Wd = nullptr, *flux_d = nullptr, *avg_d = nullptr, *bounds_d = nullptr;
+    double *zd = nullptr, *neld = nullptr, *rd = nullptr, *rt = nullptr;
+    double fwd_ms = 0, bwd_ms = 0, tlm_ms = 0;
+};
+
+}  // namespace dgr
+
+void adjoint_release(dgr_ctx *c)
+{
+    AdjointState *a = c->adj;
+    if (!a) return;
+    void *ptrs[] = {a->g_el, a->g_w, a->target, a->resid, a->sums, a->dt_hist, a->time_hist, a->ckU, a->ckWd,
+                    a->ckClk, a->segU, a->segW, a->segR, a->segAvg, a->segB, a->segWd, a->lamU, a->lamW,
+                    a->Rbar, a->bbar, a->bnode, a->fbar, a->zvb, a->zeb, a->nbar, a->zbar, a->barg, a->Ud,
+                    a->Wd, a->flux_d, a->avg_d, a->bounds_d, a->zd, a->neld, a->rd, a->rt};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    delete a;
+    c->adj = nullptr;
+}
+
+/* ------------------------------------------------------------- storage layout ---- */
+
+static size_t plane9(const dgr_ctx *c) { return (size_t)9 * c->ldE; }
+static double *seg_U(const dgr_ctx *c, int j) { return c->adj->segU + (size_t)j * plane9(c); }
+static double *seg_W(const dgr_ctx *c, int j) { return c->adj->segW + (size_t)j * plane9(c); }
+static double *seg_R(const dgr_ctx *c, int j, int s) { return c->adj->segR + (size_t)(2 * j + s) * plane9(c); }
+static double *seg_avg(const dgr_ctx *c, int j, int s)
+{
+    return c->adj->segAvg + (size_t)(2 * j + s) * 3 * c->ldE;
+}
+static double *seg_B(const dgr_ctx *c, int j, int s) { return c->adj->segB + (size_t)(2 * j + s) * 6 * c->ldN; }
+static int *seg_wd(const dgr_ctx *c, int j, int s) { return c->adj->segWd + (size_t)(2 * j + s) * c->ne; }
+
+extern "C" int dgr_adjoint_setup(dgr_ctx *c, int nsteps, int ckpt_every, int ngauges, const int *gauge_el,
+                                 const double *gauge_w, const double *target)
+{
+    if (!c || c->nscen != 1 || nsteps <= 0 || ckpt_every <= 0 || ngauges <= 0 || !gauge_el || !gauge_w)
+        return DGR_ERR_INVALID;
+    for (int g = 0; g < ngauges; ++g)
+        if (gauge_el[g] < 0 || gauge_el[g] >= c->ne) return DGR_ERR_INVALID;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    adjoint_release(c);
+    AdjointState *a = new AdjointState();
+    c->adj = a;
+    a->nsteps = nsteps;
+    a->K = std::min(ckpt_every, nsteps);
+    a->nseg = (nsteps + a->K - 1) / a->K;
+    a->ng = ngauges;
+    const size_t E = c->ldE, F = c->ldF, N = c->ldN, K = a->K;
+    const size_t ns = nsteps, ng = ngauges;
+    int r = 0;
+#define AL(p, n)                       \
+    do {                               \
+        r = dalloc(&(p), (n));         \
+        if (r) {                       \
+            adjoint_release(c);        \
+            return r;                  \
+        }                              \
+    } while (0)
+    AL(a->g_el, ng);
+    AL(a->g_w, 3 * ng);
+    AL(a->target, ns * ng);
+    AL(a->resid, ns * ng);
+    AL(a->rd, ns * ng);
+    AL(a->rt, ns * ng);
+    AL(a->sums, 2);
+    AL(a->dt_hist, ns);
+    AL(a->time_hist, ns);
+    AL(a->ckU, (size_t)a->nseg * 9 * E);
+    AL(a->ckWd, (size_t)a->nseg * c->ne);
+    AL(a->ckClk, a->nseg);
+    AL(a->segU, K * 9 * E);
+    AL(a->segW, K * 9 * E);
+    AL(a->segR, K * 2 * 9 * E);
+    AL(a->segAvg, K * 2 * 3 * E);
+    AL(a->segB, K * 2 * 6 * N);
+    AL(a->segWd, K * 2 * c->ne);
+    AL(a->lamU, 9 * E);
+    AL(a->lamW, 9 * E);
+    AL(a->Rbar, 9 * E);
+    AL(a->bbar, 18 * E);
+    AL(a->bnode, 6 * N);
+    AL(a->barg, 6 * N);
+    AL(a->fbar, 6 * F);
+    AL(a->zvb, 3 * E);
+    AL(a->zeb, F);
+    AL(a->nbar, E);
+    AL(a->zbar, (size_t)c->nn);
+#undef AL
+    cudaStream_t s = c->stream;
+    CK(cudaMemcpyAsync(a->g_el, gauge_el, ng * 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(a->g_w, gauge_w, 3 * ng * 8, cudaMemcpyHostToDevice, s));
+    if (target)
+        CK(cudaMemcpyAsync(a->target, target, ns * ng * 8, cudaMemcpyHostToDevice, s));
+    else
+        CK(cudaMemsetAsync(a->target, 0, ns * ng * 8, s));
+    CK(cudaMemsetAsync(a->fbar, 0, 6 * F * 8, s));
+    CK(cudaStreamSynchronize(s));
+    return DGR_OK;
+}
+
+extern "C" int dgr_adjoint_set_target(dgr_ctx *c, const double *target)
+{
+    if (!c || !c->adj || !target) return DGR_ERR_INVALID;
+    CK(cudaSetDevice(c->device));
+    const size_t n = (size_t)c->adj->nsteps * c->adj->ng;
+    CK(cudaMemcpyAsync(c->adj->target, target, n * 8, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return DGR_OK;
+}
+
+extern "C" int dgr_set_bathymetry(dgr_ctx *c, const double *z)
+{
+    if (!c || !z || c->nscen != 1) return DGR_ERR_INVALID;
+    CK(cudaSetDevice(c->device));
+    CK(cudaMemcpyAsync(c->zn, z, (size_t)c->nn * 8, cudaMemcpyHostToDevice, c->stream));
+    k_edge_zsetup<<<blocks(c->nf, 256), 256, 0, c->stream>>>(mesh_dev(c), c->e_geo);
+    c->launches++;
+    int r = upload_geometry(c);
+    if (r) return r;
+    c->wd_fresh = 0; /* the status depends on the depths */
+    CK(cudaStreamSynchronize(c->stream));
+    return DGR_OK;
+}
+
+/* ------------------------------------------------------------------ forward ---- */
+
+static void clock_begin_step(dgr_ctx *c, int n, int replay)
+{
+    AdjointState *a = c->adj;
+    k_adj_clock_begin<<<1, 256, 0, c->stream>>>(c->clk, phys(c), c->bnd_edges, c->bnd_type, c->nbnd, c->bzeta,
+                                                  c->bqn, a->dt_hist, a->time_hist, n, replay);
+}
+
+static int start_clock(dgr_ctx *c, double time, double dt)
+{
+    int r = read_clock(c);
+    if (r) return r;
+    DevClock &h = c->h_clk[0];
+    if (time < 0) {
+        time = 0.0;
+        dt = c->p.dt0;
+    }
+    h.time = time;
+    h.dt = dt;
+    h.final_time = 1e300;
+    h.step = 0;
+    h.nsteps = c->adj->nsteps;
+    h.done = 0;
+    h.dt_pending = 0;
+    h.err = ~0ull;
+    return write_clock(c);
+}
+
+extern "C" int dgr_adjoint_forward(dgr_ctx *c, const double *zeta, const double *Qx, const double *Qy, const int *WD,
+                                   double time, double dt, int replay_dt, double *J, double *gauge_values)
+{
+    if (!c || !c->adj || !zeta || !Qx || !Qy || !WD) return DGR_ERR_INVALID;
+    AdjointState *a = c->adj;
+    if (replay_dt && !a->have_forward) return DGR_ERR_INVALID;
+    CK(cudaSetDevice(c->device));
+    int r = dgr_upload_state(c, zeta, Qx, Qy, WD);
+    if (r) return r;
+    r = start_clock(c, time, dt);
+    if (r) return r;
+    cudaStream_t s = c->stream;
+    const size_t E9 = plane9(c);
+    CK(cudaEventRecord(c->ev0, s));
+    launch_wd_refresh(c);
+    for (int n = 0; n < a->nsteps; ++n) {
+        if (n % a->K == 0) {
+            const int sg = n / a->K;
+            CK(cudaMemcpyAsync(a->ckU + sg * E9, c->U, E9 * 8, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(a->ckWd + (size_t)sg * c->ne, c->wdA, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice,
+                               s));
+            CK(cudaMemcpyAsync(a->ckClk + sg, c->clk, sizeof(DevClock), cudaMemcpyDeviceToDevice, s));
+        }
+        clock_begin_step(c, n, replay_dt);
+        launch_stage(c, 0, true);
+        launch_stage(c, 1, true);
+        k_clock_end<<<1, 32, 0, s>>>(c->clk, 1);
+        k_misfit<<<1, 32, 0, s>>>(c->U, c->ldE, a->ng, a->g_el, a->g_w, a->target + (size_t)n * a->ng,
+                                  a->resid + (size_t)n * a->ng);
+        c->launches += 3;
+    }
+    k_misfit_sum<<<1, 32, 0, s>>>(a->resid, nullptr, (long long)a->nsteps * a->ng, a->sums);
+    k_clock_finish<<<1, 32, 0, s>>>(c->clk, 1, phys(c));
+    c->launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev1, s));
+    r = read_clock(c);
+    if (r) return r;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    a->fwd_ms = ms;
+    if (c->p.wet_dry) {
+        c->wd_fresh = 1;
+        c->wd_cur_is_B = 1;
+    }
+    r = first_error(c);
+    if (r) return r;
+    if (c->h_clk[0].step != a->nsteps) return DGR_ERR_INVALID;
+    double sums[2];
+    CK(cudaMemcpy(sums, a->sums, 16, cudaMemcpyDeviceToHost));
+    if (J) *J = sums[0];
+    if (gauge_values) {
+        const size_t cnt = (size_t)a->nsteps * a->ng;
+        std::vector<double> rr(cnt), tt(cnt);
+        CK(cudaMemcpy(rr.data(), a->resid, cnt * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(tt.data(), a->target, cnt * 8, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < cnt; ++i) gauge_values[i] = rr[i] + tt[i];
+    }
+    a->have_forward = 1;
+    return DGR_OK;
+}
+
+extern "C" int dgr_adjoint_dt(dgr_ctx *c, double *dt_out, double *time_out)
+{
+    if (!c || !c->adj || !c->adj->have_forward) return DGR_ERR_INVALID;
+    CK(cudaSetDevice(c->device));
+    const size_t n = c->adj->nsteps;
+    if (dt_out) CK(cudaMemcpy(dt_out, c->adj->dt_hist, n * 8, cudaMemcpyDeviceToHost));
+    if (time_out) CK(cudaMemcpy(time_out, c->adj->time_hist, n * 8, cudaMemcpyDeviceToHost));
+    return DGR_OK;
+}
+
+/* ----------------------------------------------------------------- backward ---- */
+
+/* one recorded stage of step slot j: the stage kernels with the pre-limiter output, means
+ * and bounds kept in the segment store; S -> OUT (OUT may be the next step's input slot) */
+static void recorded_stage(dgr_ctx *c, int j, int stage, const double *S, double *OUT, const int *wd_in,
+                           int *wd_out)
+{
+    const MeshDev m = mesh_dev(c);
+    cudaStream_t s = c->stream;
+    const bool wd = c->p.wet_dry != 0;
+    double *R = seg_R(c, j, stage), *avg = seg_avg(c, j, stage), *bnd = seg_B(c, j, stage);
+    if (wd)
+        k_edge_flux<true><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, c->flux, c->clk, stage,
+                                                             2 * stage, c->p.g);
+    else
+        k_edge_flux<false><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, c->flux, c->clk,
+                                                              stage, 2 * stage, c->p.g);
+    if (stage == 0)
+        k_element<MODE_STAGE1, 128><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, S, wd_in, c->flux, R, avg, c->clk,
+                                                                       c->p.g);
+    else
+        k_element<MODE_STAGE2, 128><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, seg_U(c, j), wd_in, c->flux, R, avg,
+                                                                       c->clk, c->p.g);
+    k_node_bounds<<<blocks(c->nn, 256), 256, 0, s>>>(m, avg, bnd);
+    if (wd)
+        k_limit_to<true><<<blocks(c->ne, 128), 128, 0, s>>>(m, R, OUT, bnd, wd_in, wd_out, c->clk, c->p.H0,
+                                                            c->p.VELZERO, 2 * stage + 1);
+    else
+        k_limit_to<false><<<blocks(c->ne, 128), 128, 0, s>>>(m, R, OUT, bnd, wd_in, wd_out, c->clk, c->p.H0,
+                                                             c->p.VELZERO, 2 * stage + 1);
+    c->launches += 4;
+}
+
+/* reverse of one stage of step n (slot j): lamO is the adjoint of the stage output */
+static void reverse_stage(dgr_ctx *c, int j, int n, int stage)
+{
+    AdjointState *a = c->adj;
+    const MeshDev m = mesh_dev(c);
+    cudaStream_t s = c->stream;
+    const bool wd = c->p.wet_dry != 0;
+    const double *S = stage == 0 ? seg_U(c, j) : seg_W(c, j);
+    const int *wd_in = seg_wd(c, j, stage);
+    double *lamO = stage == 0 ? a->lamW : a->lamU;
+    double *lamS = stage == 0 ? a->lamU : a->lamW;
+    const double h0 = c->p.H0, vz = c->p.VELZERO, g = c->p.g;
+    if (wd)
+        k_adj_limit<true><<<blocks(c->ne, 128), 128, 0, s>>>(m, seg_R(c, j, stage), seg_B(c, j, stage), lamO, a->Rbar,
+                                                             a->bbar, a->zvb, h0, vz);
+    else
+        k_adj_limit<false><<<blocks(c->ne, 128), 128, 0, s>>>(m, seg_R(c, j, stage), seg_B(c, j, stage), lamO,
+                                                              a->Rbar, a->bbar, a->zvb, h0, vz);
+    k_adj_node<<<blocks(c->nn, 256), 256, 0, s>>>(m, seg_avg(c, j, stage), a->bbar, a->bnode, a->barg);
+    if (stage == 1)
+        k_adj_element<MODE_STAGE2><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, wd_in, a->Rbar, a->bnode, a->barg, lamS,
+                                                                      a->lamU, a->fbar, a->zvb, a->nbar, c->n_el, g,
+                                                                      a->dt_hist, n);
+    else
+        k_adj_element<MODE_STAGE1><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, wd_in, a->Rbar, a->bnode, a->barg, lamS,
+                                                                      a->lamU, a->fbar, a->zvb, a->nbar, c->n_el, g,
+                                                                      a->dt_hist, n);
+    if (wd)
+        k_adj_edge<true><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, a->fbar, lamS, a->zeb, g);
+    else
+        k_adj_edge<false><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, a->fbar, lamS, a->zeb, g);
+    c->launches += 4;
+}
+
+/* planar [9][ldE] -> the reference layout zeta/Qx/Qy[3*el+k] on the host */
+static int to_reference_layout(dgr_ctx *c, const double *planar, double *zeta, double *Qx, double *Qy)
+{
+    if (!zeta && !Qx && !Qy) return DGR_OK;
+    const size_t n3 = (size_t)3 * c->ne;
+    double *tmp = nullptr;
+    int r = dalloc(&tmp, 3 * n3);
+    if (r) return r;
+    k_planar_to_aos<<<blocks(c->ne, 256), 256, 0, c->stream>>>(c->ne, c->ldE, planar, tmp, tmp + n3, tmp + 2 * n3);
+    c->launches++;
+    std::vector<double> h(3 * n3);
+    cudaError_t e = cudaMemcpyAsync(h.data(), tmp, 3 * n3 * 8, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(tmp);
+    CK(e);
+    if (zeta) memcpy(zeta, h.data(), n3 * 8);
+    if (Qx) memcpy(Qx, h.data() + n3, n3 * 8);
+    if (Qy) memcpy(Qy, h.data() + 2 * n3, n3 * 8);
+    return DGR_OK;
+}
+
+extern "C" int dgr_adjoint_backward(dgr_ctx *c, double *grad_n_el, double *grad_z, double *grad_zeta0,
+                                    double *grad_Qx0, double *grad_Qy0)
+{
+    if (!c || !c->adj || !c->adj->have_forward) return DGR_ERR_INVALID;
+    AdjointState *a = c->adj;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    const MeshDev m = mesh_dev(c);
+    const size_t E9 = plane9(c);
+    CK(cudaEventRecord(c->ev0, s));
+    CK(cudaMemsetAsync(a->lamU, 0, E9 * 8, s));
+    CK(cudaMemsetAsync(a->zvb, 0, (size_t)3 * c->ldE * 8, s));
+    CK(cudaMemsetAsync(a->zeb, 0, (size_t)c->ldF * 8, s));
+    CK(cudaMemsetAsync(a->nbar, 0, (size_t)c->ldE * 8, s));
+    for (int sg = a->nseg - 1; sg >= 0; --sg) {
+        const int n0 = sg * a->K, len = std::min(a->K, a->nsteps - n0);
+        /* 1. recompute the segment, recording */
+        CK(cudaMemcpyAsync(seg_U(c, 0), a->ckU + sg * E9, E9 * 8, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(seg_wd(c, 0, 0), a->ckWd + (size_t)sg * c->ne, (size_t)c->ne * 4,
+                           cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(c->clk, a->ckClk + sg, sizeof(DevClock), cudaMemcpyDeviceToDevice, s));
+        for (int j = 0; j < len; ++j) {
+            clock_begin_step(c, n0 + j, 1);
+            recorded_stage(c, j, 0, seg_U(c, j), seg_W(c, j), seg_wd(c, j, 0), seg_wd(c, j, 1));
+            const bool last = j + 1 == len;
+            recorded_stage(c, j, 1, seg_W(c, j), last ? c->U : seg_U(c, j + 1), seg_wd(c, j, 1),
+                           last ? c->wdA : seg_wd(c, j + 1, 0));
+            k_clock_end<<<1, 32, 0, s>>>(c->clk, 1);
+            c->launches += 2;
+        }
+        /* 2. reverse the segment */
+        for (int j = len - 1; j >= 0; --j) {
+            const int n = n0 + j;
+            if (c->nbnd)
+                k_adj_forcing<<<blocks(c->nbnd, 256), 256, 0, s>>>(c->clk, a->time_hist, n, c->bnd_edges, c->bnd_type,
+                                                                   c->nbnd, c->bzeta, c->bqn);
+            k_misfit_rev<<<1, 32, 0, s>>>(a->lamU, c->ldE, a->ng, a->g_el, a->g_w, a->resid + (size_t)n * a->ng);
+            c->launches += 2;
+            reverse_stage(c, j, n, 1);
+            reverse_stage(c, j, n, 0);
+        }
+    }
+    k_adj_zfold<<<blocks(c->ne, 256), 256, 0, s>>>(m, a->zeb, a->zvb);
+    k_adj_znode<<<blocks(c->nn, 256), 256, 0, s>>>(m, a->zvb, a->zbar);
+    c->launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev1, s));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    a->bwd_ms = ms;
+    int r = read_clock(c);
+    if (r) return r;
+    r = first_error(c);
+    if (r) return r;
+    if (grad_n_el) CK(cudaMemcpy(grad_n_el, a->nbar, (size_t)c->ne * 8, cudaMemcpyDeviceToHost));
+    if (grad_z) CK(cudaMemcpy(grad_z, a->zbar, (size_t)c->nn * 8, cudaMemcpyDeviceToHost));
+    r = to_reference_layout(c, a->lamU, grad_zeta0, grad_Qx0, grad_Qy0);
+    if (r) return r;
+    c->wd_fresh = 0; /* the context state is the last recomputed one */
+    return DGR_OK;
+}
+
+/* ---------------------------------------------------------------------- TLM ---- */
+
+static int ensure_tlm(dgr_ctx *c)
+{
+    AdjointState *a = c->adj;
+    if (a->Ud) return DGR_OK;
+    const size_t E = c->ldE, F = c->ldF, N = c->ldN;
+    int r = 0;
+    if ((r = dalloc(&a->Ud, 9 * E)) || (r = dalloc(&a->Wd, 9 * E)) || (r = dalloc(&a->flux_d, 6 * F)) ||
+        (r = dalloc(&a->avg_d, 3 * E)) || (r = dalloc(&a->bounds_d, 6 * N)) || (r = dalloc(&a->zd, (size_t)c->nn)) ||
+        (r = dalloc(&a->neld, (size_t)c->ne)))
+        return r;
+    return DGR_OK;
+}
+
+extern "C" int dgr_tlm(dgr_ctx *c, const double *zeta, const double *Qx, const double *Qy, const int *WD,
+                       const double *dzeta0, const double *dQx0, const double *dQy0, const double *dn_el,
+                       const double *dz, double *J, double *dJ)
+{
+    if (!c || !c->adj || !c->adj->have_forward || !zeta || !Qx || !Qy || !WD) return DGR_ERR_INVALID;
+    AdjointState *a = c->adj;
+    CK(cudaSetDevice(c->device));
+    int r = ensure_tlm(c);
+    if (r) return r;
+    r = dgr_upload_state(c, zeta, Qx, Qy, WD);
+    if (r) return r;
+    cudaStream_t s = c->stream;
+    const MeshDev m = mesh_dev(c);
+    const size_t ne = c->ne, E9 = plane9(c);
+    /* tangent of the initial state (reference layout [3*el+k] -> planar) */
+    CK(cudaMemsetAsync(a->Ud, 0, E9 * 8, s));
+    if (dzeta0 || dQx0 || dQy0) {
+        const size_t n3 = 3 * ne;
+        std::vector<double> h(3 * n3, 0.0);
+        if (dzeta0) memcpy(h.data(), dzeta0, n3 * 8);
+        if (dQx0) memcpy(h.data() + n3, dQx0, n3 * 8);
+        if (dQy0) memcpy(h.data() + 2 * n3, dQy0, n3 * 8);
+        double *tmp = nullptr;
+        r = dalloc(&tmp, 3 * n3);
+        if (r) return r;
+        cudaError_t e = cudaMemcpyAsync(tmp, h.data(), 3 * n3 * 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) {
+            k_aos_to_planar<<<blocks(c->ne, 256), 256, 0, s>>>(c->ne, c->ldE, tmp, tmp + n3, tmp + 2 * n3, a->Ud);
+            e = cudaStreamSynchronize(s);
+        }
+        cudaFree(tmp);
+        CK(e);
+    }
+    if (dz)
+        CK(cudaMemcpyAsync(a->zd, dz, (size_t)c->nn * 8, cudaMemcpyHostToDevice, s));
+    else
+        CK(cudaMemsetAsync(a->zd, 0, (size_t)c->nn * 8, s));
+    if (dn_el)
+        CK(cudaMemcpyAsync(a->neld, dn_el, ne * 8, cudaMemcpyHostToDevice, s));
+    else
+        CK(cudaMemsetAsync(a->neld, 0, ne * 8, s));
+    CK(cudaMemsetAsync(a->flux_d, 0, (size_t)6 * c->ldF * 8, s));
+
+    const bool wd = c->p.wet_dry != 0;
+    const double g = c->p.g, h0 = c->p.H0, vz = c->p.VELZERO;
+    CK(cudaEventRecord(c->ev0, s));
+    launch_wd_refresh(c);
+    for (int n = 0; n < a->nsteps; ++n) {
+        if (c->nbnd)
+            k_adj_forcing<<<blocks(c->nbnd, 256), 256, 0, s>>>(c->clk, a->time_hist, n, c->bnd_edges, c->bnd_type,
+                                                               c->nbnd, c->bzeta, c->bqn);
+        for (int stage = 0; stage < 2; ++stage) {
+            double *S = stage == 0 ? c->U : c->W, *Sd = stage == 0 ? a->Ud : a->Wd;
+            double *OUT = stage == 0 ? c->W : c->U, *OUTd = stage == 0 ? a->Wd : a->Ud;
+            const int *wd_in = (stage == 0 || !wd) ? c->wdA : c->wdB;
+            int *wd_out = stage == 0 ? c->wdB : c->wdA;
+            if (wd)
+                k_tlm_edge<true><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, Sd, wd_in, c->bzeta, c->bqn, a->zd, c->flux,
+                                                                    a->flux_d, g);
+            else
+                k_tlm_edge<false><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, Sd, wd_in, c->bzeta, c->bqn, a->zd,
+                                                                     c->flux, a->flux_d, g);
+            if (stage == 0)
+                k_tlm_element<MODE_STAGE1><<<blocks(c->ne, 128), 128, 0, s>>>(
+                    m, S, Sd, c->U, a->Ud, wd_in, c->flux, a->flux_d, a->zd, c->n_el, a->neld, OUT, OUTd, c->avg,
+                    a->avg_d, c->clk, g, a->dt_hist, n);
+            else
+                k_tlm_element<MODE_STAGE2><<<blocks(c->ne, 128), 128, 0, s>>>(
+                    m, S, Sd, c->U, a->Ud, wd_in, c->flux, a->flux_d, a->zd, c->n_el, a->neld, OUT, OUTd, c->avg,
+                    a->avg_d, c->clk, g, a->dt_hist, n);
+            k_tlm_node<<<blocks(c->nn, 256), 256, 0, s>>>(m, c->avg, a->avg_d, c->bounds, a->bounds_d);
+            if (wd)
+                k_tlm_limit<true><<<blocks(c->ne, 128), 128, 0, s>>>(m, OUT, OUTd, c->bounds, a->bounds_d, a->zd,
+                                                                     wd_in, wd_out, h0, vz);
+            else
+                k_tlm_limit<false><<<blocks(c->ne, 128), 128, 0, s>>>(m, OUT, OUTd, c->bounds, a->bounds_d, a->zd,
+                                                                      wd_in, wd_out, h0, vz);
+        }
+        /* residuals and their tangents (the tangent of a gauge value is the same functional
+         * of the state tangent; its target is 0) */
+        k_misfit<<<1, 32, 0, s>>>(c->U, c->ldE, a->ng, a->g_el, a->g_w, a->target + (size_t)n * a->ng,
+                                  a->rt + (size_t)n * a->ng);
+        k_misfit<<<1, 32, 0, s>>>(a->Ud, c->ldE, a->ng, a->g_el, a->g_w, nullptr, a->rd + (size_t)n * a->ng);
+        c->launches += 11;
+    }
+    k_misfit_sum<<<1, 32, 0, s>>>(a->rt, a->rd, (long long)a->nsteps * a->ng, a->sums);
+    c->launches++;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev1, s));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    a->tlm_ms = ms;
+    double sums[2];
+    CK(cudaMemcpy(sums, a->sums, 16, cudaMemcpyDeviceToHost));
+    if (J) *J = sums[0];
+    if (dJ) *dJ = sums[1];
+    if (c->p.wet_dry) {
+        c->wd_fresh = 1;
+        c->wd_cur_is_B = 1;
+    }
+    return DGR_OK;
+}
+
+extern "C" int dgr_adjoint_timing(const dgr_ctx *c, double *forward_ms, double *backward_ms, double *tlm_ms)
+{
+    if (!c || !c->adj) return DGR_ERR_INVALID;
+    if (forward_ms) *forward_ms = c->adj->fwd_ms;
+    if (backward_ms) *backward_ms = c->adj->bwd_ms;
+    if (tlm_ms) *tlm_ms = c->adj->tlm_ms;
+    return DGR_OK;
+}

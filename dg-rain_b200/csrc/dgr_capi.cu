@@ -61,15 +61,7 @@ extern "C" int dgr_params_default(dgr_params *p)
     return DGR_OK;
 }
 
-template <class T>
-static int dalloc(T **p, size_t n)
-{
-    *p = nullptr;
-    CK(cudaMalloc((void **)p, (n ? n : 1) * sizeof(T)));
-    return DGR_OK;
-}
-
-static void drop_graph(dgr_ctx *c)
+void drop_graph(dgr_ctx *c)
 {
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
@@ -87,6 +79,7 @@ static void release(dgr_ctx *c)
                     c->bqn, c->bstage, c->wdA, c->wdB, c->dec, c->bar, c->clk};
     for (void *q : ptrs)
         if (q) cudaFree(q);
+    adjoint_release(c);
     if (c->h_clk) cudaFreeHost(c->h_clk);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -95,7 +88,7 @@ static void release(dgr_ctx *c)
     delete c;
 }
 
-static int upload_geometry(dgr_ctx *c)
+int upload_geometry(dgr_ctx *c)
 {
     k_element_setup<<<blocks(c->ne, 128), 128, 0, c->stream>>>(c->ne, c->ldE, c->el2v_aos, c->x, c->y, c->zn,
                                                                c->nfric, c->n_el, c->p.g, c->el2v, c->geo);
@@ -431,14 +424,14 @@ extern "C" int dgr_get_params(const dgr_ctx *c, dgr_params *out)
     return DGR_OK;
 }
 
-static int read_clock(dgr_ctx *c)
+int read_clock(dgr_ctx *c)
 {
     CK(cudaMemcpyAsync(c->h_clk, c->clk, sizeof(DevClock) * c->nscen, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return DGR_OK;
 }
 
-static int write_clock(dgr_ctx *c)
+int write_clock(dgr_ctx *c)
 {
     CK(cudaMemcpyAsync(c->clk, c->h_clk, sizeof(DevClock) * c->nscen, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -668,7 +661,7 @@ static void launch_edge(dgr_ctx *c, const double *S, const int *wd, int lam_slot
 }
 
 /* one RK stage as four kernels; stage 0 reads U writes W, stage 1 reads W and U writes U */
-static void launch_stage(dgr_ctx *c, int stage, bool count)
+void launch_stage(dgr_ctx *c, int stage, bool count)
 {
     const bool wd = c->p.wet_dry != 0;
     const double *S = stage == 0 ? c->U : c->W;
@@ -690,7 +683,7 @@ static void launch_stage(dgr_ctx *c, int stage, bool count)
     if (count) c->launches += 4;
 }
 
-static void launch_wd_refresh(dgr_ctx *c)
+void launch_wd_refresh(dgr_ctx *c)
 {
     if (c->p.wet_dry && !c->wd_fresh) {
         /* the flags the caller sees (WA after an upload, WB after a step) seed the status */
@@ -792,7 +785,7 @@ static cudaError_t launch_step(dgr_ctx *c)
 
 static int kernels_per_step(const dgr_ctx *c) { return c->fusion == 2 ? 1 : (c->fusion == 1 ? 4 : 10); }
 
-static int decode_err(unsigned long long key, int *code, int *index, int *step)
+int decode_err(unsigned long long key, int *code, int *index, int *step)
 {
     if (key == ~0ull) {
         if (code) *code = 0;
@@ -807,7 +800,7 @@ static int decode_err(unsigned long long key, int *code, int *index, int *step)
     return cd;
 }
 
-static int first_error(const dgr_ctx *c)
+int first_error(const dgr_ctx *c)
 {
     for (int k = 0; k < c->nscen; ++k) {
         const int cd = decode_err(c->h_clk[k].err, nullptr, nullptr, nullptr);

@@ -10,29 +10,47 @@
  */
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 
+#ifndef __CUDACC__
+/* plain C++ compilers (the host test harness of the derivative cores): the library's
+ * overloads in the global namespace, as CUDA provides them */
+using std::isnan;
+#endif
+
 #define DGR_DEV __device__ __forceinline__
+/* arithmetic shared by the kernels and by the host-compiled test harness of the
+ * differentiation cores */
+#define DGR_HD __host__ __device__ __forceinline__
 
 namespace dgr {
 
 /* sign() of 2DCode/mathfunctions.c:4-12 */
-DGR_DEV int sgn(double a)
+template <class T>
+DGR_HD int sgn(const T &a)
 {
     if (a < 0) return -1;
     if (a == 0) return 0;
     return 1;
 }
 /* max()/min() macros of 2DCode/mathfunctions.h:8-14 (not fmax/fmin: NaN order matters) */
-DGR_DEV double rmax(double a, double b) { return (a > b) ? a : b; }
-DGR_DEV double rmin(double a, double b) { return (a < b) ? a : b; }
+template <class T>
+DGR_HD T rmax(const T &a, const T &b) { return (a > b) ? a : b; }
+template <class T>
+DGR_HD T rmin(const T &a, const T &b) { return (a < b) ? a : b; }
+
+/* Which operand fmax(a, b) passes on, for derivatives: b when b > a or a is NaN.  At a
+ * tie the values agree and a is taken. */
+DGR_HD bool fmax_takes_b(double a, double b) { return (b > a) || isnan(a); }
 
 /* Dense 3x3 times vector, summed from +0 in column order (2DCode/mathfunctions.c:24-35). */
-DGR_DEV void matvec3(const double m[3][3], const double v[3], double out[3])
+template <class T>
+DGR_HD void matvec3(const T m[3][3], const T v[3], T out[3])
 {
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        double s = 0;
+        T s = 0;
 #pragma unroll
         for (int j = 0; j < 3; ++j) s += m[i][j] * v[j];
         out[i] = s;
@@ -41,67 +59,65 @@ DGR_DEV void matvec3(const double m[3][3], const double v[3], double out[3])
 
 /* Roe flux with entropy fix, 2DCode/numericalFlux2D.c:6-108.  Returns max |lambda| of the
  * two traces.  local_g scales the pressure term only; g sets the eigen-structure. */
-DGR_DEV double roe_flux(double fh[3], double zeta_in, double zeta_ex, double qx_in, double qx_ex,
-                        double qy_in, double qy_ex, double z_edge, double nx, double ny,
-                        double local_g, double g)
+template <class T>
+DGR_HD T roe_flux(T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy_ex, T z_edge, double nx,
+                  double ny, double local_g, double g)
 {
-    const double h_in = zeta_in + z_edge;
-    const double h_ex = zeta_ex + z_edge;
-    const double u_in = qx_in / h_in, u_ex = qx_ex / h_ex;
-    const double v_in = qy_in / h_in, v_ex = qy_ex / h_ex;
-    const double jump[3] = {zeta_in - zeta_ex, qx_in - qx_ex, qy_in - qy_ex};
+    const T h_in = zeta_in + z_edge;
+    const T h_ex = zeta_ex + z_edge;
+    const T u_in = qx_in / h_in, u_ex = qx_ex / h_ex;
+    const T v_in = qy_in / h_in, v_ex = qy_ex / h_ex;
+    const T jump[3] = {zeta_in - zeta_ex, qx_in - qx_ex, qy_in - qy_ex};
 
-    const double p_in = 0.5 * local_g * (h_in * h_in - z_edge * z_edge);
-    const double p_ex = 0.5 * local_g * (h_ex * h_ex - z_edge * z_edge);
-    const double huv_in = h_in * u_in * v_in, huv_ex = h_ex * u_ex * v_ex;
-    const double fn_in[3] = {h_in * u_in * nx + h_in * v_in * ny,
-                             (h_in * u_in * u_in + p_in) * nx + huv_in * ny,
-                             huv_in * nx + (h_in * v_in * v_in + p_in) * ny};
-    const double fn_ex[3] = {h_ex * u_ex * nx + h_ex * v_ex * ny,
-                             (h_ex * u_ex * u_ex + p_ex) * nx + huv_ex * ny,
-                             huv_ex * nx + (h_ex * v_ex * v_ex + p_ex) * ny};
+    const T p_in = 0.5 * local_g * (h_in * h_in - z_edge * z_edge);
+    const T p_ex = 0.5 * local_g * (h_ex * h_ex - z_edge * z_edge);
+    const T huv_in = h_in * u_in * v_in, huv_ex = h_ex * u_ex * v_ex;
+    const T fn_in[3] = {h_in * u_in * nx + h_in * v_in * ny, (h_in * u_in * u_in + p_in) * nx + huv_in * ny,
+                        huv_in * nx + (h_in * v_in * v_in + p_in) * ny};
+    const T fn_ex[3] = {h_ex * u_ex * nx + h_ex * v_ex * ny, (h_ex * u_ex * u_ex + p_ex) * nx + huv_ex * ny,
+                        huv_ex * nx + (h_ex * v_ex * v_ex + p_ex) * ny};
 
-    const double s_in = sqrt(h_in), s_ex = sqrt(h_ex);
-    const double h_hat = 0.5 * (h_in + h_ex);
-    const double u_hat = (u_in * s_in + u_ex * s_ex) / (s_in + s_ex);
-    const double v_hat = (v_in * s_in + v_ex * s_ex) / (s_in + s_ex);
-    const double c = sqrt(g * h_hat);
+    const T s_in = sqrt(h_in), s_ex = sqrt(h_ex);
+    const T h_hat = 0.5 * (h_in + h_ex);
+    const T u_hat = (u_in * s_in + u_ex * s_ex) / (s_in + s_ex);
+    const T v_hat = (v_in * s_in + v_ex * s_ex) / (s_in + s_ex);
+    const T c = sqrt(g * h_hat);
 
-    const double r[3][3] = {{1, 0, 1}, {u_hat - c * nx, -ny, u_hat + c * nx}, {v_hat - c * ny, nx, v_hat + c * ny}};
-    const double den = -2 * c;
+    const T r[3][3] = {{1, 0, 1}, {u_hat - c * nx, -ny, u_hat + c * nx}, {v_hat - c * ny, nx, v_hat + c * ny}};
+    const T den = -2 * c;
     /* (-nx)/den is exactly -(nx/den): IEEE division is symmetric in sign, so the third
      * row reuses the first row's quotients. */
-    const double nx_den = nx / den, ny_den = ny / den;
-    const double ri[3][3] = {{(-c - nx * u_hat - ny * v_hat) / den, nx_den, ny_den},
-                             {(-2 * c * ny * u_hat + 2 * c * nx * v_hat) / den, 2 * c * ny / den, -2 * c * nx / den},
-                             {(-c + nx * u_hat + ny * v_hat) / den, -nx_den, -ny_den}};
+    const T nx_den = nx / den, ny_den = ny / den;
+    const T ri[3][3] = {{(-c - nx * u_hat - ny * v_hat) / den, nx_den, ny_den},
+                        {(-2 * c * ny * u_hat + 2 * c * nx * v_hat) / den, 2 * c * ny / den, -2 * c * nx / den},
+                        {(-c + nx * u_hat + ny * v_hat) / den, -nx_den, -ny_den}};
 
-    const double un_in = u_in * nx + v_in * ny, un_ex = u_ex * nx + v_ex * ny;
-    const double c_in = sqrt(g * h_in), c_ex = sqrt(g * h_ex);
-    const double l1_in = un_in - c_in, l2_in = un_in, l3_in = un_in + c_in;
-    const double l1_ex = un_ex - c_ex, l2_ex = un_ex, l3_ex = un_ex + c_ex;
-    const double un_hat = u_hat * nx + v_hat * ny;
-    double lh1 = un_hat - c, lh2 = un_hat, lh3 = un_hat + c;
+    const T un_in = u_in * nx + v_in * ny, un_ex = u_ex * nx + v_ex * ny;
+    const T c_in = sqrt(g * h_in), c_ex = sqrt(g * h_ex);
+    const T l1_in = un_in - c_in, l2_in = un_in, l3_in = un_in + c_in;
+    const T l1_ex = un_ex - c_ex, l2_ex = un_ex, l3_ex = un_ex + c_ex;
+    const T un_hat = u_hat * nx + v_hat * ny;
+    T lh1 = un_hat - c, lh2 = un_hat, lh3 = un_hat + c;
 
-    double e1 = fmax(0.0, (lh1 - l1_in));
+    T e1 = fmax(0.0, (lh1 - l1_in));
     e1 = fmax(e1, (l1_ex - lh1));
     lh1 = fmax(e1, fabs(lh1));
-    double e2 = fmax(0.0, (lh2 - l2_in));
+    T e2 = fmax(0.0, (lh2 - l2_in));
     e2 = fmax(e2, (l2_ex - lh2));
     lh2 = fmax(e2, fabs(lh2));
-    double e3 = fmax(0.0, (lh3 - l3_in));
+    T e3 = fmax(0.0, (lh3 - l3_in));
     e3 = fmax(e3, (l3_ex - lh3));
     lh3 = fmax(e3, fabs(lh3));
 
-    const double lam[3][3] = {{lh1, 0, 0}, {0, lh2, 0}, {0, 0, lh3}};
-    double p1[3], p2[3], p3[3];
+    const T lam[3][3] = {{lh1, 0, 0}, {0, lh2, 0}, {0, 0, lh3}};
+    T p1[3], p2[3], p3[3];
     matvec3(ri, jump, p1);
     matvec3(lam, p1, p2);
     matvec3(r, p2, p3);
 #pragma unroll
     for (int k = 0; k < 3; ++k) fh[k] = 0.5 * (fn_in[k] + fn_ex[k]) + 0.5 * p3[k];
 
-    double m = rmax(fabs(l1_in), fabs(l1_ex));
+    T m = rmax(fabs(l1_in), fabs(l1_ex));
     m = rmax(m, fabs(l2_in));
     m = rmax(m, fabs(l2_ex));
     m = rmax(m, fabs(l3_in));
@@ -128,18 +144,27 @@ DGR_DEV double roe_flux(double fh[3], double zeta_in, double zeta_ex, double qx_
  * Zero, negative, non-finite and extreme arguments go to pow(), whose special-case
  * results are the C standard's on both sides.
  */
-DGR_DEV double pow43(double x)
+DGR_HD double fma_exact(double a, double b, double c)
+{
+#ifdef __CUDA_ARCH__
+    return __fma_rn(a, b, c);
+#else
+    return fma(a, b, c);
+#endif
+}
+
+DGR_HD double pow43(double x)
 {
     if (!(x >= 1e-200 && x <= 1e200)) return pow(x, 4. / 3);
     const double c0 = cbrt(x);
     const double a_h = c0 * c0;
-    const double a_l = __fma_rn(c0, c0, -a_h);
+    const double a_l = fma_exact(c0, c0, -a_h);
     const double b_h = a_h * c0;
-    const double b_l = __fma_rn(a_h, c0, -b_h);
+    const double b_l = fma_exact(a_h, c0, -b_h);
     const double r = ((b_h - x) + b_l) + a_l * c0; /* c0^3 - x */
     const double d = r / (3.0 * a_h);
     const double p_h = x * c0;
-    const double p_l = __fma_rn(x, c0, -p_h);
+    const double p_l = fma_exact(x, c0, -p_h);
     const double eta = log(x) * -7.401486830834377e-17;
     const double lo = (p_l - x * d) + p_h * eta;
     return p_h + lo;
@@ -148,7 +173,8 @@ DGR_DEV double pow43(double x)
 /* x / d for the limiter's redistribution count d in {1, 2, 3} (as a double).  Division
  * by 1 and by 2 are exact (x and x*0.5 are the correctly rounded x/d); only d = 3 needs
  * the full IEEE division. */
-DGR_DEV double div_by_count(double x, double d)
+template <class T>
+DGR_HD T div_by_count(const T &x, double d)
 {
     if (d == 1.0) return x;
     if (d == 2.0) return x * 0.5;
@@ -157,9 +183,9 @@ DGR_DEV double div_by_count(double x, double d)
 
 /* RT0 fit F = (a + b x, c + b y) through three normal-flux values (Cramer's rule of
  * 2DCode/2DInnerProducts.c:134-146 and :507-519). */
-DGR_DEV void rt0_fit(double R1, double R2, double R3, double M11, double M12, double M13, double M21,
-                     double M22, double M23, double M31, double M32, double M33, double dM, double &a,
-                     double &b, double &c)
+template <class T>
+DGR_HD void rt0_fit(const T &R1, const T &R2, const T &R3, double M11, double M12, double M13, double M21,
+                    double M22, double M23, double M31, double M32, double M33, double dM, T &a, T &b, T &c)
 {
     a = (R3 * M13 * M22 - R3 * M12 * M23 - R2 * M13 * M32 + R1 * M23 * M32 + R2 * M12 * M33 - R1 * M22 * M33) / dM;
     b = -(R3 * M13 * M21 - R3 * M11 * M23 - R2 * M13 * M31 + R1 * M23 * M31 + R2 * M11 * M33 - R1 * M21 * M33) / dM;
@@ -168,7 +194,7 @@ DGR_DEV void rt0_fit(double R1, double R2, double R3, double M11, double M12, do
 
 /* Status key: earlier step, then earlier phase, then lower index wins under atomicMin,
  * which is the failure the sequential reference would have stopped at. */
-DGR_DEV unsigned long long err_key(int step, int phase, int code, int index)
+DGR_HD unsigned long long err_key(int step, int phase, int code, int index)
 {
     return ((unsigned long long)(unsigned)step << 40) | ((unsigned long long)(phase & 15) << 36) |
            ((unsigned long long)(code & 15) << 32) | (unsigned long long)(unsigned)index;

@@ -42,6 +42,14 @@ static inline double bits_to_double(unsigned long long b)
 
 static inline unsigned blocks(int n, int t) { return (unsigned)((n + t - 1) / t); }
 
+template <class T>
+static inline int dalloc(T **p, size_t n)
+{
+    *p = nullptr;
+    CK(cudaMalloc((void **)p, (n ? n : 1) * sizeof(T)));
+    return DGR_OK;
+}
+
 struct dgr_ctx {
     dgr_params p;
     int device;
@@ -113,3 +121,16 @@ static inline dgr::PhysParams phys(const dgr_ctx *c)
     return q;
 }
 
+
+/* dgr_capi.cu */
+void drop_graph(dgr_ctx *c);
+int upload_geometry(dgr_ctx *c);                 /* element geometry planes from x, y, zn, n */
+int read_clock(dgr_ctx *c);                      /* device clocks -> h_clk (synchronises) */
+int write_clock(dgr_ctx *c);                     /* h_clk -> device clocks (synchronises) */
+void launch_stage(dgr_ctx *c, int stage, bool count); /* one RK stage, four kernels */
+void launch_wd_refresh(dgr_ctx *c);              /* status for the next step when stale */
+int decode_err(unsigned long long key, int *code, int *index, int *step);
+int first_error(const dgr_ctx *c);               /* first scenario failure code in h_clk */
+
+/* dgr_adjoint.cu */
+void adjoint_release(dgr_ctx *c);

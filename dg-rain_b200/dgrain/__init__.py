@@ -6,8 +6,10 @@ from ._lib import DgrError, load
 from .mesh import (Mesh, build_connectivity, initial_state, read_fort14, rectangle,
                    rectangle_with_elements, write_fort14)
 from .solver import Ensemble, Solver, StepError, default_params
+from .adjoint import GaugeMisfit, cr_weights, gauge_misfit, intertidal_points, place_gauges
 
 __all__ = [
     "_lib", "DgrError", "load", "Mesh", "build_connectivity", "initial_state", "read_fort14",
     "rectangle", "rectangle_with_elements", "write_fort14", "Ensemble", "Solver", "StepError", "default_params",
+    "GaugeMisfit", "cr_weights", "gauge_misfit", "intertidal_points", "place_gauges",
 ]

@@ -141,6 +141,15 @@ SIGNATURES = [
     ("dgr_autotune", C.c_int, [C.c_void_p, C.c_int, iptr, iptr, dptr]),
     ("dgr_slope_limiter_noalloc", C.c_int,
      [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
+    ("dgr_adjoint_setup", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, iptr, dptr, dptr]),
+    ("dgr_adjoint_set_target", C.c_int, [C.c_void_p, dptr]),
+    ("dgr_adjoint_forward", C.c_int,
+     [C.c_void_p, dptr, dptr, dptr, iptr, C.c_double, C.c_double, C.c_int, dptr, dptr]),
+    ("dgr_adjoint_backward", C.c_int, [C.c_void_p, dptr, dptr, dptr, dptr, dptr]),
+    ("dgr_tlm", C.c_int, [C.c_void_p, dptr, dptr, dptr, iptr, dptr, dptr, dptr, dptr, dptr, dptr, dptr]),
+    ("dgr_adjoint_dt", C.c_int, [C.c_void_p, dptr, dptr]),
+    ("dgr_adjoint_timing", C.c_int, [C.c_void_p, dptr, dptr, dptr]),
+    ("dgr_set_bathymetry", C.c_int, [C.c_void_p, dptr]),
 ]
 
 _lib = None

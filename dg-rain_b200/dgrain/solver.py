@@ -77,6 +77,13 @@ class Solver:
         assert n_el.shape == (self.ne,)
         _lib.check(self.lib.dgr_set_element_manning(self.ctx, _dp(n_el)), "dgr_set_element_manning")
 
+    def set_bathymetry(self, z: np.ndarray) -> None:
+        """Node depths (the fort.14 depth column); every depth-dependent factor is
+        recomputed on the device."""
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        assert z.shape == (self.mesh.num_nodes,)
+        _lib.check(self.lib.dgr_set_bathymetry(self.ctx, _dp(z)), "dgr_set_bathymetry")
+
     # ----------------------------------------------------------------- state ----
     def upload_state(self, zeta, qx, qy, wd=None) -> None:
         z = np.ascontiguousarray(zeta, dtype=np.float64)

@@ -270,6 +270,47 @@ DGR_API int dgr_profile_step(dgr_ctx *ctx, int nsteps, double *kernel_ms, int n)
 DGR_API int dgr_slope_limiter_noalloc(int num_el, int num_nodes, const int *d_EltoVert, const double *d_z,
                                       double *d_zeta, double *d_Qx, double *d_Qy, double H0, void *stream);
 
+/* ---- discrete adjoint and tangent-linear model (single mesh) ----------------------
+ * Extension: the reference has no derivatives.  Objective over a run of nsteps steps:
+ *   J = sum_n sum_g (zeta_g(u^{n+1}) - target[n*ngauges + g])^2,
+ *   zeta_g(u) = w[3g] zeta_0 + w[3g+1] zeta_1 + w[3g+2] zeta_2 of element gauge_el[g]
+ * (midpoint values; the Crouzeix-Raviart interpolation at a point is such a functional).
+ * Derivatives are those of the discrete scheme with every decision (wet/dry flags,
+ * limiter clamps and redistribution, PDop branches, entropy-fix selections, node max/min
+ * elements) and the CFL dt sequence frozen at the recorded forward run.  Parameters: the
+ * per-element Manning n (dgr_set_element_manning; required for its gradient), the node
+ * depth z (dgr_set_bathymetry) and the initial state. */
+
+/* Allocates the adjoint storage: a checkpoint every ckpt_every steps plus a recompute
+ * store of ckpt_every steps (about 390 B per element and step); target may be NULL (0). */
+DGR_API int dgr_adjoint_setup(dgr_ctx *ctx, int nsteps, int ckpt_every, int ngauges, const int *gauge_el,
+                              const double *gauge_w, const double *target);
+DGR_API int dgr_adjoint_set_target(dgr_ctx *ctx, const double *target);
+/* Forward run from the given state (reference layout; time < 0 starts at t = 0 with dt0)
+ * with checkpoints; its steps are dgr_run's bit for bit.  replay_dt = 1 reuses the dt
+ * sequence of the previous forward run instead of the CFL dt (finite differences with
+ * frozen dt).  J and the gauge values [nsteps*ngauges] (NULL to skip) on return. */
+DGR_API int dgr_adjoint_forward(dgr_ctx *ctx, const double *zeta, const double *Qx, const double *Qy,
+                                const int *WD, double time, double dt, int replay_dt, double *J,
+                                double *gauge_values);
+/* Gradient of J of the last forward run: per-element n [num_el], node depth [num_nodes],
+ * initial state (reference layout); any output may be NULL.  The context's state is
+ * unspecified afterwards. */
+DGR_API int dgr_adjoint_backward(dgr_ctx *ctx, double *grad_n_el, double *grad_z, double *grad_zeta0,
+                                 double *grad_Qx0, double *grad_Qy0);
+/* Tangent-linear run over the recorded dt sequence: J and dJ = J'(p) . (dn_el, dz, d state)
+ * for the given directions (any may be NULL = 0). */
+DGR_API int dgr_tlm(dgr_ctx *ctx, const double *zeta, const double *Qx, const double *Qy, const int *WD,
+                    const double *dzeta0, const double *dQx0, const double *dQy0, const double *dn_el,
+                    const double *dz, double *J, double *dJ);
+/* dt and boundary-value time of every step of the last forward run [nsteps]. */
+DGR_API int dgr_adjoint_dt(dgr_ctx *ctx, double *dt, double *time);
+/* Device time in ms of the last forward, backward and tangent-linear runs. */
+DGR_API int dgr_adjoint_timing(const dgr_ctx *ctx, double *forward_ms, double *backward_ms, double *tlm_ms);
+/* Node depths z [num_nodes] (the fort.14 depth column): recomputes every depth-dependent
+ * factor on the device. */
+DGR_API int dgr_set_bathymetry(dgr_ctx *ctx, const double *z);
+
 /* Diagnostic: y[i] = x[i]^(4./3) as the kernels evaluate the Manning term of
  * 2DCode/2DInnerProducts.c:318 (correctly rounded; see dgr_device.cuh). */
 DGR_API int dgr_pow43_batch(const double *x, double *y, int n, int device);
