@@ -40,6 +40,8 @@ NX, NY, JITTER, CFL, AMP, PERIOD = 2000, 1000, 0.1, 0.3, 0.5, 44712.0
 LAND_FILM = 0.5e-3      # dry land holds H0/2: with exactly H0 the reference wet/dry step stops on a NaN flux
 ALG_BYTES = 216         # algorithmic bytes per element-stage (state in, step input, state out)
 METRIC = "element-stage updates/s"
+ADJ_CFL = 0.1           # the reference's own CFL (2DCode/time_evolution.c:399) for the 4,000-step adjoint run:
+                        # at 0.3 the rising tide takes the reference wet/dry scheme to a NaN flux at step 2,610
 
 
 def log(*a):
@@ -250,6 +252,78 @@ def ensemble_bench(nscen: int, steps: int, warmup: int, device: int = 0):
                         "tide 0.2-1.5 m, rain 0-100 mm/h, Manning 0.02-0.06, per-scenario CFL dt"}
 
 
+def adjoint_bench(steps: int, ckpt: int, fd_dirs: int, device: int = 0, nx: int = 447, ny: int = 224):
+    """Gradient of a gauge misfit by the discrete adjoint: the 200k-triangle coastal
+    rectangle (447 x 224 cells, jitter 0.1, seed 3, wet/dry on, tide 0.5 m, land film H0/2),
+    `steps` steps with a checkpoint every `ckpt`, 32 gauges at random points of the
+    intertidal band (bed elevation within +-0.5 m), target = the same run with Manning n
+    (0.03) perturbed by +-20 % log-normal noise per element.  Times the recorded forward run,
+    the backward sweep (recomputation included) and the plain device loop over the same
+    steps; checks the adjoint against the tangent-linear model on random directions in n and
+    depth, and central finite differences with the recorded (frozen) dt on fd_dirs of them."""
+    import dgrain
+
+    t0 = time.perf_counter()
+    m = dgrain.rectangle(nx, ny, jitter=JITTER, seed=3)
+    state = dgrain.initial_state(m, np.maximum(0.0, LAND_FILM - m.z))
+    rng = np.random.default_rng(3)
+    n_el = np.full(m.num_el, 0.03)
+    el, w = dgrain.place_gauges(m, dgrain.intertidal_points(m, 32, AMP, 3))
+    s = dgrain.Solver(m, wet_dry=1, cfl=ADJ_CFL, tide_on=1, tide_amp=AMP, tide_period=PERIOD, device=device)
+    mis = dgrain.GaugeMisfit(s, steps, ckpt, el, w)
+    s.set_element_manning(n_el * np.exp(rng.normal(0.0, 0.2, m.num_el)))
+    _, target = mis.forward(state)
+    mis.set_target(target)
+    s.set_element_manning(n_el)
+    log(f"[bench] adjoint: {m.num_el} triangles, {steps} steps, set up in {time.perf_counter() - t0:.1f} s")
+    J, _ = mis.forward(state)
+    g = mis.backward()
+    J, _ = mis.forward(state)
+    g = mis.backward()
+    fwd_ms, bwd_ms, _ = mis.timing()
+    s.upload_state(*state)
+    s.time_evolution(1e300, steps)
+    run_ms = s.last_device_ms()
+    mis.forward(state)  # the recorded run for the checks
+    checks = []
+    z0 = m.z.copy()
+    for k in range(max(2, fd_dirs)):
+        d = rng.normal(size=m.num_el if k % 2 == 0 else m.num_nodes)
+        d /= np.linalg.norm(d)
+        if k % 2 == 0:
+            _, dJ = mis.tlm(state, dn_el=d)
+            adj = float(g["n_el"] @ d)
+            h0 = 1e-4 * 0.03 / np.abs(d).max()
+            Jf = lambda e: mis.frozen(state, n_el=n_el + e * d)[1]  # noqa: E731
+        else:
+            _, dJ = mis.tlm(state, dz=d)
+            adj = float(g["z"] @ d)
+            h0 = 1e-3 * LAND_FILM / np.abs(d).max()  # small against the film on dry land
+            Jf = lambda e: mis.frozen(state, z=z0 + e * d)[1]  # noqa: E731
+        c = {"param": "n" if k % 2 == 0 else "z", "tlm": dJ, "adjoint": adj,
+             "tlm_vs_adjoint": abs(adj - dJ) / abs(dJ)}
+        if k < fd_dirs:
+            fds = [(Jf(h) - Jf(-h)) / (2 * h) for h in (h0, h0 / 10)]
+            c["fd"] = fds
+            c["fd_rel"] = min(abs(f - dJ) for f in fds) / abs(dJ)
+        checks.append(c)
+    s.close()
+    units = m.num_el * 2 * steps
+    return {"triangles": m.num_el, "steps": steps, "checkpoint_every": ckpt, "gauges": 32, "J": J,
+            "forward_ms": fwd_ms, "backward_ms": bwd_ms, "plain_run_ms": run_ms,
+            "adjoint_over_forward": bwd_ms / run_ms,
+            "backward_element_stage_updates_per_s": units / (bwd_ms / 1e3),
+            "tlm_vs_adjoint_max_rel": max(c["tlm_vs_adjoint"] for c in checks),
+            "fd_max_rel": max((c["fd_rel"] for c in checks if "fd_rel" in c), default=None),
+            "checks": checks,
+            "workload": f"coastal rectangle {nx}x{ny} cells, {m.num_el} triangles, jitter 0.1, wet/dry on, "
+                        f"CFL {ADJ_CFL}, tide 0.5 m, land film H0/2, Manning 0.03, 32 intertidal gauges, target "
+                        "from n x exp(N(0, 0.2)); forward = recorded run with checkpoints; backward = "
+                        "recomputation + reverse sweep; plain = dgr_run (CUDA graph) over the same steps; FD with "
+                        "frozen masks and dt (dgr_fd_frozen), steps of 1e-4 and 1e-5 of n, and of 1e-3 and 1e-4 of "
+                        "the land film for the depth, best of the two"}
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -283,6 +357,10 @@ def main():
     ap.add_argument("--ensemble-scenarios", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=100)
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=4000)
+    ap.add_argument("--adjoint-ckpt", type=int, default=100)
+    ap.add_argument("--adjoint-fd", type=int, default=4)
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -411,6 +489,11 @@ def main():
         solver.close()
         ens = ensemble_bench(args.ensemble_scenarios, args.ensemble_steps, 3, device=local)
 
+    adj = None
+    if not args.no_adjoint and args.adjoint_steps > 0:
+        solver.close()
+        adj = adjoint_bench(args.adjoint_steps, args.adjoint_ckpt, args.adjoint_fd, device=local)
+
     if rank == 0:
         cs = clocks.summary()
         line = {
@@ -431,6 +514,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": cs,
             "ensemble": ens,
+            "adjoint": adj,
         }
         print(json.dumps(line), flush=True)
     solver.close()

@@ -23,6 +23,7 @@
  * its directional derivative; its primal part is the forward bit for bit.
  */
 #include <algorithm>
+#include <type_traits>
 
 #include "dgr_internal.cuh"
 #include "dgr_tlm.cuh"
@@ -32,9 +33,9 @@ using namespace dgr;
 namespace dgr {
 
 struct AdjointState {
-    int nsteps = 0, K = 0, nseg = 0, ng = 0;
+    int nsteps = 0, K = 0, nseg = 0, ng = 0, nu = 0;
     int have_forward = 0;
-    int *g_el = nullptr;
+    int *g_el = nullptr, *u_el = nullptr, *u_ptr = nullptr, *u_g = nullptr; /* gauges; per gauge element */
     double *g_w = nullptr, *target = nullptr, *resid = nullptr, *sums = nullptr;
     double *dt_hist = nullptr, *time_hist = nullptr;
     double *ckU = nullptr;
@@ -59,7 +60,7 @@ void adjoint_release(dgr_ctx *c)
 {
     AdjointState *a = c->adj;
     if (!a) return;
-    void *ptrs[] = {a->g_el, a->g_w, a->target, a->resid, a->sums, a->dt_hist, a->time_hist, a->ckU, a->ckWd,
+    void *ptrs[] = {a->g_el, a->u_el, a->u_ptr, a->u_g, a->g_w, a->target, a->resid, a->sums, a->dt_hist, a->time_hist, a->ckU, a->ckWd,
                     a->ckClk, a->segU, a->segW, a->segR, a->segAvg, a->segB, a->segWd, a->lamU, a->lamW,
                     a->Rbar, a->bbar, a->bnode, a->fbar, a->zvb, a->zeb, a->nbar, a->zbar, a->barg, a->Ud,
                     a->Wd, a->flux_d, a->avg_d, a->bounds_d, a->zd, a->neld, a->rd, a->rt};
@@ -109,7 +110,23 @@ extern "C" int dgr_adjoint_setup(dgr_ctx *c, int nsteps, int ckpt_every, int nga
             return r;                  \
         }                              \
     } while (0)
+    /* gauges grouped by element, in gauge order within an element */
+    std::vector<int> order(ngauges);
+    for (int g = 0; g < ngauges; ++g) order[g] = g;
+    std::stable_sort(order.begin(), order.end(), [&](int p, int q) { return gauge_el[p] < gauge_el[q]; });
+    std::vector<int> uel, uptr;
+    for (int j = 0; j < ngauges; ++j) {
+        if (j == 0 || gauge_el[order[j]] != gauge_el[order[j - 1]]) {
+            uel.push_back(gauge_el[order[j]]);
+            uptr.push_back(j);
+        }
+    }
+    uptr.push_back(ngauges);
+    a->nu = (int)uel.size();
     AL(a->g_el, ng);
+    AL(a->u_el, uel.size());
+    AL(a->u_ptr, uptr.size());
+    AL(a->u_g, ng);
     AL(a->g_w, 3 * ng);
     AL(a->target, ns * ng);
     AL(a->resid, ns * ng);
@@ -141,6 +158,9 @@ extern "C" int dgr_adjoint_setup(dgr_ctx *c, int nsteps, int ckpt_every, int nga
 #undef AL
     cudaStream_t s = c->stream;
     CK(cudaMemcpyAsync(a->g_el, gauge_el, ng * 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(a->u_el, uel.data(), uel.size() * 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(a->u_ptr, uptr.data(), uptr.size() * 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(a->u_g, order.data(), ng * 4, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(a->g_w, gauge_w, 3 * ng * 8, cudaMemcpyHostToDevice, s));
     if (target)
         CK(cudaMemcpyAsync(a->target, target, ns * ng * 8, cudaMemcpyHostToDevice, s));
@@ -235,7 +255,7 @@ extern "C" int dgr_adjoint_forward(dgr_ctx *c, const double *zeta, const double 
                                   a->resid + (size_t)n * a->ng);
         c->launches += 3;
     }
-    k_misfit_sum<<<1, 32, 0, s>>>(a->resid, nullptr, (long long)a->nsteps * a->ng, a->sums);
+    k_misfit_sum<<<1, 32, 0, s>>>(a->resid, nullptr, (long long)a->nsteps * a->ng, 0, a->sums);
     k_clock_finish<<<1, 32, 0, s>>>(c->clk, 1, phys(c));
     c->launches += 2;
     CK(cudaGetLastError());
@@ -400,7 +420,8 @@ extern "C" int dgr_adjoint_backward(dgr_ctx *c, double *grad_n_el, double *grad_
             if (c->nbnd)
                 k_adj_forcing<<<blocks(c->nbnd, 256), 256, 0, s>>>(c->clk, a->time_hist, n, c->bnd_edges, c->bnd_type,
                                                                    c->nbnd, c->bzeta, c->bqn);
-            k_misfit_rev<<<1, 32, 0, s>>>(a->lamU, c->ldE, a->ng, a->g_el, a->g_w, a->resid + (size_t)n * a->ng);
+            k_misfit_rev<<<blocks(a->nu, 128), 128, 0, s>>>(a->lamU, c->ldE, a->nu, a->u_el, a->u_ptr, a->u_g, a->g_w,
+                                                            a->resid + (size_t)n * a->ng);
             c->launches += 2;
             reverse_stage(c, j, n, 1);
             reverse_stage(c, j, n, 0);
@@ -442,6 +463,104 @@ static int ensure_tlm(dgr_ctx *c)
     return DGR_OK;
 }
 
+/* reference layout [3*el+k] x 3 (host) -> planar [9][ldE] (device) */
+static int upload_planar(dgr_ctx *c, const double *z, const double *x, const double *y, double *dst)
+{
+    const size_t n3 = (size_t)3 * c->ne;
+    std::vector<double> h(3 * n3, 0.0);
+    if (z) memcpy(h.data(), z, n3 * 8);
+    if (x) memcpy(h.data() + n3, x, n3 * 8);
+    if (y) memcpy(h.data() + 2 * n3, y, n3 * 8);
+    double *tmp = nullptr;
+    int r = dalloc(&tmp, 3 * n3);
+    if (r) return r;
+    cudaError_t e = cudaMemcpyAsync(tmp, h.data(), 3 * n3 * 8, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        k_aos_to_planar<<<blocks(c->ne, 256), 256, 0, c->stream>>>(c->ne, c->ldE, tmp, tmp + n3, tmp + 2 * n3, dst);
+        c->launches++;
+        e = cudaStreamSynchronize(c->stream);
+    }
+    cudaFree(tmp);
+    CK(e);
+    return DGR_OK;
+}
+
+/*
+ * The recorded run's steps in two-lane arithmetic over the recorded dt sequence: T = Dual
+ * gives the tangent-linear model (second lanes = tangents), T = Pert the scheme at a
+ * perturbed point with the base run's decisions frozen (second lanes = perturbed values).
+ * The second lanes of the state, depths and element n are in a->Ud, a->zd, a->neld on
+ * entry.  Returns J of the base lane and, in out2, dJ (Dual) or J of the perturbed lane.
+ */
+template <class T>
+static int run_lanes(dgr_ctx *c, double *J, double *out2)
+{
+    AdjointState *a = c->adj;
+    cudaStream_t s = c->stream;
+    const MeshDev m = mesh_dev(c);
+    const bool wd = c->p.wet_dry != 0;
+    const bool pert = std::is_same<T, ad::Pert>::value;
+    const double g = c->p.g, h0 = c->p.H0, vz = c->p.VELZERO;
+    CK(cudaMemsetAsync(a->flux_d, 0, (size_t)6 * c->ldF * 8, s));
+    CK(cudaEventRecord(c->ev0, s));
+    launch_wd_refresh(c);
+    for (int n = 0; n < a->nsteps; ++n) {
+        if (c->nbnd)
+            k_adj_forcing<<<blocks(c->nbnd, 256), 256, 0, s>>>(c->clk, a->time_hist, n, c->bnd_edges, c->bnd_type,
+                                                               c->nbnd, c->bzeta, c->bqn);
+        for (int stage = 0; stage < 2; ++stage) {
+            double *S = stage == 0 ? c->U : c->W, *Sx = stage == 0 ? a->Ud : a->Wd;
+            double *OUT = stage == 0 ? c->W : c->U, *OUTx = stage == 0 ? a->Wd : a->Ud;
+            const int *wd_in = (stage == 0 || !wd) ? c->wdA : c->wdB;
+            int *wd_out = stage == 0 ? c->wdB : c->wdA;
+            if (wd)
+                k_tlm_edge<true, T><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, Sx, wd_in, c->bzeta, c->bqn, a->zd,
+                                                                       c->flux, a->flux_d, g);
+            else
+                k_tlm_edge<false, T><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, Sx, wd_in, c->bzeta, c->bqn, a->zd,
+                                                                        c->flux, a->flux_d, g);
+            if (stage == 0)
+                k_tlm_element<MODE_STAGE1, T><<<blocks(c->ne, 128), 128, 0, s>>>(
+                    m, S, Sx, c->U, a->Ud, wd_in, c->flux, a->flux_d, a->zd, c->n_el, a->neld, OUT, OUTx, c->avg,
+                    a->avg_d, c->clk, g, a->dt_hist, n);
+            else
+                k_tlm_element<MODE_STAGE2, T><<<blocks(c->ne, 128), 128, 0, s>>>(
+                    m, S, Sx, c->U, a->Ud, wd_in, c->flux, a->flux_d, a->zd, c->n_el, a->neld, OUT, OUTx, c->avg,
+                    a->avg_d, c->clk, g, a->dt_hist, n);
+            k_tlm_node<<<blocks(c->nn, 256), 256, 0, s>>>(m, c->avg, a->avg_d, c->bounds, a->bounds_d);
+            if (wd)
+                k_tlm_limit<true, T><<<blocks(c->ne, 128), 128, 0, s>>>(m, OUT, OUTx, c->bounds, a->bounds_d, a->zd,
+                                                                        wd_in, wd_out, h0, vz);
+            else
+                k_tlm_limit<false, T><<<blocks(c->ne, 128), 128, 0, s>>>(m, OUT, OUTx, c->bounds, a->bounds_d, a->zd,
+                                                                         wd_in, wd_out, h0, vz);
+        }
+        /* residuals of the base lane and of the second lane (a tangent has target 0) */
+        k_misfit<<<1, 32, 0, s>>>(c->U, c->ldE, a->ng, a->g_el, a->g_w, a->target + (size_t)n * a->ng,
+                                  a->rt + (size_t)n * a->ng);
+        k_misfit<<<1, 32, 0, s>>>(a->Ud, c->ldE, a->ng, a->g_el, a->g_w,
+                                  pert ? a->target + (size_t)n * a->ng : nullptr, a->rd + (size_t)n * a->ng);
+        c->launches += 11;
+    }
+    k_misfit_sum<<<1, 32, 0, s>>>(a->rt, a->rd, (long long)a->nsteps * a->ng, pert ? 1 : 0, a->sums);
+    c->launches++;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ev1, s));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    a->tlm_ms = ms;
+    double sums[2];
+    CK(cudaMemcpy(sums, a->sums, 16, cudaMemcpyDeviceToHost));
+    if (J) *J = sums[0];
+    if (out2) *out2 = sums[1];
+    if (c->p.wet_dry) {
+        c->wd_fresh = 1;
+        c->wd_cur_is_B = 1;
+    }
+    return DGR_OK;
+}
+
 extern "C" int dgr_tlm(dgr_ctx *c, const double *zeta, const double *Qx, const double *Qy, const int *WD,
                        const double *dzeta0, const double *dQx0, const double *dQy0, const double *dn_el,
                        const double *dz, double *J, double *dJ)
@@ -454,26 +573,11 @@ extern "C" int dgr_tlm(dgr_ctx *c, const double *zeta, const double *Qx, const d
     r = dgr_upload_state(c, zeta, Qx, Qy, WD);
     if (r) return r;
     cudaStream_t s = c->stream;
-    const MeshDev m = mesh_dev(c);
-    const size_t ne = c->ne, E9 = plane9(c);
-    /* tangent of the initial state (reference layout [3*el+k] -> planar) */
-    CK(cudaMemsetAsync(a->Ud, 0, E9 * 8, s));
+    const size_t ne = c->ne;
+    CK(cudaMemsetAsync(a->Ud, 0, plane9(c) * 8, s));
     if (dzeta0 || dQx0 || dQy0) {
-        const size_t n3 = 3 * ne;
-        std::vector<double> h(3 * n3, 0.0);
-        if (dzeta0) memcpy(h.data(), dzeta0, n3 * 8);
-        if (dQx0) memcpy(h.data() + n3, dQx0, n3 * 8);
-        if (dQy0) memcpy(h.data() + 2 * n3, dQy0, n3 * 8);
-        double *tmp = nullptr;
-        r = dalloc(&tmp, 3 * n3);
+        r = upload_planar(c, dzeta0, dQx0, dQy0, a->Ud);
         if (r) return r;
-        cudaError_t e = cudaMemcpyAsync(tmp, h.data(), 3 * n3 * 8, cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) {
-            k_aos_to_planar<<<blocks(c->ne, 256), 256, 0, s>>>(c->ne, c->ldE, tmp, tmp + n3, tmp + 2 * n3, a->Ud);
-            e = cudaStreamSynchronize(s);
-        }
-        cudaFree(tmp);
-        CK(e);
     }
     if (dz)
         CK(cudaMemcpyAsync(a->zd, dz, (size_t)c->nn * 8, cudaMemcpyHostToDevice, s));
@@ -483,67 +587,35 @@ extern "C" int dgr_tlm(dgr_ctx *c, const double *zeta, const double *Qx, const d
         CK(cudaMemcpyAsync(a->neld, dn_el, ne * 8, cudaMemcpyHostToDevice, s));
     else
         CK(cudaMemsetAsync(a->neld, 0, ne * 8, s));
-    CK(cudaMemsetAsync(a->flux_d, 0, (size_t)6 * c->ldF * 8, s));
+    return run_lanes<ad::Dual>(c, J, dJ);
+}
 
-    const bool wd = c->p.wet_dry != 0;
-    const double g = c->p.g, h0 = c->p.H0, vz = c->p.VELZERO;
-    CK(cudaEventRecord(c->ev0, s));
-    launch_wd_refresh(c);
-    for (int n = 0; n < a->nsteps; ++n) {
-        if (c->nbnd)
-            k_adj_forcing<<<blocks(c->nbnd, 256), 256, 0, s>>>(c->clk, a->time_hist, n, c->bnd_edges, c->bnd_type,
-                                                               c->nbnd, c->bzeta, c->bqn);
-        for (int stage = 0; stage < 2; ++stage) {
-            double *S = stage == 0 ? c->U : c->W, *Sd = stage == 0 ? a->Ud : a->Wd;
-            double *OUT = stage == 0 ? c->W : c->U, *OUTd = stage == 0 ? a->Wd : a->Ud;
-            const int *wd_in = (stage == 0 || !wd) ? c->wdA : c->wdB;
-            int *wd_out = stage == 0 ? c->wdB : c->wdA;
-            if (wd)
-                k_tlm_edge<true><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, Sd, wd_in, c->bzeta, c->bqn, a->zd, c->flux,
-                                                                    a->flux_d, g);
-            else
-                k_tlm_edge<false><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, Sd, wd_in, c->bzeta, c->bqn, a->zd,
-                                                                     c->flux, a->flux_d, g);
-            if (stage == 0)
-                k_tlm_element<MODE_STAGE1><<<blocks(c->ne, 128), 128, 0, s>>>(
-                    m, S, Sd, c->U, a->Ud, wd_in, c->flux, a->flux_d, a->zd, c->n_el, a->neld, OUT, OUTd, c->avg,
-                    a->avg_d, c->clk, g, a->dt_hist, n);
-            else
-                k_tlm_element<MODE_STAGE2><<<blocks(c->ne, 128), 128, 0, s>>>(
-                    m, S, Sd, c->U, a->Ud, wd_in, c->flux, a->flux_d, a->zd, c->n_el, a->neld, OUT, OUTd, c->avg,
-                    a->avg_d, c->clk, g, a->dt_hist, n);
-            k_tlm_node<<<blocks(c->nn, 256), 256, 0, s>>>(m, c->avg, a->avg_d, c->bounds, a->bounds_d);
-            if (wd)
-                k_tlm_limit<true><<<blocks(c->ne, 128), 128, 0, s>>>(m, OUT, OUTd, c->bounds, a->bounds_d, a->zd,
-                                                                     wd_in, wd_out, h0, vz);
-            else
-                k_tlm_limit<false><<<blocks(c->ne, 128), 128, 0, s>>>(m, OUT, OUTd, c->bounds, a->bounds_d, a->zd,
-                                                                      wd_in, wd_out, h0, vz);
-        }
-        /* residuals and their tangents (the tangent of a gauge value is the same functional
-         * of the state tangent; its target is 0) */
-        k_misfit<<<1, 32, 0, s>>>(c->U, c->ldE, a->ng, a->g_el, a->g_w, a->target + (size_t)n * a->ng,
-                                  a->rt + (size_t)n * a->ng);
-        k_misfit<<<1, 32, 0, s>>>(a->Ud, c->ldE, a->ng, a->g_el, a->g_w, nullptr, a->rd + (size_t)n * a->ng);
-        c->launches += 11;
-    }
-    k_misfit_sum<<<1, 32, 0, s>>>(a->rt, a->rd, (long long)a->nsteps * a->ng, a->sums);
-    c->launches++;
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(c->ev1, s));
-    CK(cudaEventSynchronize(c->ev1));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    a->tlm_ms = ms;
-    double sums[2];
-    CK(cudaMemcpy(sums, a->sums, 16, cudaMemcpyDeviceToHost));
-    if (J) *J = sums[0];
-    if (dJ) *dJ = sums[1];
-    if (c->p.wet_dry) {
-        c->wd_fresh = 1;
-        c->wd_cur_is_B = 1;
-    }
-    return DGR_OK;
+extern "C" int dgr_fd_frozen(dgr_ctx *c, const double *zeta, const double *Qx, const double *Qy, const int *WD,
+                             const double *zeta_p, const double *Qx_p, const double *Qy_p, const double *n_el_p,
+                             const double *z_p, double *J, double *J_p)
+{
+    if (!c || !c->adj || !c->adj->have_forward || !zeta || !Qx || !Qy || !WD) return DGR_ERR_INVALID;
+    AdjointState *a = c->adj;
+    CK(cudaSetDevice(c->device));
+    int r = ensure_tlm(c);
+    if (r) return r;
+    r = dgr_upload_state(c, zeta, Qx, Qy, WD);
+    if (r) return r;
+    cudaStream_t s = c->stream;
+    const size_t ne = c->ne;
+    r = upload_planar(c, zeta_p ? zeta_p : zeta, Qx_p ? Qx_p : Qx, Qy_p ? Qy_p : Qy, a->Ud);
+    if (r) return r;
+    if (z_p)
+        CK(cudaMemcpyAsync(a->zd, z_p, (size_t)c->nn * 8, cudaMemcpyHostToDevice, s));
+    else
+        CK(cudaMemcpyAsync(a->zd, c->zn, (size_t)c->nn * 8, cudaMemcpyDeviceToDevice, s));
+    if (n_el_p)
+        CK(cudaMemcpyAsync(a->neld, n_el_p, ne * 8, cudaMemcpyHostToDevice, s));
+    else if (c->n_el)
+        CK(cudaMemcpyAsync(a->neld, c->n_el, ne * 8, cudaMemcpyDeviceToDevice, s));
+    else
+        CK(cudaMemsetAsync(a->neld, 0, ne * 8, s));
+    return run_lanes<ad::Pert>(c, J, J_p);
 }
 
 extern "C" int dgr_adjoint_timing(const dgr_ctx *c, double *forward_ms, double *backward_ms, double *tlm_ms)

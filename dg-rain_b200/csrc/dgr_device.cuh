@@ -40,6 +40,10 @@ DGR_HD T rmax(const T &a, const T &b) { return (a > b) ? a : b; }
 template <class T>
 DGR_HD T rmin(const T &a, const T &b) { return (a < b) ? a : b; }
 
+/* value of a scalar (decisions are taken on values; the dual-number overload lives with
+ * the dual type) */
+DGR_HD double val(double x) { return x; }
+
 /* Which operand fmax(a, b) passes on, for derivatives: b when b > a or a is NaN.  At a
  * tie the values agree and a is taken. */
 DGR_HD bool fmax_takes_b(double a, double b) { return (b > a) || isnan(a); }

@@ -94,10 +94,74 @@ DGR_HD Dual pow43(const Dual &a)
     return Dual(p, a.d * (4.0 / 3.0) * (p / a.v));
 }
 
+/* value part (the double overload is in dgr_device.cuh) */
+DGR_HD double val(const Dual &x) { return x.v; }
+
+/*
+ * A base value v and a perturbed value p evaluated side by side, every decision taken on
+ * v: running the scheme in Pert arithmetic from (u, u + h du) gives the scheme at the
+ * perturbed point with the base run's decisions frozen (finite differences "with frozen
+ * masks").  Each operation applies the double operation to both lanes; fabs and fmax
+ * choose by the base lane (the same kink conventions as Dual).
+ */
+struct Pert {
+    double v, p;
+    DGR_HD Pert() : v(0.0), p(0.0) {}
+    DGR_HD Pert(double x) : v(x), p(x) {}
+    DGR_HD Pert(double x, double xp) : v(x), p(xp) {}
+};
+
+DGR_HD Pert operator-(const Pert &a) { return Pert(-a.v, -a.p); }
+DGR_HD Pert operator+(const Pert &a, const Pert &b) { return Pert(a.v + b.v, a.p + b.p); }
+DGR_HD Pert operator+(const Pert &a, double b) { return Pert(a.v + b, a.p + b); }
+DGR_HD Pert operator+(double a, const Pert &b) { return Pert(a + b.v, a + b.p); }
+DGR_HD Pert operator-(const Pert &a, const Pert &b) { return Pert(a.v - b.v, a.p - b.p); }
+DGR_HD Pert operator-(const Pert &a, double b) { return Pert(a.v - b, a.p - b); }
+DGR_HD Pert operator-(double a, const Pert &b) { return Pert(a - b.v, a - b.p); }
+DGR_HD Pert operator*(const Pert &a, const Pert &b) { return Pert(a.v * b.v, a.p * b.p); }
+DGR_HD Pert operator*(const Pert &a, double b) { return Pert(a.v * b, a.p * b); }
+DGR_HD Pert operator*(double a, const Pert &b) { return Pert(a * b.v, a * b.p); }
+DGR_HD Pert operator/(const Pert &a, const Pert &b) { return Pert(a.v / b.v, a.p / b.p); }
+DGR_HD Pert operator/(const Pert &a, double b) { return Pert(a.v / b, a.p / b); }
+DGR_HD Pert operator/(double a, const Pert &b) { return Pert(a / b.v, a / b.p); }
+DGR_HD Pert &operator+=(Pert &a, const Pert &b) { return a = a + b; }
+DGR_HD Pert &operator-=(Pert &a, const Pert &b) { return a = a - b; }
+
+DGR_HD bool operator<(const Pert &a, const Pert &b) { return a.v < b.v; }
+DGR_HD bool operator<(const Pert &a, double b) { return a.v < b; }
+DGR_HD bool operator<(double a, const Pert &b) { return a < b.v; }
+DGR_HD bool operator>(const Pert &a, const Pert &b) { return a.v > b.v; }
+DGR_HD bool operator>(const Pert &a, double b) { return a.v > b; }
+DGR_HD bool operator>(double a, const Pert &b) { return a > b.v; }
+DGR_HD bool operator<=(const Pert &a, const Pert &b) { return a.v <= b.v; }
+DGR_HD bool operator<=(const Pert &a, double b) { return a.v <= b; }
+DGR_HD bool operator>=(const Pert &a, const Pert &b) { return a.v >= b.v; }
+DGR_HD bool operator>=(const Pert &a, double b) { return a.v >= b; }
+DGR_HD bool operator==(const Pert &a, double b) { return a.v == b; }
+
+DGR_HD bool isnan(const Pert &a) { return ::isnan(a.v); }
+DGR_HD Pert sqrt(const Pert &a) { return Pert(::sqrt(a.v), ::sqrt(a.p)); }
+DGR_HD Pert fabs(const Pert &a) { return a.v < 0 ? -a : a; }
+DGR_HD Pert fmax(const Pert &a, const Pert &b)
+{
+    const bool take_b = (b.v > a.v) || ::isnan(a.v);
+    return Pert(::fmax(a.v, b.v), take_b ? b.p : a.p);
+}
+DGR_HD Pert fmax(double a, const Pert &b) { return fmax(Pert(a), b); }
+DGR_HD Pert fmax(const Pert &a, double b) { return fmax(a, Pert(b)); }
+DGR_HD Pert pow43(const Pert &a) { return Pert(dgr::pow43(a.v), dgr::pow43(a.p)); }
+DGR_HD double val(const Pert &x) { return x.v; }
+
+/* lanes of the two types: a value with its tangent (Dual) or its perturbed value (Pert) */
+DGR_HD Dual lane(const Dual *, double v, double x) { return Dual(v, x); }
+DGR_HD Pert lane(const Pert *, double v, double x) { return Pert(v, x); }
+DGR_HD double second(const Dual &a) { return a.d; }
+DGR_HD double second(const Pert &a) { return a.p; }
+
+/* g n^2 of the Manning term: tangent 2 g n dn, or the value at the perturbed n (the
+ * expression of the element set-up, (g n) n) */
+DGR_HD Dual gnn_lane(const Dual *, double gnn, double g, double n, double x) { return Dual(gnn, 2.0 * g * n * x); }
+DGR_HD Pert gnn_lane(const Pert *, double gnn, double g, double n, double x) { return Pert(gnn, g * x * x); }
+
 }  // namespace ad
-
-/* value of a scalar of either kind (decisions are taken on values) */
-DGR_HD double val(double x) { return x; }
-DGR_HD double val(const ad::Dual &x) { return x.v; }
-
 }  // namespace dgr

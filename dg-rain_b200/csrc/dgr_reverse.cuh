@@ -67,11 +67,6 @@ DGR_HD void roe_flux_rev(const double fhb[3], double zeta_in, double zeta_ex, do
     const double u_hat = (u_in * s_in + u_ex * s_ex) / D;
     const double v_hat = (v_in * s_in + v_ex * s_ex) / D;
     const double c = sqrt(g * h_hat);
-    const double den = -2 * c;
-    const double nx_den = nx / den, ny_den = ny / den;
-    const double ri[3][3] = {{(-c - nx * u_hat - ny * v_hat) / den, nx_den, ny_den},
-                             {(-2 * c * ny * u_hat + 2 * c * nx * v_hat) / den, 2 * c * ny / den, -2 * c * nx / den},
-                             {(-c + nx * u_hat + ny * v_hat) / den, -nx_den, -ny_den}};
     const double un_in = u_in * nx + v_in * ny, un_ex = u_ex * nx + v_ex * ny;
     const double c_in = sqrt(g * h_in), c_ex = sqrt(g * h_ex);
     const double un_hat = u_hat * nx + v_hat * ny;
@@ -93,12 +88,16 @@ DGR_HD void roe_flux_rev(const double fhb[3], double zeta_in, double zeta_ex, do
         lh[i] = fmax(e, al);
         sel[i] = s;
     }
-    double p1[3], p2[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        p1[i] = ri[i][0] * jump[0] + ri[i][1] * jump[1] + ri[i][2] * jump[2];
-        p2[i] = lh[i] * p1[i];
-    }
+    /* p1 = R^-1 jump in closed form (the forward's matrix entries simplified):
+     * p1_0 = j0/2 + A, p1_2 = j0/2 - A, A = (un' j0 - nx j1 - ny j2)/(2c),
+     * p1_1 = (ny u_hat - nx v_hat) j0 - ny j1 + nx j2.  These values only scale
+     * derivatives, so their last-bit rounding does not matter. */
+    const double ic2 = 1.0 / (2.0 * c);
+    const double unp = nx * u_hat + ny * v_hat;
+    const double A = (unp * jump[0] - nx * jump[1] - ny * jump[2]) * ic2;
+    const double p1[3] = {0.5 * jump[0] + A, (ny * u_hat - nx * v_hat) * jump[0] - ny * jump[1] + nx * jump[2],
+                          0.5 * jump[0] - A};
+    const double p2[3] = {lh[0] * p1[0], lh[1] * p1[1], lh[2] * p1[2]};
 
     /* fh = 0.5 (fn_in + fn_ex) + 0.5 r p2 */
     const double p3b[3] = {0.5 * fhb[0], 0.5 * fhb[1], 0.5 * fhb[2]};
@@ -111,11 +110,7 @@ DGR_HD void roe_flux_rev(const double fhb[3], double zeta_in, double zeta_ex, do
     const double lhb[3] = {p2b[0] * p1[0], p2b[1] * p1[1], p2b[2] * p1[2]};
     const double p1b[3] = {lh[0] * p2b[0], lh[1] * p2b[1], lh[2] * p2b[2]};
 
-    /* p1 = ri jump: p1_0 = j0/2 + A, p1_2 = j0/2 - A, A = (un' j0 - nx j1 - ny j2)/(2c),
-     * p1_1 = (ny u_hat - nx v_hat) j0 - ny j1 + nx j2 */
-    const double ic2 = 1.0 / (2.0 * c);
-    const double unp = nx * u_hat + ny * v_hat;
-    const double A = (unp * jump[0] - nx * jump[1] - ny * jump[2]) * ic2;
+    /* p1 = R^-1 jump */
     const double Ab = p1b[0] - p1b[2];
     const double j0b = 0.5 * (p1b[0] + p1b[2]) + Ab * unp * ic2 + p1b[1] * (ny * u_hat - nx * v_hat);
     const double j1b = -Ab * nx * ic2 - ny * p1b[1];
@@ -123,7 +118,7 @@ DGR_HD void roe_flux_rev(const double fhb[3], double zeta_in, double zeta_ex, do
     const double unpb = Ab * jump[0] * ic2;
     uhb += nx * unpb + p1b[1] * ny * jump[0];
     vhb += ny * unpb - p1b[1] * nx * jump[0];
-    cb -= Ab * A / c;
+    cb -= 2.0 * Ab * A * ic2;
 
     /* entropy fix */
     double rawb[3] = {0, 0, 0}, linb[3] = {0, 0, 0}, lexb[3] = {0, 0, 0};
@@ -151,13 +146,14 @@ DGR_HD void roe_flux_rev(const double fhb[3], double zeta_in, double zeta_ex, do
     double heb = c_ex == 0.0 ? 0.0 : c_ex_b * g / (2.0 * c_ex);
 
     /* c = sqrt(g h_hat), h_hat = (h_in + h_ex)/2 */
-    const double hhb = c == 0.0 ? 0.0 : cb * g / (2.0 * c);
+    const double hhb = c == 0.0 ? 0.0 : cb * g * ic2;
     hib += 0.5 * hhb;
     heb += 0.5 * hhb;
 
     /* Roe averages */
-    const double Nub = uhb / D, Nvb = vhb / D;
-    const double Db = -(uhb * u_hat + vhb * v_hat) / D;
+    const double iD = 1.0 / D;
+    const double Nub = uhb * iD, Nvb = vhb * iD;
+    const double Db = -(uhb * u_hat + vhb * v_hat) * iD;
     uib += Nub * s_in;
     ueb += Nub * s_ex;
     vib += Nvb * s_in;
@@ -172,12 +168,13 @@ DGR_HD void roe_flux_rev(const double fhb[3], double zeta_in, double zeta_ex, do
     normal_flux_rev(p3b, h_ex, u_ex, v_ex, z_edge, nx, ny, local_g, heb, ueb, veb, zb);
 
     /* velocities */
-    b.qxin += uib / h_in;
-    b.qyin += vib / h_in;
-    hib -= (uib * u_in + vib * v_in) / h_in;
-    b.qxex += ueb / h_ex;
-    b.qyex += veb / h_ex;
-    heb -= (ueb * u_ex + veb * v_ex) / h_ex;
+    const double ihi = 1.0 / h_in, ihe = 1.0 / h_ex;
+    b.qxin += uib * ihi;
+    b.qyin += vib * ihi;
+    hib -= (uib * u_in + vib * v_in) * ihi;
+    b.qxex += ueb * ihe;
+    b.qyex += veb * ihe;
+    heb -= (ueb * u_ex + veb * v_ex) * ihe;
 
     /* jump and depths */
     b.zin += j0b + hib;
@@ -451,7 +448,8 @@ DGR_HD LimitDecisions limit_core_rev(const double w[3][3], const Bnd &bnd, const
 #pragma unroll
         for (int k = 0; k < 3; ++k) wl[v][k] = w[v][k];
     LimitDecisions dec;
-    limit_core<LIMIT, false, double>(wl, bnd, zn, h0, velzero, dec);
+    LimitTrace trace;
+    limit_core<LIMIT, false, double, Bnd, true>(wl, bnd, zn, h0, velzero, dec, &trace);
     const int modify = dec.modify;
 
     if (PDOP) {
@@ -627,65 +625,20 @@ DGR_HD LimitDecisions limit_core_rev(const double w[3][3], const Bnd &bnd, const
     if (LIMIT && modify) {
 #pragma unroll
         for (int v = 0; v < 3; ++v) {
-            /* forward trace of variable v (limit_core, :157-311) */
-            const double w1 = w[v][0], w2 = w[v][1], w3 = w[v][2];
-            const double raw[3] = {w1 - w2 + w3, w1 + w2 - w3, -w1 + w2 + w3};
-            double vmax[3], vmin[3], vx[3];
-            int clamp[3]; /* 0 raw, 1 vmax, 2 vmin */
-            const double avg = (w1 + w2 + w3) / 3;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                vmax[k] = bnd(v, k, 0);
-                vmin[k] = bnd(v, k, 1);
-                const double r1 = rmin(raw[k], vmax[k]);
-                clamp[k] = raw[k] < vmax[k] ? 0 : 1;
-                if (fmax_takes_b(r1, vmin[k])) clamp[k] = 2;
-                vx[k] = fmax(r1, vmin[k]);
-            }
-            int sdv[3];
-            int step[3][3]; /* bit 0: diff > 0, bit 1: redmax taken; bits 2-3: div */
-#pragma unroll
-            for (int ll = 0; ll < 3; ++ll) {
-                const double sumloc = (vx[0] + vx[1] + vx[2]) / 3;
-                double sumdiff = (sumloc - avg) * 3;
-                const int sd = sgn(sumdiff);
-                const double sdd = (double)sd;
-                sdv[ll] = sd;
-                const double diff[3] = {(vx[0] - avg) * sdd, (vx[1] - avg) * sdd, (vx[2] - avg) * sdd};
-                double kdp = (double)((diff[0] > 0) + (diff[1] > 0) + (diff[2] > 0));
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const double div = fmax(1.0, kdp);
-                    double redfac;
-                    int bits = 0;
-                    if (diff[k] > 0) {
-                        redfac = div_by_count(sumdiff * sdd, div);
-                        kdp -= 1;
-                        bits |= 1;
-                    } else {
-                        redfac = 0;
-                    }
-                    const double redmax = (sd > 0) ? vx[k] - vmin[k] : vmax[k] - vx[k];
-                    if (!(redfac < redmax)) bits |= 2;
-                    redfac = rmin(redfac, redmax);
-                    sumdiff -= redfac * sdd;
-                    vx[k] -= redfac * sdd;
-                    step[ll][k] = bits | ((int)div << 2);
-                }
-            }
-            /* reverse */
+            const unsigned long long tb = trace.bits[v];
             double vxb[3] = {0.5 * (wb[v][0] + wb[v][2]), 0.5 * (wb[v][0] + wb[v][1]), 0.5 * (wb[v][1] + wb[v][2])};
             double avgb = 0;
 #pragma unroll
             for (int ll = 2; ll >= 0; --ll) {
-                const double sdd = (double)sdv[ll];
+                const int sd = (int)((tb >> (6 + 2 * ll)) & 3) - 1;
+                const double sdd = (double)sd;
                 double sumdiffb = 0;
 #pragma unroll
                 for (int k = 2; k >= 0; --k) {
-                    const int bits = step[ll][k];
+                    const int bits = (int)((tb >> (12 + 4 * (3 * ll + k))) & 15);
                     const double rfb = -sdd * (sumdiffb + vxb[k]);
                     if (bits & 2) {
-                        if (sdv[ll] > 0) {
+                        if (sd > 0) {
                             vxb[k] += rfb;
                             bminb[v][k] -= rfb;
                         } else {
@@ -704,9 +657,10 @@ DGR_HD LimitDecisions limit_core_rev(const double w[3][3], const Bnd &bnd, const
             double rawb[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
+                const int clamp = (int)((tb >> (2 * k)) & 3);
                 rawb[k] = 0;
-                if (clamp[k] == 2) bminb[v][k] += vxb[k];
-                else if (clamp[k] == 1) bmaxb[v][k] += vxb[k];
+                if (clamp == 2) bminb[v][k] += vxb[k];
+                else if (clamp == 1) bmaxb[v][k] += vxb[k];
                 else rawb[k] = vxb[k];
             }
             double inb[3];

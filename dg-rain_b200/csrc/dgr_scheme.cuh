@@ -364,14 +364,24 @@ struct LimitDecisions {
     int code;        /* 4: NaN depth, 5: NaN velocity */
 };
 
+/* The limiter's path for one variable, recorded for the adjoint (48 bits): clamp of
+ * vertex k in bits 2k..2k+1 (0 none, 1 to the node max, 2 to the node min); sign of the
+ * redistribution pass ll plus one in bits 6+2ll..; per pass ll and vertex k four bits at
+ * 12 + 4(3ll+k): bit 0 diff > 0, bit 1 the cap redmax taken, bits 2-3 the divisor. */
+struct LimitTrace {
+    unsigned long long bits[3];
+};
+
 /*
  * One element: vertex-based limiter (2DCode/SlopeLimiter2D.c:157-343), then the
  * positive-depth operator (2DCode/wetDry2D.c:63-260), in place on w[variable][midpoint].
  * bnd(v, k, is_min) is the node max (is_min = 0) or min (1) of variable v's element means
- * at the element's vertex k; zn are the vertex depths.
+ * at the element's vertex k; zn are the vertex depths.  With TRACE the limiter's path is
+ * recorded in *trace (values are unaffected).
  */
-template <bool LIMIT, bool PDOP, class T, class Bnd>
-DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, double velzero, LimitDecisions &dec)
+template <bool LIMIT, bool PDOP, class T, class Bnd, bool TRACE = false>
+DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, double velzero, LimitDecisions &dec,
+                       LimitTrace *trace = nullptr)
 {
     dec.modify = 0;
     dec.mass_branch = 0;
@@ -396,14 +406,24 @@ DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, doub
                 const T m0 = vmin[0] + zn[0], m1 = vmin[1] + zn[1], m2 = vmin[2] + zn[2];
                 if (h1 > h0 && h2 > h0 && h3 > h0 && m0 > h0 && m1 > h0 && m2 > h0) modify = 1;
             }
+            unsigned long long tb = 0;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) vx[k] = fmax(rmin(vx[k], vmax[k]), vmin[k]);
+            for (int k = 0; k < 3; ++k) {
+                if (TRACE) {
+                    const T r1 = rmin(vx[k], vmax[k]);
+                    unsigned long long c = (vx[k] < vmax[k]) ? 0 : 1;
+                    if (fmax_takes_b(val(r1), val(vmin[k]))) c = 2;
+                    tb |= c << (2 * k);
+                }
+                vx[k] = fmax(rmin(vx[k], vmax[k]), vmin[k]);
+            }
 #pragma unroll
             for (int ll = 0; ll < 3; ++ll) { /* :254-299 */
                 const T sumloc = (vx[0] + vx[1] + vx[2]) / 3;
                 T sumdiff = (sumloc - avg) * 3;
                 const int sd = sgn(sumdiff);
                 const double sdd = (double)sd;
+                if (TRACE) tb |= (unsigned long long)(sd + 1) << (6 + 2 * ll);
                 const T diff[3] = {(vx[0] - avg) * sdd, (vx[1] - avg) * sdd, (vx[2] - avg) * sdd};
                 double kdp = (double)((diff[0] > 0) + (diff[1] > 0) + (diff[2] > 0));
 #pragma unroll
@@ -417,11 +437,16 @@ DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, doub
                         redfac = 0;
                     }
                     const T redmax = (sd > 0) ? vx[k] - vmin[k] : vmax[k] - vx[k];
+                    if (TRACE)
+                        tb |= (unsigned long long)((diff[k] > 0 ? 1 : 0) | (redfac < redmax ? 0 : 2) |
+                                                   ((int)div << 2))
+                              << (12 + 4 * (3 * ll + k));
                     redfac = rmin(redfac, redmax);
                     sumdiff -= redfac * sdd;
                     vx[k] -= redfac * sdd;
                 }
             }
+            if (TRACE) trace->bits[v] = tb;
             out[v][0] = (vx[0] + vx[1]) / 2;
             out[v][1] = (vx[1] + vx[2]) / 2;
             out[v][2] = (vx[2] + vx[0]) / 2;

@@ -26,33 +26,49 @@
 #include "dgr_kernels.cuh"
 #include "dgr_reverse.cuh"
 
+/* Minimum resident blocks per SM of the reverse kernels (register caps 65536 / (threads x
+ * blocks)); chosen by measurement, overridable at build time. */
+#ifndef DGR_ADJ_MINB_EDGE
+#define DGR_ADJ_MINB_EDGE 2
+#endif
+#ifndef DGR_ADJ_MINB_ELEMENT
+#define DGR_ADJ_MINB_ELEMENT 4
+#endif
+#ifndef DGR_ADJ_MINB_LIMIT
+#define DGR_ADJ_MINB_LIMIT 4
+#endif
+
 namespace dgr {
 
 using ad::Dual;
 
-/* Depth and Manning factors of one element as Duals: values from the geometry planes,
- * derivatives from the vertex-depth tangents and the element-n tangent. */
-struct DualZGeo {
-    Dual mz[3], gn[3], gz[2];
-    DGR_HD Dual midz(int e) const { return mz[e]; }
-    DGR_HD Dual gnn(int e) const { return gn[e]; }
-    DGR_HD Dual gradz(int j) const { return gz[j]; }
+/* Depth and Manning factors of one element in two-lane arithmetic (T = Dual or Pert):
+ * values from the geometry planes, second lanes from the vertex-depth lanes zvx (tangents
+ * or perturbed depths) and the element-n lane nelx, by the set-up's own expressions. */
+template <class T>
+struct LaneZGeo {
+    T mz[3], gn[3], gz[2];
+    DGR_HD T midz(int e) const { return mz[e]; }
+    DGR_HD T gnn(int e) const { return gn[e]; }
+    DGR_HD T gradz(int j) const { return gz[j]; }
 };
 
-template <class Geo>
-DGR_HD DualZGeo dual_zgeo(const Geo &geo, const double zvd[3], double nel, double neld, double g)
+template <class T, class Geo>
+DGR_HD LaneZGeo<T> lane_zgeo(const Geo &geo, const double zvx[3], double nel, double nelx, double g)
 {
-    DualZGeo z;
+    LaneZGeo<T> z;
+    const T *tag = nullptr;
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
-        z.mz[e] = Dual(geo(G_MIDZ + e), 0.5 * (zvd[e] + zvd[(e + 1) % 3]));
-        /* g n n: d = 2 g n dn (per-element n only) */
-        z.gn[e] = Dual(geo(G_GNN + e), nel >= 0.0 ? 2.0 * g * nel * neld : 0.0);
+        z.mz[e] = lane(tag, geo(G_MIDZ + e), 0.5 * (zvx[e] + zvx[(e + 1) % 3]));
+        /* per-element n only; the node-average n is not a parameter */
+        z.gn[e] = nel >= 0.0 ? gnn_lane(tag, geo(G_GNN + e), g, nel, nelx) : T(geo(G_GNN + e));
     }
 #pragma unroll
     for (int j = 0; j < 2; ++j)
-        z.gz[j] = Dual(geo(G_GRADZ + j),
-                       z.mz[0].d * geo(G_GP + j) + z.mz[1].d * geo(G_GP + 2 + j) + z.mz[2].d * geo(G_GP + 4 + j));
+        z.gz[j] = lane(tag, geo(G_GRADZ + j),
+                       second(z.mz[0]) * geo(G_GP + j) + second(z.mz[1]) * geo(G_GP + 2 + j) +
+                           second(z.mz[2]) * geo(G_GP + 4 + j));
     return z;
 }
 
@@ -163,129 +179,144 @@ static __global__ void k_misfit(const double *__restrict__ S, int ld, int ng, co
     }
 }
 
-/* J = sum_n sum_g r^2 and, with rd, dJ = sum 2 r rd; sequential for a fixed order. */
-static __global__ void k_misfit_sum(const double *__restrict__ resid, const double *__restrict__ rd, long long count, double *out)
+/* J = sum_n sum_g r^2 into out[0] and, with rx: the tangent sum 2 r rx (squared = 0) or
+ * the objective sum rx^2 of the perturbed lane (squared = 1) into out[1]; sequential for a
+ * fixed order. */
+static __global__ void k_misfit_sum(const double *__restrict__ resid, const double *__restrict__ rx, long long count,
+                                    int squared, double *out)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double J = 0, dJ = 0;
+    double J = 0, J2 = 0;
     for (long long i = 0; i < count; ++i) {
         J += resid[i] * resid[i];
-        if (rd) dJ += 2.0 * resid[i] * rd[i];
+        if (rx) J2 += squared ? rx[i] * rx[i] : 2.0 * resid[i] * rx[i];
     }
     out[0] = J;
-    out[1] = dJ;
+    out[1] = J2;
 }
 
-/* adjoint of the misfit of step n: lam(zeta) += 2 r_g w_gk at the gauges (gauges sharing an
- * element are taken one after another) */
-static __global__ void k_misfit_rev(double *__restrict__ lam, int ld, int ng, const int *__restrict__ g_el,
-                             const double *__restrict__ g_w, const double *__restrict__ resid)
+/* adjoint of the misfit of step n: lam(zeta) += 2 r_g w_gk at the gauges.  One thread per
+ * gauge element (u_el, CSR u_ptr/u_g of its gauges in ascending order), so gauges that share
+ * an element are added in a fixed order. */
+static __global__ void k_misfit_rev(double *__restrict__ lam, int ld, int nu, const int *__restrict__ u_el,
+                                    const int *__restrict__ u_ptr, const int *__restrict__ u_g,
+                                    const double *__restrict__ g_w, const double *__restrict__ resid)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    for (int g = 0; g < ng; ++g) {
-        const int el = g_el[g];
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= nu) return;
+    const int el = u_el[u];
+    double a0 = lam[el], a1 = lam[ld + el], a2 = lam[2 * ld + el];
+    for (int j = u_ptr[u]; j < u_ptr[u + 1]; ++j) {
+        const int g = u_g[j];
         const double r2 = 2.0 * resid[g];
-        lam[el] += r2 * g_w[3 * g];
-        lam[ld + el] += r2 * g_w[3 * g + 1];
-        lam[2 * ld + el] += r2 * g_w[3 * g + 2];
+        a0 += r2 * g_w[3 * g];
+        a1 += r2 * g_w[3 * g + 1];
+        a2 += r2 * g_w[3 * g + 2];
     }
+    lam[el] = a0;
+    lam[ld + el] = a1;
+    lam[2 * ld + el] = a2;
 }
 
 /* ==================================================================== tangent ==== */
 
-template <bool WD>
+/* Tangent (T = Dual) or frozen-decision perturbation (T = Pert) of the edge flux: the
+ * "_x" arrays hold the second lane of their primal (tangents or perturbed values). */
+template <bool WD, class T>
 __global__ void __launch_bounds__(256) k_tlm_edge(MeshDev m, const double *__restrict__ S,
-                                                  const double *__restrict__ Sd, const int *__restrict__ wd,
+                                                  const double *__restrict__ Sx, const int *__restrict__ wd,
                                                   const double *__restrict__ bzeta, const double *__restrict__ bqn,
-                                                  const double *__restrict__ zd, double *__restrict__ flux,
-                                                  double *__restrict__ flux_d, double g)
+                                                  const double *__restrict__ zx, double *__restrict__ flux,
+                                                  double *__restrict__ flux_x, double g)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.nf) return;
+    const T *tag = nullptr;
     const int el_in = m.e_in[i], el_ex = m.e_ex[i], info = m.e_info[i];
     const int k_in = info & 3, k_ex = (info >> 2) & 3, bd = (info >> 4) & 7;
     const double nx = m.e_geo[i], ny = m.e_geo[m.ldF + i];
     const int ld = m.ldE;
     int va, vb;
     edge_vertices(m, el_in, k_in, va, vb);
-    const Dual z_edge(m.e_geo[2 * m.ldF + i], 0.5 * (zd[va] + zd[vb]));
-    const auto st = [S, Sd, ld](int plane, int el) { return Dual(S[plane * ld + el], Sd[plane * ld + el]); };
-    const Dual zi = st(k_in, el_in), qxi = st(3 + k_in, el_in), qyi = st(6 + k_in, el_in);
-    Dual ze, qxe, qye;
+    const T z_edge = lane(tag, m.e_geo[2 * m.ldF + i], 0.5 * (zx[va] + zx[vb]));
+    const auto st = [S, Sx, ld, tag](int plane, int el) { return lane(tag, S[plane * ld + el], Sx[plane * ld + el]); };
+    const T zi = st(k_in, el_in), qxi = st(3 + k_in, el_in), qyi = st(6 + k_in, el_in);
+    T ze, qxe, qye;
     if (bd)
-        ghost_state<Dual>(bd, nx, ny, zi, qxi, qyi, bzeta[i], bqn[i], Dual(0.0), ze, qxe, qye);
+        ghost_state<T>(bd, nx, ny, zi, qxi, qyi, bzeta[i], bqn[i], T(0.0), ze, qxe, qye);
     else if (el_in == el_ex)
-        ghost_state<Dual>(0, nx, ny, zi, qxi, qyi, 0.0, 0.0, st(k_ex, el_ex), ze, qxe, qye);
+        ghost_state<T>(0, nx, ny, zi, qxi, qyi, 0.0, 0.0, st(k_ex, el_ex), ze, qxe, qye);
     else {
         ze = st(k_ex, el_ex);
         qxe = st(3 + k_ex, el_ex);
         qye = st(6 + k_ex, el_ex);
     }
     const int wdi = WD ? wd[el_in] : 1, wde = WD ? wd[el_ex] : 1;
-    Dual fin[3], fex[3];
+    T fin[3], fex[3];
     int code;
-    flux_core<Dual, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code);
+    flux_core<T, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code);
     const int lf = m.ldF;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        flux[k * lf + i] = fin[k].v;
-        flux_d[k * lf + i] = fin[k].d;
-        flux[(3 + k) * lf + i] = fex[k].v;
-        flux_d[(3 + k) * lf + i] = fex[k].d;
+        flux[k * lf + i] = val(fin[k]);
+        flux_x[k * lf + i] = second(fin[k]);
+        flux[(3 + k) * lf + i] = val(fex[k]);
+        flux_x[(3 + k) * lf + i] = second(fex[k]);
     }
 }
 
-template <int MODE>
+template <int MODE, class T>
 __global__ void __launch_bounds__(128) k_tlm_element(MeshDev m, const double *__restrict__ S,
-                                                     const double *__restrict__ Sd, const double *U,
-                                                     const double *Ud, const int *__restrict__ wd,
+                                                     const double *__restrict__ Sx, const double *U,
+                                                     const double *Ux, const int *__restrict__ wd,
                                                      const double *__restrict__ flux,
-                                                     const double *__restrict__ flux_d,
-                                                     const double *__restrict__ zd, const double *__restrict__ n_el,
-                                                     const double *__restrict__ neld, double *out, double *out_d,
-                                                     double *__restrict__ avg, double *__restrict__ avg_d,
+                                                     const double *__restrict__ flux_x,
+                                                     const double *__restrict__ zx, const double *__restrict__ n_el,
+                                                     const double *__restrict__ nelx, double *out, double *out_x,
+                                                     double *__restrict__ avg, double *__restrict__ avg_x,
                                                      const DevClock *clk, double g, const double *dt_hist, int n)
 {
     const int el = blockIdx.x * blockDim.x + threadIdx.x;
     if (el >= m.ne) return;
+    const T *tag = nullptr;
     const int ld = m.ldE;
     const double *G = m.geo + el;
-    Dual F[3][3];
+    T F[3][3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const int ee = m.elem_edge[k * ld + el];
         const int e = ee >> 1, side = ee & 1;
 #pragma unroll
         for (int v = 0; v < 3; ++v) {
-            const Dual f(flux[(3 * side + v) * m.ldF + e], flux_d[(3 * side + v) * m.ldF + e]);
+            const T f = lane(tag, flux[(3 * side + v) * m.ldF + e], flux_x[(3 * side + v) * m.ldF + e]);
             F[v][k] = side ? -f : f;
         }
     }
-    Dual zr[3], qxr[3], qyr[3];
+    T zr[3], qxr[3], qyr[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        zr[k] = Dual(S[k * ld + el], Sd[k * ld + el]);
-        qxr[k] = Dual(S[(3 + k) * ld + el], Sd[(3 + k) * ld + el]);
-        qyr[k] = Dual(S[(6 + k) * ld + el], Sd[(6 + k) * ld + el]);
+        zr[k] = lane(tag, S[k * ld + el], Sx[k * ld + el]);
+        qxr[k] = lane(tag, S[(3 + k) * ld + el], Sx[(3 + k) * ld + el]);
+        qyr[k] = lane(tag, S[(6 + k) * ld + el], Sx[(6 + k) * ld + el]);
     }
     const double local_g = (wd[el] == 0) ? 0.0 : g;
     const auto geo = [G, ld](int j) { return G[(size_t)j * ld]; };
-    const double zvd[3] = {zd[m.el2v[el]], zd[m.el2v[ld + el]], zd[m.el2v[2 * ld + el]]};
-    const DualZGeo zg = dual_zgeo(geo, zvd, n_el ? n_el[el] : -1.0, neld ? neld[el] : 0.0, g);
-    const auto uin = [U, Ud, ld, el](int v, int k) {
-        return Dual(U[(3 * v + k) * ld + el], Ud[(3 * v + k) * ld + el]);
+    const double zvx[3] = {zx[m.el2v[el]], zx[m.el2v[ld + el]], zx[m.el2v[2 * ld + el]]};
+    const LaneZGeo<T> zg = lane_zgeo<T>(geo, zvx, n_el ? n_el[el] : -1.0, nelx ? nelx[el] : 0.0, g);
+    const auto uin = [U, Ux, ld, el, tag](int v, int k) {
+        return lane(tag, U[(3 * v + k) * ld + el], Ux[(3 * v + k) * ld + el]);
     };
-    Dual w[3][3], a[3];
-    element_core<MODE, Dual>(F, zr, qxr, qyr, geo, zg, uin, local_g, clk->rain, dt_hist[n], w, a);
+    T w[3][3], a[3];
+    element_core<MODE, T>(F, zr, qxr, qyr, geo, zg, uin, local_g, clk->rain, dt_hist[n], w, a);
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            out[(3 * v + k) * ld + el] = w[v][k].v;
-            out_d[(3 * v + k) * ld + el] = w[v][k].d;
+            out[(3 * v + k) * ld + el] = val(w[v][k]);
+            out_x[(3 * v + k) * ld + el] = second(w[v][k]);
         }
-        avg[v * ld + el] = a[v].v;
-        avg_d[v * ld + el] = a[v].d;
+        avg[v * ld + el] = val(a[v]);
+        avg_x[v * ld + el] = second(a[v]);
     }
 }
 
@@ -322,40 +353,42 @@ static __global__ void __launch_bounds__(256) k_tlm_node(MeshDev m, const double
     }
 }
 
-template <bool WD>
-__global__ void __launch_bounds__(128) k_tlm_limit(MeshDev m, double *__restrict__ S, double *__restrict__ Sd,
+template <bool WD, class T>
+__global__ void __launch_bounds__(128) k_tlm_limit(MeshDev m, double *__restrict__ S, double *__restrict__ Sx,
                                                    const double *__restrict__ bounds,
-                                                   const double *__restrict__ bounds_d,
-                                                   const double *__restrict__ zd, const int *__restrict__ wd_in,
+                                                   const double *__restrict__ bounds_x,
+                                                   const double *__restrict__ zx, const int *__restrict__ wd_in,
                                                    int *__restrict__ wd_out, double h0, double velzero)
 {
     const int el = blockIdx.x * blockDim.x + threadIdx.x;
     if (el >= m.ne) return;
+    const T *tag = nullptr;
     const int ld = m.ldE;
     const int nd[3] = {m.el2v[el], m.el2v[ld + el], m.el2v[2 * ld + el]};
-    const Dual zn[3] = {Dual(m.zn[nd[0]], zd[nd[0]]), Dual(m.zn[nd[1]], zd[nd[1]]), Dual(m.zn[nd[2]], zd[nd[2]])};
-    Dual w[3][3];
+    const T zn[3] = {lane(tag, m.zn[nd[0]], zx[nd[0]]), lane(tag, m.zn[nd[1]], zx[nd[1]]),
+                     lane(tag, m.zn[nd[2]], zx[nd[2]])};
+    T w[3][3];
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) w[v][k] = Dual(S[(3 * v + k) * ld + el], Sd[(3 * v + k) * ld + el]);
+        for (int k = 0; k < 3; ++k) w[v][k] = lane(tag, S[(3 * v + k) * ld + el], Sx[(3 * v + k) * ld + el]);
     const int lb = m.ldN;
-    const auto bnd = [bounds, bounds_d, lb, &nd](int v, int k, int is_min) {
+    const auto bnd = [bounds, bounds_x, lb, &nd, tag](int v, int k, int is_min) {
         const int idx = (3 * is_min + v) * lb + nd[k];
-        return Dual(bounds[idx], bounds_d[idx]);
+        return lane(tag, bounds[idx], bounds_x[idx]);
     };
     LimitDecisions dec;
-    limit_core<true, WD, Dual>(w, bnd, zn, h0, velzero, dec);
+    limit_core<true, WD, T>(w, bnd, zn, h0, velzero, dec);
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            S[(3 * v + k) * ld + el] = w[v][k].v;
-            Sd[(3 * v + k) * ld + el] = w[v][k].d;
+            S[(3 * v + k) * ld + el] = val(w[v][k]);
+            Sx[(3 * v + k) * ld + el] = second(w[v][k]);
         }
     if (WD) {
-        const double w0[3] = {w[0][0].v, w[0][1].v, w[0][2].v};
-        const double znv[3] = {zn[0].v, zn[1].v, zn[2].v};
+        const double w0[3] = {val(w[0][0]), val(w[0][1]), val(w[0][2])};
+        const double znv[3] = {val(zn[0]), val(zn[1]), val(zn[2])};
         wd_out[el] = wd_status(w0, znv, wd_in[el], h0);
     }
 }
@@ -364,7 +397,7 @@ __global__ void __launch_bounds__(128) k_tlm_limit(MeshDev m, double *__restrict
 
 /* limiter + PDop reverse of one element */
 template <bool WD>
-__global__ void __launch_bounds__(128) k_adj_limit(MeshDev m, const double *__restrict__ R,
+__global__ void __launch_bounds__(128, DGR_ADJ_MINB_LIMIT) k_adj_limit(MeshDev m, const double *__restrict__ R,
                                                    const double *__restrict__ bounds,
                                                    const double *__restrict__ lamO, double *__restrict__ Rbar,
                                                    double *__restrict__ bbar, double *__restrict__ zvb, double h0,
@@ -443,7 +476,7 @@ static __global__ void __launch_bounds__(256) k_adj_node(MeshDev m, const double
  * stage 1: lamS += adjoint of the stage input), the per-edge-side flux adjoints and the
  * depth / Manning adjoints */
 template <int MODE>
-__global__ void __launch_bounds__(128) k_adj_element(MeshDev m, const double *__restrict__ S,
+__global__ void __launch_bounds__(128, DGR_ADJ_MINB_ELEMENT) k_adj_element(MeshDev m, const double *__restrict__ S,
                                                      const int *__restrict__ wd, const double *__restrict__ Rbar,
                                                      const double *__restrict__ bnode, const int *__restrict__ barg,
                                                      double *lamS, double *lamU, double *__restrict__ fbar,
@@ -510,7 +543,7 @@ __global__ void __launch_bounds__(128) k_adj_element(MeshDev m, const double *__
 /* edge reverse: Roe flux(es), ghost states; adds the trace adjoints into the slots of the
  * adjacent elements (each slot belongs to one edge side) and the mid-edge depth adjoint */
 template <bool WD>
-__global__ void __launch_bounds__(256) k_adj_edge(MeshDev m, const double *__restrict__ S, const int *__restrict__ wd,
+__global__ void __launch_bounds__(256, DGR_ADJ_MINB_EDGE) k_adj_edge(MeshDev m, const double *__restrict__ S, const int *__restrict__ wd,
                                                   const double *__restrict__ bzeta, const double *__restrict__ bqn,
                                                   const double *__restrict__ fbar, double *__restrict__ lamS,
                                                   double *__restrict__ zeb, double g)

@@ -147,6 +147,7 @@ SIGNATURES = [
      [C.c_void_p, dptr, dptr, dptr, iptr, C.c_double, C.c_double, C.c_int, dptr, dptr]),
     ("dgr_adjoint_backward", C.c_int, [C.c_void_p, dptr, dptr, dptr, dptr, dptr]),
     ("dgr_tlm", C.c_int, [C.c_void_p, dptr, dptr, dptr, iptr, dptr, dptr, dptr, dptr, dptr, dptr, dptr]),
+    ("dgr_fd_frozen", C.c_int, [C.c_void_p, dptr, dptr, dptr, iptr, dptr, dptr, dptr, dptr, dptr, dptr, dptr]),
     ("dgr_adjoint_dt", C.c_int, [C.c_void_p, dptr, dptr]),
     ("dgr_adjoint_timing", C.c_int, [C.c_void_p, dptr, dptr, dptr]),
     ("dgr_set_bathymetry", C.c_int, [C.c_void_p, dptr]),

@@ -138,6 +138,19 @@ class GaugeMisfit:
                                              C.byref(J), C.byref(dJ)), "dgr_tlm")
         return J.value, dJ.value
 
+    def frozen(self, state, n_el=None, z=None, state_p=None):
+        """(J, J_p): J at the recorded point and J_p at the perturbed point (n_el, z, state_p;
+        None = unperturbed) with the recorded run's decisions and dt sequence frozen."""
+        zz, x, y, wd = self._state(state)
+        opt = lambda a: None if a is None else _dp(np.ascontiguousarray(a, dtype=np.float64))  # noqa: E731
+        keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                for a in ((state_p or (None, None, None))[:3] + (n_el, z))]
+        J, Jp = C.c_double(), C.c_double()
+        self.solver._status(self.lib.dgr_fd_frozen(self.solver.ctx, _dp(zz), _dp(x), _dp(y), _ip(wd),
+                                                   *[opt(a) for a in keep], C.byref(J), C.byref(Jp)),
+                            "dgr_fd_frozen")
+        return J.value, Jp.value
+
     def dt_history(self):
         dt = np.empty(self.nsteps)
         t = np.empty(self.nsteps)

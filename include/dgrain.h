@@ -303,6 +303,13 @@ DGR_API int dgr_adjoint_backward(dgr_ctx *ctx, double *grad_n_el, double *grad_z
 DGR_API int dgr_tlm(dgr_ctx *ctx, const double *zeta, const double *Qx, const double *Qy, const int *WD,
                     const double *dzeta0, const double *dQx0, const double *dQy0, const double *dn_el,
                     const double *dz, double *J, double *dJ);
+/* The recorded run at a perturbed point (state *_p, per-element n n_el_p, node depths z_p;
+ * NULL = unperturbed) with every decision and the dt sequence frozen at the recorded run's:
+ * J of the base point and J_p of the perturbed one.  Central differences of J_p are
+ * "finite differences with frozen masks and dt", the derivative the adjoint computes. */
+DGR_API int dgr_fd_frozen(dgr_ctx *ctx, const double *zeta, const double *Qx, const double *Qy, const int *WD,
+                          const double *zeta_p, const double *Qx_p, const double *Qy_p, const double *n_el_p,
+                          const double *z_p, double *J, double *J_p);
 /* dt and boundary-value time of every step of the last forward run [nsteps]. */
 DGR_API int dgr_adjoint_dt(dgr_ctx *ctx, double *dt, double *time);
 /* Device time in ms of the last forward, backward and tangent-linear runs. */
