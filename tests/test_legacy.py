@@ -1,0 +1,72 @@
+"""The link-level drop-in: the reference's own program (2DCode main.c, time_evolution.c,
+initialize.c, boundary_conditions.c, extract_mesh_attributes.c, mathfunctions.c, all
+unmodified) linked with the GPU shim dg-rain_b200/csrc/dgr_legacy.c in place of the
+reference's operator files, against the same program built entirely from the reference
+(oracle/Makefile: _ref/Simulation_gpu and _ref/Simulation).
+
+Both read a fort.14 from disk and FinalTime from stdin, print dt and time every step and
+write the .dat files of time_evolution.c:324-390; those outputs are compared."""
+from __future__ import annotations
+
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import has_gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.path.join(HERE, "..", "oracle", "_ref")
+BIN_REF = os.path.join(REF, "Simulation")
+BIN_GPU = os.path.join(REF, "Simulation_gpu")
+
+needs_bins = pytest.mark.skipif(not (os.path.exists(BIN_REF) and os.path.exists(BIN_GPU)),
+                                reason="reference programs not built (oracle/Makefile needs the reference tree)")
+
+
+def run(binary, workdir, final_time):
+    r = subprocess.run([binary, "fort.14"], cwd=workdir, input=f"{final_time}\n", capture_output=True, text=True,
+                       timeout=600)
+    return r.returncode, r.stdout
+
+
+def write_mesh(dgrain, path, manning):
+    m = dgrain.rectangle(24, 12, jitter=0.15, seed=5, datum=7.0, manning=manning)
+    dgrain.write_fort14(m, str(path))
+    return m
+
+
+@needs_bins
+@pytest.mark.skipif(has_gpu(), reason="checks the behaviour without a GPU")
+def test_legacy_program_fails_loudly_without_gpu(dgrain, tmp_path):
+    write_mesh(dgrain, tmp_path / "fort.14", 0.03)
+    rc, out = run(BIN_GPU, tmp_path, 10.0)
+    assert rc != 0 and "no CUDA device" in out
+
+
+@needs_bins
+@pytest.mark.gpu
+@pytest.mark.parametrize("manning", [0.0, 0.03])
+def test_legacy_program_matches_reference_program(dgrain, tmp_path, manning):
+    """Same dt sequence (as printed) and the same .dat output: identical text with Manning
+    n = 0; within 1e-11 of each field's max with friction (pow(H, 4/3) is correctly rounded
+    on the GPU, glibc's pow is not always)."""
+    outs = {}
+    for name, binary in (("ref", BIN_REF), ("gpu", BIN_GPU)):
+        d = tmp_path / name
+        d.mkdir()
+        write_mesh(dgrain, d / "fort.14", manning)
+        rc, out = run(binary, d, 150.0)
+        assert rc == 0, out[-2000:]
+        outs[name] = (d, out)
+    lines = {k: [ln for ln in v[1].splitlines() if ln.startswith(("dt =", "time ="))] for k, v in outs.items()}
+    assert len(lines["ref"]) > 100 and lines["gpu"] == lines["ref"]
+    for f in ("000_zeta", "001_H", "001_Qx", "001_Qy"):
+        a = (outs["ref"][0] / f"{f}.dat").read_text()
+        b = (outs["gpu"][0] / f"{f}.dat").read_text()
+        if manning == 0.0:
+            assert a == b, f
+        else:
+            x, y = np.loadtxt(outs["ref"][0] / f"{f}.dat"), np.loadtxt(outs["gpu"][0] / f"{f}.dat")
+            assert np.abs(x - y).max() <= 1e-11 * max(np.abs(x).max(), 1e-300), f
