@@ -34,6 +34,7 @@ namespace dgr {
 
 struct AdjointState {
     int nsteps = 0, K = 0, nseg = 0, ng = 0, nu = 0;
+    int ns = 2; /* RK stages the storage was laid out for */
     int have_forward = 0;
     int *g_el = nullptr, *u_el = nullptr, *u_ptr = nullptr, *u_g = nullptr; /* gauges; per gauge element */
     double *g_w = nullptr, *target = nullptr, *resid = nullptr, *sums = nullptr;
@@ -73,15 +74,21 @@ void adjoint_release(dgr_ctx *c)
 /* ------------------------------------------------------------- storage layout ---- */
 
 static size_t plane9(const dgr_ctx *c) { return (size_t)9 * c->ldE; }
+/* segment store, per step slot j: the step input u^n (seg_U), the inputs of stages 1..ns-1
+ * (seg_W(j, s-1)), and per stage s the pre-limiter output, element means, node bounds and
+ * input wet/dry flags */
 static double *seg_U(const dgr_ctx *c, int j) { return c->adj->segU + (size_t)j * plane9(c); }
-static double *seg_W(const dgr_ctx *c, int j) { return c->adj->segW + (size_t)j * plane9(c); }
-static double *seg_R(const dgr_ctx *c, int j, int s) { return c->adj->segR + (size_t)(2 * j + s) * plane9(c); }
-static double *seg_avg(const dgr_ctx *c, int j, int s)
+static double *seg_W(const dgr_ctx *c, int j, int s)
 {
-    return c->adj->segAvg + (size_t)(2 * j + s) * 3 * c->ldE;
+    return c->adj->segW + ((size_t)j * (c->adj->ns - 1) + s) * plane9(c);
 }
-static double *seg_B(const dgr_ctx *c, int j, int s) { return c->adj->segB + (size_t)(2 * j + s) * 6 * c->ldN; }
-static int *seg_wd(const dgr_ctx *c, int j, int s) { return c->adj->segWd + (size_t)(2 * j + s) * c->ne; }
+static size_t seg_slot(const dgr_ctx *c, int j, int s) { return (size_t)j * c->adj->ns + s; }
+static double *seg_R(const dgr_ctx *c, int j, int s) { return c->adj->segR + seg_slot(c, j, s) * plane9(c); }
+static double *seg_avg(const dgr_ctx *c, int j, int s) { return c->adj->segAvg + seg_slot(c, j, s) * 3 * c->ldE; }
+static double *seg_B(const dgr_ctx *c, int j, int s) { return c->adj->segB + seg_slot(c, j, s) * 6 * c->ldN; }
+static int *seg_wd(const dgr_ctx *c, int j, int s) { return c->adj->segWd + seg_slot(c, j, s) * c->ne; }
+/* adjoint of the input of stage s >= 1 */
+static double *lam_stage(const dgr_ctx *c, int s) { return c->adj->lamW + (size_t)(s - 1) * plane9(c); }
 
 extern "C" int dgr_adjoint_setup(dgr_ctx *c, int nsteps, int ckpt_every, int ngauges, const int *gauge_el,
                                  const double *gauge_w, const double *target)
@@ -138,14 +145,15 @@ extern "C" int dgr_adjoint_setup(dgr_ctx *c, int nsteps, int ckpt_every, int nga
     AL(a->ckU, (size_t)a->nseg * 9 * E);
     AL(a->ckWd, (size_t)a->nseg * c->ne);
     AL(a->ckClk, a->nseg);
+    const size_t S = a->ns = c->p.rk_stages;
     AL(a->segU, K * 9 * E);
-    AL(a->segW, K * 9 * E);
-    AL(a->segR, K * 2 * 9 * E);
-    AL(a->segAvg, K * 2 * 3 * E);
-    AL(a->segB, K * 2 * 6 * N);
-    AL(a->segWd, K * 2 * c->ne);
+    AL(a->segW, K * (S - 1) * 9 * E);
+    AL(a->segR, K * S * 9 * E);
+    AL(a->segAvg, K * S * 3 * E);
+    AL(a->segB, K * S * 6 * N);
+    AL(a->segWd, K * S * c->ne);
     AL(a->lamU, 9 * E);
-    AL(a->lamW, 9 * E);
+    AL(a->lamW, (S - 1) * 9 * E);
     AL(a->Rbar, 9 * E);
     AL(a->bbar, 18 * E);
     AL(a->bnode, 6 * N);
@@ -230,6 +238,7 @@ extern "C" int dgr_adjoint_forward(dgr_ctx *c, const double *zeta, const double 
     if (!c || !c->adj || !zeta || !Qx || !Qy || !WD) return DGR_ERR_INVALID;
     AdjointState *a = c->adj;
     if (replay_dt && !a->have_forward) return DGR_ERR_INVALID;
+    if (c->p.rk_stages != a->ns) return DGR_ERR_INVALID; /* storage laid out for another scheme */
     CK(cudaSetDevice(c->device));
     int r = dgr_upload_state(c, zeta, Qx, Qy, WD);
     if (r) return r;
@@ -248,8 +257,7 @@ extern "C" int dgr_adjoint_forward(dgr_ctx *c, const double *zeta, const double 
             CK(cudaMemcpyAsync(a->ckClk + sg, c->clk, sizeof(DevClock), cudaMemcpyDeviceToDevice, s));
         }
         clock_begin_step(c, n, replay_dt);
-        launch_stage(c, 0, true);
-        launch_stage(c, 1, true);
+        for (int st = 0; st < c->p.rk_stages; ++st) launch_stage(c, st, true);
         k_clock_end<<<1, 32, 0, s>>>(c->clk, 1);
         k_misfit<<<1, 32, 0, s>>>(c->U, c->ldE, a->ng, a->g_el, a->g_w, a->target + (size_t)n * a->ng,
                                   a->resid + (size_t)n * a->ng);
@@ -267,7 +275,7 @@ extern "C" int dgr_adjoint_forward(dgr_ctx *c, const double *zeta, const double 
     a->fwd_ms = ms;
     if (c->p.wet_dry) {
         c->wd_fresh = 1;
-        c->wd_cur_is_B = 1;
+        c->wd_stepped = 1;
     }
     r = first_error(c);
     if (r) return r;
@@ -306,56 +314,71 @@ static void recorded_stage(dgr_ctx *c, int j, int stage, const double *S, double
     const MeshDev m = mesh_dev(c);
     cudaStream_t s = c->stream;
     const bool wd = c->p.wet_dry != 0;
+    const int mode = stage_io(c, stage).mode;
     double *R = seg_R(c, j, stage), *avg = seg_avg(c, j, stage), *bnd = seg_B(c, j, stage);
+    const double *U = seg_U(c, j);
     if (wd)
         k_edge_flux<true><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, c->flux, c->clk, stage,
                                                              2 * stage, c->p.g);
     else
         k_edge_flux<false><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, c->flux, c->clk,
                                                               stage, 2 * stage, c->p.g);
-    if (stage == 0)
-        k_element<MODE_STAGE1, 128><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, S, wd_in, c->flux, R, avg, c->clk,
-                                                                       c->p.g);
+    const unsigned nb = blocks(c->ne, 128);
+    if (mode == MODE_STAGE1)
+        k_element<MODE_STAGE1, 128><<<nb, 128, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
+    else if (mode == MODE_STAGE2)
+        k_element<MODE_STAGE2, 128><<<nb, 128, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
+    else if (mode == MODE_RK3_2)
+        k_element<MODE_RK3_2, 128><<<nb, 128, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
     else
-        k_element<MODE_STAGE2, 128><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, seg_U(c, j), wd_in, c->flux, R, avg,
-                                                                       c->clk, c->p.g);
+        k_element<MODE_RK3_3, 128><<<nb, 128, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
     k_node_bounds<<<blocks(c->nn, 256), 256, 0, s>>>(m, avg, bnd);
     if (wd)
-        k_limit_to<true><<<blocks(c->ne, 128), 128, 0, s>>>(m, R, OUT, bnd, wd_in, wd_out, c->clk, c->p.H0,
-                                                            c->p.VELZERO, 2 * stage + 1);
+        k_limit_to<true><<<nb, 128, 0, s>>>(m, R, OUT, bnd, wd_in, wd_out, c->clk, c->p.H0, c->p.VELZERO,
+                                            2 * stage + 1);
     else
-        k_limit_to<false><<<blocks(c->ne, 128), 128, 0, s>>>(m, R, OUT, bnd, wd_in, wd_out, c->clk, c->p.H0,
-                                                             c->p.VELZERO, 2 * stage + 1);
+        k_limit_to<false><<<nb, 128, 0, s>>>(m, R, OUT, bnd, wd_in, wd_out, c->clk, c->p.H0, c->p.VELZERO,
+                                             2 * stage + 1);
     c->launches += 4;
 }
 
-/* reverse of one stage of step n (slot j): lamO is the adjoint of the stage output */
+/* reverse of one stage of step n (slot j).  The adjoint of the stage output is lamU for the
+ * last stage, else the adjoint of the next stage's input; the stage input's adjoint goes to
+ * lamU (stage 0) or lam_stage(stage). */
 static void reverse_stage(dgr_ctx *c, int j, int n, int stage)
 {
     AdjointState *a = c->adj;
     const MeshDev m = mesh_dev(c);
     cudaStream_t s = c->stream;
     const bool wd = c->p.wet_dry != 0;
-    const double *S = stage == 0 ? seg_U(c, j) : seg_W(c, j);
+    const int ns = a->ns;
+    const int mode = stage_io(c, stage).mode;
+    const double *S = stage == 0 ? seg_U(c, j) : seg_W(c, j, stage - 1);
     const int *wd_in = seg_wd(c, j, stage);
-    double *lamO = stage == 0 ? a->lamW : a->lamU;
-    double *lamS = stage == 0 ? a->lamU : a->lamW;
+    double *lamO = stage == ns - 1 ? a->lamU : lam_stage(c, stage + 1);
+    double *lamS = stage == 0 ? a->lamU : lam_stage(c, stage);
+    const int u_acc = stage < ns - 1 ? 1 : 0;
     const double h0 = c->p.H0, vz = c->p.VELZERO, g = c->p.g;
+    const unsigned nb = blocks(c->ne, 128);
     if (wd)
-        k_adj_limit<true><<<blocks(c->ne, 128), 128, 0, s>>>(m, seg_R(c, j, stage), seg_B(c, j, stage), lamO, a->Rbar,
-                                                             a->bbar, a->zvb, h0, vz);
+        k_adj_limit<true><<<nb, 128, 0, s>>>(m, seg_R(c, j, stage), seg_B(c, j, stage), lamO, a->Rbar, a->bbar, a->zvb,
+                                             h0, vz);
     else
-        k_adj_limit<false><<<blocks(c->ne, 128), 128, 0, s>>>(m, seg_R(c, j, stage), seg_B(c, j, stage), lamO,
-                                                              a->Rbar, a->bbar, a->zvb, h0, vz);
+        k_adj_limit<false><<<nb, 128, 0, s>>>(m, seg_R(c, j, stage), seg_B(c, j, stage), lamO, a->Rbar, a->bbar,
+                                              a->zvb, h0, vz);
     k_adj_node<<<blocks(c->nn, 256), 256, 0, s>>>(m, seg_avg(c, j, stage), a->bbar, a->bnode, a->barg);
-    if (stage == 1)
-        k_adj_element<MODE_STAGE2><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, wd_in, a->Rbar, a->bnode, a->barg, lamS,
-                                                                      a->lamU, a->fbar, a->zvb, a->nbar, c->n_el, g,
-                                                                      a->dt_hist, n);
+#define ADJ_EL(MD)                                                                                                 \
+    k_adj_element<MD><<<nb, 128, 0, s>>>(m, S, wd_in, a->Rbar, a->bnode, a->barg, lamS, a->lamU, u_acc, a->fbar,   \
+                                         a->zvb, a->nbar, c->n_el, g, a->dt_hist, n)
+    if (mode == MODE_STAGE1)
+        ADJ_EL(MODE_STAGE1);
+    else if (mode == MODE_STAGE2)
+        ADJ_EL(MODE_STAGE2);
+    else if (mode == MODE_RK3_2)
+        ADJ_EL(MODE_RK3_2);
     else
-        k_adj_element<MODE_STAGE1><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, wd_in, a->Rbar, a->bnode, a->barg, lamS,
-                                                                      a->lamU, a->fbar, a->zvb, a->nbar, c->n_el, g,
-                                                                      a->dt_hist, n);
+        ADJ_EL(MODE_RK3_3);
+#undef ADJ_EL
     if (wd)
         k_adj_edge<true><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, a->fbar, lamS, a->zeb, g);
     else
@@ -405,12 +428,16 @@ extern "C" int dgr_adjoint_backward(dgr_ctx *c, double *grad_n_el, double *grad_
         CK(cudaMemcpyAsync(seg_wd(c, 0, 0), a->ckWd + (size_t)sg * c->ne, (size_t)c->ne * 4,
                            cudaMemcpyDeviceToDevice, s));
         CK(cudaMemcpyAsync(c->clk, a->ckClk + sg, sizeof(DevClock), cudaMemcpyDeviceToDevice, s));
+        const int ns = a->ns;
         for (int j = 0; j < len; ++j) {
             clock_begin_step(c, n0 + j, 1);
-            recorded_stage(c, j, 0, seg_U(c, j), seg_W(c, j), seg_wd(c, j, 0), seg_wd(c, j, 1));
             const bool last = j + 1 == len;
-            recorded_stage(c, j, 1, seg_W(c, j), last ? c->U : seg_U(c, j + 1), seg_wd(c, j, 1),
-                           last ? c->wdA : seg_wd(c, j + 1, 0));
+            for (int st = 0; st < ns; ++st) {
+                const double *S = st == 0 ? seg_U(c, j) : seg_W(c, j, st - 1);
+                double *OUT = st < ns - 1 ? seg_W(c, j, st) : (last ? c->U : seg_U(c, j + 1));
+                int *wd_out = st < ns - 1 ? seg_wd(c, j, st + 1) : (last ? c->wdA : seg_wd(c, j + 1, 0));
+                recorded_stage(c, j, st, S, OUT, seg_wd(c, j, st), wd_out);
+            }
             k_clock_end<<<1, 32, 0, s>>>(c->clk, 1);
             c->launches += 2;
         }
@@ -423,8 +450,7 @@ extern "C" int dgr_adjoint_backward(dgr_ctx *c, double *grad_n_el, double *grad_
             k_misfit_rev<<<blocks(a->nu, 128), 128, 0, s>>>(a->lamU, c->ldE, a->nu, a->u_el, a->u_ptr, a->u_g, a->g_w,
                                                             a->resid + (size_t)n * a->ng);
             c->launches += 2;
-            reverse_stage(c, j, n, 1);
-            reverse_stage(c, j, n, 0);
+            for (int st = ns - 1; st >= 0; --st) reverse_stage(c, j, n, st);
         }
     }
     k_adj_zfold<<<blocks(c->ne, 256), 256, 0, s>>>(m, a->zeb, a->zvb);
@@ -508,25 +534,33 @@ static int run_lanes(dgr_ctx *c, double *J, double *out2)
         if (c->nbnd)
             k_adj_forcing<<<blocks(c->nbnd, 256), 256, 0, s>>>(c->clk, a->time_hist, n, c->bnd_edges, c->bnd_type,
                                                                c->nbnd, c->bzeta, c->bqn);
-        for (int stage = 0; stage < 2; ++stage) {
-            double *S = stage == 0 ? c->U : c->W, *Sx = stage == 0 ? a->Ud : a->Wd;
-            double *OUT = stage == 0 ? c->W : c->U, *OUTx = stage == 0 ? a->Wd : a->Ud;
-            const int *wd_in = (stage == 0 || !wd) ? c->wdA : c->wdB;
-            int *wd_out = stage == 0 ? c->wdB : c->wdA;
+        for (int stage = 0; stage < a->ns; ++stage) {
+            const StageIO io = stage_io(c, stage);
+            const double *S = io.S;
+            double *OUT = io.OUT;
+            const double *Sx = stage == 0 ? a->Ud : a->Wd;
+            double *OUTx = stage == a->ns - 1 ? a->Ud : a->Wd;
+            const int *wd_in = io.wd_in;
+            int *wd_out = io.wd_out;
             if (wd)
                 k_tlm_edge<true, T><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, Sx, wd_in, c->bzeta, c->bqn, a->zd,
                                                                        c->flux, a->flux_d, g);
             else
                 k_tlm_edge<false, T><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, Sx, wd_in, c->bzeta, c->bqn, a->zd,
                                                                         c->flux, a->flux_d, g);
-            if (stage == 0)
-                k_tlm_element<MODE_STAGE1, T><<<blocks(c->ne, 128), 128, 0, s>>>(
-                    m, S, Sx, c->U, a->Ud, wd_in, c->flux, a->flux_d, a->zd, c->n_el, a->neld, OUT, OUTx, c->avg,
-                    a->avg_d, c->clk, g, a->dt_hist, n);
+#define TLM_EL(MD)                                                                                                 \
+    k_tlm_element<MD, T><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, Sx, c->U, a->Ud, wd_in, c->flux, a->flux_d, a->zd,  \
+                                                            c->n_el, a->neld, OUT, OUTx, c->avg, a->avg_d, c->clk, g, \
+                                                            a->dt_hist, n)
+            if (io.mode == MODE_STAGE1)
+                TLM_EL(MODE_STAGE1);
+            else if (io.mode == MODE_STAGE2)
+                TLM_EL(MODE_STAGE2);
+            else if (io.mode == MODE_RK3_2)
+                TLM_EL(MODE_RK3_2);
             else
-                k_tlm_element<MODE_STAGE2, T><<<blocks(c->ne, 128), 128, 0, s>>>(
-                    m, S, Sx, c->U, a->Ud, wd_in, c->flux, a->flux_d, a->zd, c->n_el, a->neld, OUT, OUTx, c->avg,
-                    a->avg_d, c->clk, g, a->dt_hist, n);
+                TLM_EL(MODE_RK3_3);
+#undef TLM_EL
             k_tlm_node<<<blocks(c->nn, 256), 256, 0, s>>>(m, c->avg, a->avg_d, c->bounds, a->bounds_d);
             if (wd)
                 k_tlm_limit<true, T><<<blocks(c->ne, 128), 128, 0, s>>>(m, OUT, OUTx, c->bounds, a->bounds_d, a->zd,
@@ -540,7 +574,7 @@ static int run_lanes(dgr_ctx *c, double *J, double *out2)
                                   a->rt + (size_t)n * a->ng);
         k_misfit<<<1, 32, 0, s>>>(a->Ud, c->ldE, a->ng, a->g_el, a->g_w,
                                   pert ? a->target + (size_t)n * a->ng : nullptr, a->rd + (size_t)n * a->ng);
-        c->launches += 11;
+        c->launches += 3 + 4 * a->ns;
     }
     k_misfit_sum<<<1, 32, 0, s>>>(a->rt, a->rd, (long long)a->nsteps * a->ng, pert ? 1 : 0, a->sums);
     c->launches++;
@@ -556,7 +590,7 @@ static int run_lanes(dgr_ctx *c, double *J, double *out2)
     if (out2) *out2 = sums[1];
     if (c->p.wet_dry) {
         c->wd_fresh = 1;
-        c->wd_cur_is_B = 1;
+        c->wd_stepped = 1;
     }
     return DGR_OK;
 }

@@ -58,6 +58,7 @@ extern "C" int dgr_params_default(dgr_params *p)
     p->rain = 0.0;
     p->device = 0;
     p->record_decisions = 0;
+    p->rk_stages = 2;
     return DGR_OK;
 }
 
@@ -76,7 +77,7 @@ static void release(dgr_ctx *c)
     void *ptrs[] = {c->x, c->y, c->zn, c->nfric, c->n_el, c->el2v_aos, c->el2v, c->elem_edge, c->e_in,
                     c->e_ex, c->e_info, c->n2e_ptr, c->n2e, c->bnd_edges, c->bnd_type, c->bnd_sid, c->bdry,
                     c->el_sid, c->ed_sid, c->e_geo, c->geo, c->U, c->W, c->flux, c->avg, c->bounds, c->bzeta,
-                    c->bqn, c->bstage, c->wdA, c->wdB, c->dec, c->bar, c->clk};
+                    c->bqn, c->bstage, c->wdA, c->wdB, c->wdC, c->dec, c->bar, c->clk};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     adjoint_release(c);
@@ -172,6 +173,11 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     else
         dgr_params_default(&c->p);
     c->device = c->p.device;
+    if (c->p.rk_stages == 0) c->p.rk_stages = 2; /* a zero-filled struct means the reference's RK2 */
+    if (c->p.rk_stages != 2 && c->p.rk_stages != 3) {
+        delete c;
+        return DGR_ERR_INVALID;
+    }
     c->bs = 128;
     c->fusion = 0;
     if (c->device < 0 || c->device >= ndev) {
@@ -228,7 +234,8 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     TRY(dalloc(&c->bqn, nf));
     TRY(dalloc(&c->wdA, ne));
     TRY(dalloc(&c->wdB, ne));
-    TRY(dalloc(&c->dec, 4 * ne));
+    TRY(dalloc(&c->wdC, ne));
+    TRY(dalloc(&c->dec, 6 * ne));
     TRY(dalloc(&c->bar, 4));
     TRY(dalloc(&c->clk, nscen));
     TRYC(cudaHostAlloc((void **)&c->h_clk, sizeof(DevClock) * nscen, cudaHostAllocDefault));
@@ -257,7 +264,7 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     TRYC(cudaMemsetAsync(c->bqn, 0, nf * 8, s));
     TRYC(cudaMemsetAsync(c->U, 0, 9 * lE * 8, s));
     TRYC(cudaMemsetAsync(c->W, 0, 9 * lE * 8, s));
-    TRYC(cudaMemsetAsync(c->dec, 0, 4 * ne * 4, s));
+    TRYC(cudaMemsetAsync(c->dec, 0, 6 * ne * 4, s));
     TRYC(cudaMemsetAsync(c->bar, 0, 16, s));
 
     /* per-element Manning n of the scenarios that give one (negative: node average) */
@@ -389,8 +396,9 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     std::vector<int> wd(ne, -1);
     TRYC(cudaMemcpy(c->wdA, wd.data(), ne * 4, cudaMemcpyHostToDevice));
     TRYC(cudaMemcpy(c->wdB, wd.data(), ne * 4, cudaMemcpyHostToDevice));
+    TRYC(cudaMemcpy(c->wdC, wd.data(), ne * 4, cudaMemcpyHostToDevice));
     c->wd_fresh = 0;
-    c->wd_cur_is_B = 0;
+    c->wd_stepped = 0;
     *out = c;
     return DGR_OK;
 }
@@ -452,6 +460,16 @@ extern "C" int dgr_set_params(dgr_ctx *c, const dgr_params *p)
     c->p.cfl = p->cfl;
     c->p.dt0 = p->dt0;
     c->p.record_decisions = p->record_decisions;
+    const int stages = p->rk_stages == 0 ? 2 : p->rk_stages;
+    if (stages != 2 && stages != 3) return DGR_ERR_INVALID;
+    if (stages != c->p.rk_stages) {
+        if (c->wd_stepped) /* the current flags sit in the old scheme's after-step buffer */
+            CK(cudaMemcpyAsync(c->wdA, wd_after_step(c), (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->wd_stepped = 0;
+        c->wd_fresh = 0;
+        c->p.rk_stages = stages;
+    }
     if (c->nscen == 1) { /* a single mesh takes its forcing from the run parameters */
         int r = read_clock(c);
         if (r) return r;
@@ -503,10 +521,10 @@ static int upload_slice(dgr_ctx *c, int sc, const double *zeta, const double *Qx
     k_aos_to_planar<<<blocks(n, 256), 256, 0, s>>>(n, c->ldE, st, st + n3, st + 2 * n3, c->U + c->el_off[sc]);
     c->launches++;
     /* the other scenarios' current flags must sit in WA as well before WA is marked current */
-    if (c->wd_cur_is_B && c->nscen > 1)
+    if (c->wd_stepped && c->nscen > 1)
         for (int k = 0; k < c->nscen; ++k)
             if (k != sc)
-                CK(cudaMemcpyAsync(c->wdA + c->el_off[k], c->wdB + c->el_off[k],
+                CK(cudaMemcpyAsync(c->wdA + c->el_off[k], wd_after_step(c) + c->el_off[k],
                                    (size_t)(c->el_off[k + 1] - c->el_off[k]) * 4, cudaMemcpyDeviceToDevice, s));
     if (WD) CK(cudaMemcpyAsync(c->wdA + c->el_off[sc], WD, (size_t)n * 4, cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
@@ -518,7 +536,7 @@ static int upload_slice(dgr_ctx *c, int sc, const double *zeta, const double *Qx
     r = write_clock(c);
     if (r) return r;
     c->wd_fresh = 0;
-    c->wd_cur_is_B = 0;
+    c->wd_stepped = 0;
     return DGR_OK;
 }
 
@@ -536,7 +554,7 @@ static int download_slice(dgr_ctx *c, int sc, double *zeta, double *Qx, double *
     CK(cudaMemcpyAsync(Qx, st + n3, n3 * 8, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(Qy, st + 2 * n3, n3 * 8, cudaMemcpyDeviceToHost, s));
     if (WD)
-        CK(cudaMemcpyAsync(WD, (c->wd_cur_is_B ? c->wdB : c->wdA) + c->el_off[sc], (size_t)n * 4,
+        CK(cudaMemcpyAsync(WD, (c->wd_stepped ? wd_after_step(c) : c->wdA) + c->el_off[sc], (size_t)n * 4,
                            cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return DGR_OK;
@@ -609,7 +627,7 @@ extern "C" int dgr_boundary_conditions(dgr_ctx *c, double time)
 
 /* --------------------------------------------------------------- launches ---- */
 
-static const int *wd_current(const dgr_ctx *c) { return c->wd_cur_is_B ? c->wdB : c->wdA; }
+static const int *wd_current(const dgr_ctx *c) { return c->wd_stepped ? wd_after_step(c) : c->wdA; }
 
 template <int MODE>
 static void launch_element(dgr_ctx *c, const double *S, const int *wd, double *OUT)
@@ -660,26 +678,25 @@ static void launch_edge(dgr_ctx *c, const double *S, const int *wd, int lam_slot
                                                                       lam_slot, phase, c->p.g);
 }
 
-/* one RK stage as four kernels; stage 0 reads U writes W, stage 1 reads W and U writes U */
+/* one RK stage as four kernels (buffers of stage_io) */
 void launch_stage(dgr_ctx *c, int stage, bool count)
 {
     const bool wd = c->p.wet_dry != 0;
-    const double *S = stage == 0 ? c->U : c->W;
-    double *OUT = stage == 0 ? c->W : c->U;
-    const int *wd_in = (stage == 0 || !wd) ? c->wdA : c->wdB;
-    int *wd_out = stage == 0 ? c->wdB : c->wdA;
+    const StageIO io = stage_io(c, stage);
     int *dl = c->p.record_decisions ? c->dec + (size_t)(2 * stage) * c->ne : nullptr;
     int *dp = c->p.record_decisions ? c->dec + (size_t)(2 * stage + 1) * c->ne : nullptr;
-    launch_edge(c, S, wd_in, stage, 2 * stage);
-    if (stage == 0)
-        launch_element<MODE_STAGE1>(c, S, wd_in, OUT);
-    else
-        launch_element<MODE_STAGE2>(c, S, wd_in, OUT);
+    launch_edge(c, io.S, io.wd_in, stage, 2 * stage);
+    switch (io.mode) {
+    case MODE_STAGE1: launch_element<MODE_STAGE1>(c, io.S, io.wd_in, io.OUT); break;
+    case MODE_STAGE2: launch_element<MODE_STAGE2>(c, io.S, io.wd_in, io.OUT); break;
+    case MODE_RK3_2: launch_element<MODE_RK3_2>(c, io.S, io.wd_in, io.OUT); break;
+    default: launch_element<MODE_RK3_3>(c, io.S, io.wd_in, io.OUT);
+    }
     k_node_bounds<<<blocks(c->nn, 256), 256, 0, c->stream>>>(mesh_dev(c), c->avg, c->bounds);
     if (wd)
-        launch_limit<true, true, true>(c, OUT, wd_in, wd_out, 2 * stage + 1, dl, dp);
+        launch_limit<true, true, true>(c, io.OUT, io.wd_in, io.wd_out, 2 * stage + 1, dl, dp);
     else
-        launch_limit<true, false, false>(c, OUT, wd_in, wd_out, 2 * stage + 1, dl, dp);
+        launch_limit<true, false, false>(c, io.OUT, io.wd_in, io.wd_out, 2 * stage + 1, dl, dp);
     if (count) c->launches += 4;
 }
 
@@ -687,8 +704,8 @@ void launch_wd_refresh(dgr_ctx *c)
 {
     if (c->p.wet_dry && !c->wd_fresh) {
         /* the flags the caller sees (WA after an upload, WB after a step) seed the status */
-        if (c->wd_cur_is_B)
-            cudaMemcpyAsync(c->wdA, c->wdB, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, c->stream);
+        if (c->wd_stepped)
+            cudaMemcpyAsync(c->wdA, wd_after_step(c), (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, c->stream);
         k_wd_status<<<blocks(c->ne, 256), 256, 0, c->stream>>>(mesh_dev(c), c->U, c->wdA, c->clk, c->p.H0);
         c->launches++;
         c->wd_fresh = 1;
@@ -709,6 +726,7 @@ static FusedArgs fused_args(dgr_ctx *c)
     a.bqn = c->bqn;
     a.wdA = c->wdA;
     a.wdB = c->wdB;
+    a.wdC = c->wdC;
     a.clk = c->clk;
     a.nscen = c->nscen;
     a.bnd_edges = c->bnd_edges;
@@ -767,23 +785,27 @@ static cudaError_t launch_step(dgr_ctx *c)
 {
     cudaStream_t s = c->stream;
     const PhysParams p = phys(c);
-    if (c->fusion == 2) return launch_fused(c, 0, 2, 1);
+    const int ns = c->p.rk_stages;
+    if (c->fusion == 2) return launch_fused(c, 0, ns, 1);
     k_clock_begin<<<1, 256, 0, s>>>(c->clk, c->nscen, p, c->bnd_edges, c->bnd_type, c->bnd_sid, c->nbnd, c->bzeta,
                                     c->bqn);
-    if (c->fusion == 1) {
-        cudaError_t e = launch_fused(c, 0, 1, 0);
-        if (e != cudaSuccess) return e;
-        e = launch_fused(c, 1, 2, 0);
-        if (e != cudaSuccess) return e;
-    } else {
-        launch_stage(c, 0, false);
-        launch_stage(c, 1, false);
+    for (int st = 0; st < ns; ++st) {
+        if (c->fusion == 1) {
+            cudaError_t e = launch_fused(c, st, st + 1, 0);
+            if (e != cudaSuccess) return e;
+        } else {
+            launch_stage(c, st, false);
+        }
     }
     k_clock_end<<<blocks(c->nscen, 256), 256, 0, s>>>(c->clk, c->nscen);
     return cudaGetLastError();
 }
 
-static int kernels_per_step(const dgr_ctx *c) { return c->fusion == 2 ? 1 : (c->fusion == 1 ? 4 : 10); }
+static int kernels_per_step(const dgr_ctx *c)
+{
+    const int ns = c->p.rk_stages;
+    return c->fusion == 2 ? 1 : (c->fusion == 1 ? 2 + ns : 2 + 4 * ns);
+}
 
 int decode_err(unsigned long long key, int *code, int *index, int *step)
 {
@@ -826,20 +848,19 @@ extern "C" int dgr_step(dgr_ctx *c, double time, double dt, double *max_lambda)
     k_clock_set<<<1, 1, 0, s>>>(c->clk, time, dt);
     c->launches++;
     launch_wd_refresh(c);
-    launch_stage(c, 0, true);
-    launch_stage(c, 1, true);
+    for (int st = 0; st < c->p.rk_stages; ++st) launch_stage(c, st, true);
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev1, s));
     if (c->p.wet_dry) {
         c->wd_fresh = 1;
-        c->wd_cur_is_B = 1;
+        c->wd_stepped = 1;
     }
     int r = read_clock(c);
     if (r) return r;
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     c->last_ms = ms;
-    if (max_lambda) *max_lambda = bits_to_double(c->h_clk[0].lam_bits[1]);
+    if (max_lambda) *max_lambda = bits_to_double(c->h_clk[0].lam_bits[c->p.rk_stages - 1]);
     return decode_err(c->h_clk[0].err, nullptr, nullptr, nullptr);
 }
 
@@ -932,7 +953,7 @@ extern "C" int dgr_wet_dry_status(dgr_ctx *c)
     if (!c || c->nscen != 1) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
-    int *wd = c->wd_cur_is_B ? c->wdB : c->wdA;
+    int *wd = c->wd_stepped ? wd_after_step(c) : c->wdA;
     k_clock_set<<<1, 1, 0, s>>>(c->clk, 0.0, 0.0);
     k_wd_status<<<blocks(c->ne, 256), 256, 0, s>>>(mesh_dev(c), c->U, wd, c->clk, c->p.H0);
     c->launches += 2;
@@ -1026,7 +1047,7 @@ static int run_impl(dgr_ctx *c, int nsteps, const double *final_time, double *ti
     }
     if (c->p.wet_dry && any_step) {
         c->wd_fresh = 1;
-        c->wd_cur_is_B = 1;
+        c->wd_stepped = 1;
     }
     r = check_barrier(c);
     if (r) return r;
@@ -1096,14 +1117,15 @@ extern "C" int dgr_autotune(dgr_ctx *c, int trial_steps, int *block_size, int *f
     double *saveU = nullptr;
     int *saveWD = nullptr;
     CK(cudaMallocAsync((void **)&saveU, nU * 8, s));
-    CK(cudaMallocAsync((void **)&saveWD, 2 * (size_t)c->ne * 4, s));
+    CK(cudaMallocAsync((void **)&saveWD, 3 * (size_t)c->ne * 4, s));
     CK(cudaMemcpyAsync(saveU, c->U, nU * 8, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(saveWD, c->wdA, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(saveWD + c->ne, c->wdB, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(saveWD + 2 * (size_t)c->ne, c->wdC, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, s));
     int r = read_clock(c);
     if (r) return r;
     const std::vector<DevClock> clk0(c->h_clk, c->h_clk + c->nscen);
-    const int fresh0 = c->wd_fresh, curB0 = c->wd_cur_is_B;
+    const int fresh0 = c->wd_fresh, curB0 = c->wd_stepped;
     const int bss[3] = {64, 128, 256};
     double best = 1e300;
     int best_bs = c->bs, best_f = c->fusion;
@@ -1135,12 +1157,13 @@ extern "C" int dgr_autotune(dgr_ctx *c, int trial_steps, int *block_size, int *f
             CK(cudaMemcpyAsync(c->U, saveU, nU * 8, cudaMemcpyDeviceToDevice, s));
             CK(cudaMemcpyAsync(c->wdA, saveWD, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, s));
             CK(cudaMemcpyAsync(c->wdB, saveWD + c->ne, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(c->wdC, saveWD + 2 * (size_t)c->ne, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, s));
             std::copy(clk0.begin(), clk0.end(), c->h_clk);
             r = write_clock(c);
             if (r) return r;
             CK(cudaMemsetAsync(c->bar, 0, 16, s));
             c->wd_fresh = fresh0;
-            c->wd_cur_is_B = curB0;
+            c->wd_stepped = curB0;
         }
     CK(cudaFreeAsync(saveU, s));
     CK(cudaFreeAsync(saveWD, s));
@@ -1155,7 +1178,7 @@ extern "C" int dgr_autotune(dgr_ctx *c, int trial_steps, int *block_size, int *f
 
 extern "C" int dgr_get_decisions(dgr_ctx *c, int stage, int *limit, int *pdop)
 {
-    if (!c || stage < 0 || stage > 1) return DGR_ERR_INVALID;
+    if (!c || stage < 0 || stage >= c->p.rk_stages) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     const size_t n = (size_t)c->ne;
     if (limit) CK(cudaMemcpyAsync(limit, c->dec + 2 * stage * n, n * 4, cudaMemcpyDeviceToHost, c->stream));
@@ -1205,18 +1228,21 @@ extern "C" int dgr_profile_step(dgr_ctx *c, int nsteps, double *kernel_ms, int n
     int rc = DGR_OK;
     for (int it = 0; it < nsteps && rc == DGR_OK; ++it) {
         launch_wd_refresh(c);
-        for (int stage = 0; stage < 2; ++stage) {
-            const double *S = stage == 0 ? c->U : c->W;
-            double *OUT = stage == 0 ? c->W : c->U;
-            const int *wd_in = (stage == 0 || !wd) ? c->wdA : c->wdB;
-            int *wd_out = stage == 0 ? c->wdB : c->wdA;
+        for (int stage = 0; stage < c->p.rk_stages; ++stage) {
+            const StageIO io = stage_io(c, stage);
+            const double *S = io.S;
+            double *OUT = io.OUT;
+            const int *wd_in = io.wd_in;
+            int *wd_out = io.wd_out;
             cudaEventRecord(ev[0], s);
             launch_edge(c, S, wd_in, stage, 2 * stage);
             cudaEventRecord(ev[1], s);
-            if (stage == 0)
-                launch_element<MODE_STAGE1>(c, S, wd_in, OUT);
-            else
-                launch_element<MODE_STAGE2>(c, S, wd_in, OUT);
+            switch (io.mode) {
+            case MODE_STAGE1: launch_element<MODE_STAGE1>(c, S, wd_in, OUT); break;
+            case MODE_STAGE2: launch_element<MODE_STAGE2>(c, S, wd_in, OUT); break;
+            case MODE_RK3_2: launch_element<MODE_RK3_2>(c, S, wd_in, OUT); break;
+            default: launch_element<MODE_RK3_3>(c, S, wd_in, OUT);
+            }
             cudaEventRecord(ev[2], s);
             k_node_bounds<<<blocks(c->nn, 256), 256, 0, s>>>(mesh_dev(c), c->avg, c->bounds);
             cudaEventRecord(ev[3], s);
@@ -1238,13 +1264,13 @@ extern "C" int dgr_profile_step(dgr_ctx *c, int nsteps, double *kernel_ms, int n
         }
         if (wd) {
             c->wd_fresh = 1;
-            c->wd_cur_is_B = 1;
+            c->wd_stepped = 1;
         }
     }
     for (int i = 0; i < 5; ++i) cudaEventDestroy(ev[i]);
     if (rc) return rc;
     CK(cudaGetLastError());
-    for (int k = 0; k < 4; ++k) kernel_ms[k] = acc[k] / (2.0 * nsteps);
+    for (int k = 0; k < 4; ++k) kernel_ms[k] = acc[k] / ((double)c->p.rk_stages * nsteps);
     return DGR_OK;
 }
 

@@ -68,14 +68,15 @@ struct dgr_ctx {
     double *e_geo, *geo;
     /* state and work */
     double *U, *W, *flux, *avg, *bounds, *bzeta, *bqn, *bstage;
-    int *wdA, *wdB;
-    int *dec; /* [4][ne]: limit s0, pdop s0, limit s1, pdop s1 */
+    int *wdA, *wdB, *wdC; /* wet/dry flags: stage s reads buffer s, writes buffer (s+1) mod stages */
+    int *dec; /* [6][ne]: limit and pdop decisions of stage 0, 1, 2 */
     unsigned *bar;
     dgr::DevClock *clk;
     dgr::DevClock *h_clk; /* pinned mirror [nscen] */
     double *h_stage;
     int wd_fresh;    /* WA already holds the status for the next step */
-    int wd_cur_is_B; /* reference-semantic WD lives in WB */
+    int wd_stepped;  /* reference-semantic WD lives in the last stage's input buffer (WB for
+                        RK2, WC for RK3), not in WA */
     long long launches;
     double last_ms;
     /* schedule of the device loop */
@@ -118,8 +119,37 @@ static inline dgr::PhysParams phys(const dgr_ctx *c)
     q.velzero = c->p.VELZERO;
     q.cfl = c->p.cfl;
     q.dt0 = c->p.dt0;
+    q.stages = c->p.rk_stages;
     return q;
 }
+
+/* Buffers of RK stage `stage`: state in/out, wet/dry flags in/out, element mode.  RK2:
+ * U -> W -> U; RK3: U -> W -> W (in place) -> U.  Flags: stage s reads buffer s and writes
+ * buffer (s+1) mod stages, so WA holds the next step's status after the last stage. */
+struct StageIO {
+    const double *S;
+    double *OUT;
+    const int *wd_in;
+    int *wd_out;
+    int mode;
+};
+
+static inline StageIO stage_io(const dgr_ctx *c, int stage)
+{
+    const int ns = c->p.rk_stages;
+    int *bufs[3] = {c->wdA, c->wdB, c->wdC};
+    StageIO io;
+    io.S = stage == 0 ? c->U : c->W;
+    io.OUT = stage == ns - 1 ? c->U : c->W;
+    io.wd_in = c->p.wet_dry ? bufs[stage] : c->wdA;
+    io.wd_out = bufs[(stage + 1) % ns];
+    io.mode = stage == 0 ? dgr::MODE_STAGE1
+                         : (ns == 2 ? dgr::MODE_STAGE2 : (stage == 1 ? dgr::MODE_RK3_2 : dgr::MODE_RK3_3));
+    return io;
+}
+
+/* flags the reference's WD array holds after a step: the last stage's input */
+static inline int *wd_after_step(const dgr_ctx *c) { return c->p.rk_stages == 3 ? c->wdC : c->wdB; }
 
 
 /* dgr_capi.cu */

@@ -50,12 +50,12 @@ struct DevClock {
     double dt;          /* dt of the step in progress, then of the next step */
     double final_time;
     double bc2_zeta;    /* type-2 boundary elevation of the step in progress */
-    unsigned long long lam_bits[2]; /* max wave speed per stage, bits of a double >= 0 */
+    unsigned long long lam_bits[3]; /* max wave speed per stage, bits of a double >= 0 */
     unsigned long long err;         /* first failure key; ~0 = none */
     int step;           /* steps done in the current run */
     int nsteps;         /* step limit of the current run */
     int done;           /* 1: the run has finished, later kernels do nothing */
-    int dt_pending;     /* 1: dt of the next step is still to be derived from lam_bits[1] */
+    int dt_pending;     /* 1: dt of the next step is still to be derived from the last stage's lam_bits */
     /* per-scenario constants */
     double min_edge;    /* minEdgLength of this scenario's mesh */
     double rain;        /* m/s on the elevation equation (extension) */
@@ -81,6 +81,7 @@ struct MeshDev {
 
 struct PhysParams {
     double g, h0, velzero, cfl, dt0;
+    int stages; /* RK stages per step (2 or 3); the CFL dt follows the last stage's wave speed */
 };
 
 /* ------------------------------------------------------------------ edges ---- */
@@ -364,7 +365,7 @@ DGR_DEV void clock_begin_body(DevClock *clk, int nscen, const PhysParams &p, con
         DevClock *c = clk + s;
         if (c->done) continue;
         if (c->dt_pending) {
-            const double lam = __longlong_as_double((long long)c->lam_bits[1]);
+            const double lam = __longlong_as_double((long long)c->lam_bits[p.stages - 1]);
             double dt = p.cfl * c->min_edge / lam;
             if ((c->time + dt) > c->final_time) dt = c->final_time - c->time;
             c->dt = dt;
@@ -378,6 +379,7 @@ DGR_DEV void clock_begin_body(DevClock *clk, int nscen, const PhysParams &p, con
         c->time = c->time + c->dt;
         c->lam_bits[0] = 0;
         c->lam_bits[1] = 0;
+        c->lam_bits[2] = 0;
     }
     __syncthreads();
     for (int j = threadIdx.x; j < nbnd; j += blockDim.x) {
@@ -430,7 +432,7 @@ static __global__ void k_clock_finish(DevClock *clk, int nscen, PhysParams p)
     if (s >= nscen) return;
     DevClock *c = clk + s;
     if (c->dt_pending) {
-        const double lam = __longlong_as_double((long long)c->lam_bits[1]);
+        const double lam = __longlong_as_double((long long)c->lam_bits[p.stages - 1]);
         double dt = p.cfl * c->min_edge / lam;
         if ((c->time + dt) > c->final_time) dt = c->final_time - c->time;
         c->dt = dt;
@@ -446,6 +448,7 @@ static __global__ void k_clock_set(DevClock *clk, double time, double dt)
     clk->done = 0;
     clk->lam_bits[0] = 0;
     clk->lam_bits[1] = 0;
+    clk->lam_bits[2] = 0;
 }
 
 /* Device-side boundary_conditions() at time t for the stand-alone call. */
@@ -472,7 +475,7 @@ static __global__ void k_forcing(const DevClock *clk, double t, const int *__res
 struct FusedArgs {
     MeshDev m;
     double *U, *W, *flux, *avg, *bounds, *bzeta, *bqn;
-    int *wdA, *wdB;
+    int *wdA, *wdB, *wdC;
     DevClock *clk;
     int nscen;
     const int *bnd_edges, *bnd_type, *bnd_sid;
@@ -535,11 +538,15 @@ __global__ void __launch_bounds__(BS, 512 / BS) k_step_fused(FusedArgs a, int st
     }
     const int stride = gridDim.x * BS;
     const int ne = a.m.ne;
+    const int ns = a.p.stages;
+    int *bufs[3] = {a.wdA, a.wdB, a.wdC};
     for (int stage = stage_begin; stage < stage_end; ++stage) {
+        /* the buffers of stage_io (dgr_internal.cuh) */
         const double *S = stage == 0 ? a.U : a.W;
-        double *OUT = stage == 0 ? a.W : a.U;
-        const int *wd_in = (stage == 0 || !WD) ? a.wdA : a.wdB;
-        int *wd_out = stage == 0 ? a.wdB : a.wdA;
+        double *OUT = stage == ns - 1 ? a.U : a.W;
+        const int *wd_in = WD ? bufs[stage] : a.wdA;
+        int *wd_out = bufs[(stage + 1) % ns];
+        const int mode = stage == 0 ? MODE_STAGE1 : (ns == 2 ? MODE_STAGE2 : (stage == 1 ? MODE_RK3_2 : MODE_RK3_3));
         int *dl = a.dec ? a.dec + (size_t)(2 * stage) * ne : nullptr;
         int *dp = a.dec ? a.dec + (size_t)(2 * stage + 1) * ne : nullptr;
         for (int base = blockIdx.x * BS; base < a.m.nf; base += stride) {
@@ -553,10 +560,14 @@ __global__ void __launch_bounds__(BS, 512 / BS) k_step_fused(FusedArgs a, int st
         }
         if (!grid_barrier(a.bar)) return;
         for (int el = blockIdx.x * BS + threadIdx.x; el < ne; el += stride) {
-            if (stage == 0)
+            if (mode == MODE_STAGE1)
                 element_item<MODE_STAGE1, true>(a.m, S, a.U, wd_in, a.flux, OUT, a.avg, a.clk, a.p.g, el);
-            else
+            else if (mode == MODE_STAGE2)
                 element_item<MODE_STAGE2, true>(a.m, S, a.U, wd_in, a.flux, OUT, a.avg, a.clk, a.p.g, el);
+            else if (mode == MODE_RK3_2)
+                element_item<MODE_RK3_2, true>(a.m, S, a.U, wd_in, a.flux, OUT, a.avg, a.clk, a.p.g, el);
+            else
+                element_item<MODE_RK3_3, true>(a.m, S, a.U, wd_in, a.flux, OUT, a.avg, a.clk, a.p.g, el);
         }
         if (!grid_barrier(a.bar)) return;
         for (int n = blockIdx.x * BS + threadIdx.x; n < a.m.nn; n += stride) node_item<true>(a.m, a.avg, a.bounds, n);

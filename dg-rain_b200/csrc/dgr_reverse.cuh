@@ -294,7 +294,7 @@ DGR_HD void rt0_fit_rev(double ab, double bb, double cb, double M11, double M12,
  * Reverse of element_core.  wb = adjoint of its output w (of the RHS for MODE_RHS).
  * Accumulates: Fb[v][k] (adjoint of the gathered, outward F), Sb[v][k] (stage input; v = 0
  * elevation, 1 Qx, 2 Qy), midzb, gnnb, gradzb (depth and Manning factors).  The adjoint of
- * the stage-2 step input u^n is 0.5 wb, left to the caller.
+ * the step input u^n (cu wb, stage_coefficients) is left to the caller.
  */
 template <int MODE, class Geo, class ZGeoV>
 DGR_HD void element_core_rev(const double wb[3][3], const double zr[3], const double qxr[3], const double qyr[3],
@@ -309,10 +309,11 @@ DGR_HD void element_core_rev(const double wb[3][3], const double zr[3], const do
     const double weight = 1.0 / 6;
     const double m11 = geo(G_M11);
 
-    /* RK combination and the diagonal mass inverse */
+    /* RK combination w = cu u + cs s + cr dt rhs, and the diagonal mass inverse */
     double Xb[3][3];
-    const double rk = MODE == MODE_STAGE1 ? dt : (MODE == MODE_STAGE2 ? dt / 2 : 1.0);
-    const double sk = MODE == MODE_STAGE1 ? 1.0 : (MODE == MODE_STAGE2 ? 0.5 : 0.0);
+    double cu, sk, cr;
+    stage_coefficients(MODE, cu, sk, cr);
+    const double rk = MODE == MODE_RHS ? 1.0 : cr * dt;
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll

@@ -232,7 +232,22 @@ DGR_HD T flux_core(const T &zi, const T &qxi, const T &qyi, const T &ze, const T
     return lam;
 }
 
-enum { MODE_RHS = 0, MODE_STAGE1 = 1, MODE_STAGE2 = 2 };
+/* Element stage modes: the RHS alone; SSP-RK2 stages 1 and 2; SSP(3,3) stages 2 and 3
+ * (its stage 1 is MODE_STAGE1). */
+enum { MODE_RHS = 0, MODE_STAGE1 = 1, MODE_STAGE2 = 2, MODE_RK3_2 = 3, MODE_RK3_3 = 4 };
+
+/* The stage combination w = cu*u + cs*(s + dt*rhs) as coefficients of (u, s, dt*rhs), used
+ * by the reverse: RK2 stage 2 is (0.5, 0.5, 0.5). */
+DGR_HD void stage_coefficients(int mode, double &cu, double &cs, double &cr)
+{
+    cu = 0.0;
+    cs = 1.0;
+    cr = 1.0;
+    if (mode == MODE_STAGE2) { cu = 0.5; cs = 0.5; cr = 0.5; }
+    else if (mode == MODE_RK3_2) { cu = 0.75; cs = 0.25; cr = 0.25; }
+    else if (mode == MODE_RK3_3) { cu = 1.0 / 3; cs = 2.0 / 3; cr = 2.0 / 3; }
+    else if (mode == MODE_RHS) { cs = 0.0; }
+}
 
 /*
  * One element: surface and volume integrals of 2DCode/2DInnerProducts.c:8-570, the
@@ -345,12 +360,19 @@ DGR_HD void element_core(const T F[3][3], const T zr[3], const T qxr[3], const T
         for (int v = 0; v < 3; ++v)
 #pragma unroll
             for (int k = 0; k < 3; ++k) w[v][k] = s[v][k] + rhs[v][k] * dt;
-    } else {
+    } else if (MODE == MODE_STAGE2) {
         const double hdt = dt / 2;
 #pragma unroll
         for (int v = 0; v < 3; ++v)
 #pragma unroll
             for (int k = 0; k < 3; ++k) w[v][k] = (s[v][k] + uin(v, k)) * 0.5 + rhs[v][k] * hdt;
+    } else { /* SSP(3,3): u_i = a u^n + b (u_{i-1} + dt L(u_{i-1})), prep_DG.F:1253-1270 */
+        const double a = MODE == MODE_RK3_2 ? 0.75 : 1.0 / 3;
+        const double b = MODE == MODE_RK3_2 ? 0.25 : 2.0 / 3;
+#pragma unroll
+        for (int v = 0; v < 3; ++v)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) w[v][k] = a * uin(v, k) + b * (s[v][k] + rhs[v][k] * dt);
     }
 #pragma unroll
     for (int v = 0; v < 3; ++v) avg[v] = (w[v][0] + w[v][1] + w[v][2]) / 3;

@@ -471,18 +471,20 @@ static __global__ void __launch_bounds__(256) k_adj_node(MeshDev m, const double
     }
 }
 
-/* element reverse: RK combination, RHS, friction and bed terms; writes the stage-input
- * adjoint (stage 2: lamS = adjoint of the stage input, lamU = 0.5 * adjoint of the output;
- * stage 1: lamS += adjoint of the stage input), the per-edge-side flux adjoints and the
- * depth / Manning adjoints */
+/* element reverse: RK combination, RHS, friction and bed terms.  Stage-input adjoint:
+ * stage 1 (MODE_STAGE1, input u^n) adds into lamS = lamU; later stages write lamS and put
+ * cu * (output adjoint) into the step-input adjoint lamU, written at the last stage
+ * (u_accumulate = 0, where lamU's old content has been consumed) and added at the middle
+ * stage of RK3 (u_accumulate = 1).  Also writes the per-edge-side flux adjoints and
+ * accumulates the depth / Manning adjoints. */
 template <int MODE>
 __global__ void __launch_bounds__(128, DGR_ADJ_MINB_ELEMENT) k_adj_element(MeshDev m, const double *__restrict__ S,
                                                      const int *__restrict__ wd, const double *__restrict__ Rbar,
                                                      const double *__restrict__ bnode, const int *__restrict__ barg,
-                                                     double *lamS, double *lamU, double *__restrict__ fbar,
-                                                     double *__restrict__ zvb, double *__restrict__ nbar,
-                                                     const double *__restrict__ n_el, double g,
-                                                     const double *__restrict__ dt_hist, int n)
+                                                     double *lamS, double *lamU, int u_accumulate,
+                                                     double *__restrict__ fbar, double *__restrict__ zvb,
+                                                     double *__restrict__ nbar, const double *__restrict__ n_el,
+                                                     double g, const double *__restrict__ dt_hist, int n)
 {
     const int el = blockIdx.x * blockDim.x + threadIdx.x;
     if (el >= m.ne) return;
@@ -514,16 +516,18 @@ __global__ void __launch_bounds__(128, DGR_ADJ_MINB_ELEMENT) k_adj_element(MeshD
     double Fb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Sb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     double midzb[3] = {0, 0, 0}, gnnb[3] = {0, 0, 0}, gradzb[2] = {0, 0};
     element_core_rev<MODE>(wb, zr, qxr, qyr, geo, zg, local_g, dt_hist[n], Fb, Sb, midzb, gnnb, gradzb);
+    double cu, cs, cr;
+    stage_coefficients(MODE, cu, cs, cr);
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             const int idx = (3 * v + k) * ld + el;
-            if (MODE == MODE_STAGE2) {
-                lamS[idx] = Sb[v][k];
-                lamU[idx] = 0.5 * wb[v][k];
-            } else {
+            if (MODE == MODE_STAGE1) {
                 lamS[idx] += Sb[v][k];
+            } else {
+                lamS[idx] = Sb[v][k];
+                lamU[idx] = (u_accumulate ? lamU[idx] : 0.0) + cu * wb[v][k];
             }
         }
 #pragma unroll

@@ -44,6 +44,7 @@ class DgrParams(C.Structure):
         ("rain", C.c_double),
         ("device", C.c_int),
         ("record_decisions", C.c_int),
+        ("rk_stages", C.c_int),
     ]
 
 

@@ -86,6 +86,9 @@ typedef struct dgr_params {
     double rain;     /* m/s added to the elevation right-hand side (extension). Default 0. */
     int device;      /* CUDA device ordinal. Default 0. */
     int record_decisions; /* 1: keep per-element limiter/PDop decisions of the last step. */
+    int rk_stages;   /* 2: SSP-RK2 of 2DCode/time_evolution.c:10-246 (default).  3: SSP(3,3),
+                        the coefficients of DG-SWEM src/prep_DG.F:1253-1270 (extension: the
+                        limiter, PDop and status follow every stage as in the RK2 order). */
 } dgr_params;
 
 /* Mesh in the reference's arrays (2DCode/MeshAttributes.h:5-20), 0-based. */
@@ -165,7 +168,8 @@ DGR_API int dgr_params_default(dgr_params *p);
 DGR_API int dgr_create(const dgr_mesh_view *mesh, const dgr_params *params, dgr_ctx **out);
 DGR_API int dgr_destroy(dgr_ctx *ctx);
 DGR_API int dgr_get_params(const dgr_ctx *ctx, dgr_params *out);
-/* Only rain, tide_on, tide_amp, tide_period, cfl, dt0 and record_decisions may change. */
+/* Only rain, tide_on, tide_amp, tide_period, cfl, dt0, record_decisions and rk_stages may
+ * change. */
 DGR_API int dgr_set_params(dgr_ctx *ctx, const dgr_params *params);
 /* Per-element Manning n (extension); NULL restores the node average of
  * 2DCode/2DInnerProducts.c:272-274. */
@@ -236,7 +240,7 @@ DGR_API int dgr_autotune(dgr_ctx *ctx, int trial_steps, int *block_size, int *fu
 DGR_API int dgr_last_error(dgr_ctx *ctx, int *code, int *index, int *step);
 DGR_API const char *dgr_last_cuda_error(void);
 
-/* Per-element decisions of the last step (needs record_decisions = 1).  stage 0 or 1.
+/* Per-element decisions of the last step (needs record_decisions = 1).  stage 0 .. rk_stages-1.
  * limit[el] = 1 when the limiter rewrote the element; pdop[el] = 4*mass + momentum
  * branch (see oracle/dgr_oracle.h for the branch numbering). */
 DGR_API int dgr_get_decisions(dgr_ctx *ctx, int stage, int *limit, int *pdop);

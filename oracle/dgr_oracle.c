@@ -904,10 +904,61 @@ out:
     return rc;
 }
 
+/* One SSP(3,3) step (extension: the coefficients of DG-SWEM src/prep_DG.F:1253-1270 around
+ * the 2DCode operators, limiter / PDop / status after every stage as in orc_step):
+ * u1 = u + dt L(u);  u2 = 0.75 u + 0.25 (u1 + dt L(u1));  u3 = 1/3 u + 2/3 (u2 + dt L(u2)). */
+int orc_step3(orc_ctx *c, double time, double dt, int wet_dry, double rain)
+{
+    (void)time;
+    const size_t n = 3 * (size_t)c->ne;
+    int rc = 0;
+    double *w0z = dup_mem(c->zeta, n * sizeof(double));
+    double *w0x = dup_mem(c->qx, n * sizeof(double));
+    double *w0y = dup_mem(c->qy, n * sizeof(double));
+    if (wet_dry) orc_wd_status(c);
+    for (int st = 0; st < 3; ++st) {
+        if ((rc = orc_compute_L(c, wet_dry, rain))) break;
+        if (st == 0) {
+            for (size_t i = 0; i < n; ++i) {
+                c->zeta[i] = w0z[i] + c->rz[i] * dt;
+                c->qx[i] = w0x[i] + c->rqx[i] * dt;
+                c->qy[i] = w0y[i] + c->rqy[i] * dt;
+            }
+        } else {
+            const double a = st == 1 ? 0.75 : 1.0 / 3;
+            const double b = st == 1 ? 0.25 : 2.0 / 3;
+            for (size_t i = 0; i < n; ++i) {
+                c->zeta[i] = a * w0z[i] + b * (c->zeta[i] + c->rz[i] * dt);
+                c->qx[i] = a * w0x[i] + b * (c->qx[i] + c->rqx[i] * dt);
+                c->qy[i] = a * w0y[i] + b * (c->qy[i] + c->rqy[i] * dt);
+            }
+        }
+        orc_slope_limiter(c);
+        if (wet_dry) {
+            if ((rc = orc_pdop(c))) break;
+            if (st < 2) orc_wd_status(c);
+        }
+    }
+    free(w0z);
+    free(w0x);
+    free(w0y);
+    return rc;
+}
+
 /* Time loop of 2DCode/time_evolution.c:248-402 without file output. */
 int orc_run(orc_ctx *c, int nsteps, double final_time, double cfl, double dt0, int wet_dry,
             double rain, int tide_on, double amp, double period, double *time_io, double *dt_io,
             double *dt_hist, int *steps_done)
+{
+    return orc_run_rk(c, nsteps, final_time, cfl, dt0, wet_dry, rain, tide_on, amp, period, time_io, dt_io,
+                      dt_hist, steps_done, 2);
+}
+
+/* orc_run with 2 (SSP-RK2, the reference) or 3 (SSP(3,3)) stages per step; the CFL dt
+ * follows the last stage's max wave speed. */
+int orc_run_rk(orc_ctx *c, int nsteps, double final_time, double cfl, double dt0, int wet_dry,
+               double rain, int tide_on, double amp, double period, double *time_io, double *dt_io,
+               double *dt_hist, int *steps_done, int stages)
 {
     double time = *time_io, dt = *dt_io;
     int done = 0, rc = 0;
@@ -918,7 +969,9 @@ int orc_run(orc_ctx *c, int nsteps, double final_time, double cfl, double dt0, i
     }
     while (done < nsteps && time < final_time) {
         time = time + dt;
-        if ((rc = orc_step(c, time, dt, wet_dry, rain, NULL, NULL, NULL, NULL))) break;
+        rc = stages == 3 ? orc_step3(c, time, dt, wet_dry, rain)
+                         : orc_step(c, time, dt, wet_dry, rain, NULL, NULL, NULL, NULL);
+        if (rc) break;
         orc_boundary_conditions(c, time, tide_on, amp, period);
         if (dt_hist) dt_hist[done] = dt;
         ++done;

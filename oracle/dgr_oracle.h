@@ -86,6 +86,14 @@ void orc_inner_products(const orc_ctx *c, int el, double si[9], double vi[21]);
 int orc_step(orc_ctx *c, double time, double dt, int wet_dry, double rain, int *limit0,
              int *pdop0, int *limit1, int *pdop1);
 
+/* One SSP(3,3) step (extension; DG-SWEM src/prep_DG.F:1253-1270 coefficients). */
+int orc_step3(orc_ctx *c, double time, double dt, int wet_dry, double rain);
+
+/* orc_run with stages = 2 (SSP-RK2) or 3 (SSP(3,3)). */
+int orc_run_rk(orc_ctx *c, int nsteps, double final_time, double cfl, double dt0, int wet_dry,
+               double rain, int tide_on, double amp, double period, double *time_io, double *dt_io,
+               double *dt_hist, int *steps_done, int stages);
+
 /* Time loop of 2DCode/time_evolution.c:248-402 (no file output); see ref_run in
  * oracle/ref_driver.c for the clock convention. */
 int orc_run(orc_ctx *c, int nsteps, double final_time, double cfl, double dt0, int wet_dry,

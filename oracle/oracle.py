@@ -81,6 +81,7 @@ def _oracle_lib():
         lib.orc_step.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_double, iptr, iptr, iptr, iptr]
         lib.orc_run.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
                                 C.c_int, C.c_double, C.c_double, dptr, dptr, dptr, iptr]
+        lib.orc_run_rk.argtypes = lib.orc_run.argtypes + [C.c_int]
         _olib = lib
     return _olib
 
@@ -181,11 +182,11 @@ class Oracle:
         return self.lib.orc_max_lambda(self.h)
 
     def run(self, nsteps, final_time, cfl, dt0=1e-7, wet_dry=1, rain=0.0, tide_on=0, amp=0.0, period=44712.0,
-            time=-1.0, dt=0.0, want_dt=False):
+            time=-1.0, dt=0.0, want_dt=False, rk_stages=2):
         t, d, n = C.c_double(time), C.c_double(dt), C.c_int(0)
         hist = np.zeros(max(nsteps, 1)) if want_dt else None
-        rc = self.lib.orc_run(self.h, nsteps, final_time, cfl, dt0, wet_dry, rain, tide_on, amp, period,
-                              C.byref(t), C.byref(d), None if hist is None else _d(hist), C.byref(n))
+        rc = self.lib.orc_run_rk(self.h, nsteps, final_time, cfl, dt0, wet_dry, rain, tide_on, amp, period,
+                                 C.byref(t), C.byref(d), None if hist is None else _d(hist), C.byref(n), rk_stages)
         return rc, t.value, d.value, n.value, (hist[: n.value] if hist is not None else None)
 
 
