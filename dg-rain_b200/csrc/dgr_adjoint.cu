@@ -95,6 +95,7 @@ extern "C" int dgr_adjoint_setup(dgr_ctx *c, int nsteps, int ckpt_every, int nga
 {
     if (!c || c->nscen != 1 || nsteps <= 0 || ckpt_every <= 0 || ngauges <= 0 || !gauge_el || !gauge_w)
         return DGR_ERR_INVALID;
+    if (c->p.order != 1) return DGR_ERR_INVALID; /* the adjoint covers the p = 1 step */
     for (int g = 0; g < ngauges; ++g)
         if (gauge_el[g] < 0 || gauge_el[g] >= c->ne) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));

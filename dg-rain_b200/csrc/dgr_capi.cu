@@ -59,6 +59,7 @@ extern "C" int dgr_params_default(dgr_params *p)
     p->device = 0;
     p->record_decisions = 0;
     p->rk_stages = 2;
+    p->order = 1;
     return DGR_OK;
 }
 
@@ -77,7 +78,7 @@ static void release(dgr_ctx *c)
     void *ptrs[] = {c->x, c->y, c->zn, c->nfric, c->n_el, c->el2v_aos, c->el2v, c->elem_edge, c->e_in,
                     c->e_ex, c->e_info, c->n2e_ptr, c->n2e, c->bnd_edges, c->bnd_type, c->bnd_sid, c->bdry,
                     c->el_sid, c->ed_sid, c->e_geo, c->geo, c->U, c->W, c->flux, c->avg, c->bounds, c->bzeta,
-                    c->bqn, c->bstage, c->wdA, c->wdB, c->wdC, c->dec, c->bar, c->clk};
+                    c->bqn, c->bstage, c->wdA, c->wdB, c->wdC, c->dec, c->bar, c->clk, c->p2g};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     adjoint_release(c);
@@ -94,8 +95,65 @@ int upload_geometry(dgr_ctx *c)
     k_element_setup<<<blocks(c->ne, 128), 128, 0, c->stream>>>(c->ne, c->ldE, c->el2v_aos, c->x, c->y, c->zn,
                                                                c->nfric, c->n_el, c->p.g, c->el2v, c->geo);
     c->launches++;
+    if (c->p.order == 2) {
+        k_p2_setup<<<blocks(c->ne, 256), 256, 0, c->stream>>>(c->ne, c->ldE, c->el2v_aos, c->x, c->y, c->zn,
+                                                              c->nfric, c->n_el, c->p.g, c->p2g);
+        c->launches++;
+    }
     CK(cudaGetLastError());
     return DGR_OK;
+}
+
+/* The p = 2 basis at (r, s) with its derivatives, in the closed forms of dgr_p2.cuh. */
+static void p2_basis(double r, double sv, double phi[P2_NM], double dr[P2_NM], double ds[P2_NM])
+{
+    const double A = r + (1.0 + sv) / 2, B = (1.0 - sv) / 2;
+    const double f[P2_NM] = {1.0, (3.0 * sv + 1.0) / 2, A, (5.0 * sv * sv + 2.0 * sv - 1.0) / 2,
+                             A * (5.0 * sv + 3.0) / 2, (3.0 * A * A - B * B) / 2};
+    const double fr[P2_NM] = {0.0, 0.0, 1.0, 0.0, (5.0 * sv + 3.0) / 2, 3.0 * A};
+    const double fs[P2_NM] = {0.0, 1.5, 0.5, 5.0 * sv + 1.0, (5.0 * sv + 3.0) / 4 + 5.0 * A / 2, (3.0 * A + B) / 2};
+    for (int m = 0; m < P2_NM; ++m) {
+        phi[m] = f[m];
+        dr[m] = fr[m];
+        ds[m] = fs[m];
+    }
+}
+
+/* Reference tables of the p = 2 step: Radon's 7-point degree-5 area rule (centroid 9/40;
+ * a = (6 -+ sqrt 15)/21 with weights (155 -+ sqrt 15)/1200), 3-point Gauss-Legendre on the
+ * edges, the basis there, and the diagonal mass matrix. */
+static P2Ref make_p2_ref()
+{
+    P2Ref R;
+    const double s15 = sqrt(15.0);
+    const double a1 = (6.0 - s15) / 21, a2 = (6.0 + s15) / 21;
+    const double w1 = (155.0 - s15) / 1200, w2 = (155.0 + s15) / 1200;
+    const double L[P2_NQ][3] = {{1.0 / 3, 1.0 / 3, 1.0 / 3}, {1.0 - 2 * a1, a1, a1}, {a1, 1.0 - 2 * a1, a1},
+                                {a1, a1, 1.0 - 2 * a1},      {1.0 - 2 * a2, a2, a2}, {a2, 1.0 - 2 * a2, a2},
+                                {a2, a2, 1.0 - 2 * a2}};
+    const double W[P2_NQ] = {9.0 / 40, w1, w1, w1, w2, w2, w2};
+    for (int m = 0; m < P2_NM; ++m) R.mass[m] = 0.0;
+    for (int q = 0; q < P2_NQ; ++q) {
+        R.wq[q] = W[q];
+        for (int k = 0; k < 3; ++k) R.lam[q][k] = L[q][k];
+        const double r = -L[q][0] + L[q][1] - L[q][2], sv = -L[q][0] - L[q][1] + L[q][2];
+        p2_basis(r, sv, R.phi[q], R.dr[q], R.ds[q]);
+        for (int m = 0; m < P2_NM; ++m) R.mass[m] += 2.0 * W[q] * R.phi[q][m] * R.phi[q][m];
+    }
+    const double g3 = sqrt(3.0 / 5);
+    const double te[P2_NGP] = {-g3, 0.0, g3}, wg[P2_NGP] = {5.0 / 9, 8.0 / 9, 5.0 / 9};
+    for (int gp = 0; gp < P2_NGP; ++gp) {
+        R.te[gp] = te[gp];
+        R.wg[gp] = wg[gp];
+        const double t = te[gp];
+        /* local edge k runs from vertex k to k+1: (t, -1), (-t, t), (-1, -t) */
+        const double rs[3][2] = {{t, -1.0}, {-t, t}, {-1.0, -t}};
+        for (int k = 0; k < 3; ++k) {
+            double dr[P2_NM], ds[P2_NM];
+            p2_basis(rs[k][0], rs[k][1], R.phie[k][gp], dr, ds);
+        }
+    }
+    return R;
 }
 
 static int check_mesh_view(const dgr_mesh_view *m)
@@ -174,10 +232,15 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
         dgr_params_default(&c->p);
     c->device = c->p.device;
     if (c->p.rk_stages == 0) c->p.rk_stages = 2; /* a zero-filled struct means the reference's RK2 */
-    if (c->p.rk_stages != 2 && c->p.rk_stages != 3) {
+    if (c->p.order == 0) c->p.order = 1;
+    if ((c->p.rk_stages != 2 && c->p.rk_stages != 3) || (c->p.order != 1 && c->p.order != 2) ||
+        (c->p.order == 2 && c->p.wet_dry)) {
         delete c;
         return DGR_ERR_INVALID;
     }
+    c->nm = c->p.order == 2 ? P2_NM : 3;
+    c->nfp = c->p.order == 2 ? P2_FLUX : 6;
+    if (c->p.order == 2) c->p2ref = make_p2_ref();
     c->bs = 128;
     c->fusion = 0;
     if (c->device < 0 || c->device >= ndev) {
@@ -225,9 +288,11 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     TRY(dalloc(&c->bdry, nf));
     TRY(dalloc(&c->e_geo, 3 * lF));
     TRY(dalloc(&c->geo, (size_t)NG * lE));
-    TRY(dalloc(&c->U, 9 * lE));
-    TRY(dalloc(&c->W, 9 * lE));
-    TRY(dalloc(&c->flux, 6 * lF));
+    const size_t nst = 3 * (size_t)c->nm;
+    TRY(dalloc(&c->U, nst * lE));
+    TRY(dalloc(&c->W, nst * lE));
+    TRY(dalloc(&c->flux, (size_t)c->nfp * lF));
+    if (c->p.order == 2) TRY(dalloc(&c->p2g, (size_t)P2G_N * lE));
     TRY(dalloc(&c->avg, 3 * lE));
     TRY(dalloc(&c->bounds, 6 * lN));
     TRY(dalloc(&c->bzeta, nf));
@@ -262,8 +327,8 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     TRYC(cudaMemsetAsync(c->elem_edge, 0xff, 3 * lE * 4, s));
     TRYC(cudaMemsetAsync(c->bzeta, 0, nf * 8, s));
     TRYC(cudaMemsetAsync(c->bqn, 0, nf * 8, s));
-    TRYC(cudaMemsetAsync(c->U, 0, 9 * lE * 8, s));
-    TRYC(cudaMemsetAsync(c->W, 0, 9 * lE * 8, s));
+    TRYC(cudaMemsetAsync(c->U, 0, nst * lE * 8, s));
+    TRYC(cudaMemsetAsync(c->W, 0, nst * lE * 8, s));
     TRYC(cudaMemsetAsync(c->dec, 0, 6 * ne * 4, s));
     TRYC(cudaMemsetAsync(c->bar, 0, 16, s));
 
@@ -450,7 +515,7 @@ extern "C" int dgr_set_params(dgr_ctx *c, const dgr_params *p)
 {
     if (!c || !p) return DGR_ERR_INVALID;
     if (p->g != c->p.g || p->H0 != c->p.H0 || p->VELZERO != c->p.VELZERO || p->wet_dry != c->p.wet_dry ||
-        p->device != c->p.device)
+        p->device != c->p.device || (p->order == 0 ? 1 : p->order) != c->p.order)
         return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     c->p.rain = p->rain;
@@ -512,13 +577,14 @@ static int upload_slice(dgr_ctx *c, int sc, const double *zeta, const double *Qx
     if (!zeta || !Qx || !Qy || sc < 0 || sc >= c->nscen) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     const int n = c->el_off[sc + 1] - c->el_off[sc];
-    const size_t n3 = 3 * (size_t)n;
+    const size_t n3 = (size_t)c->nm * n; /* coefficients per variable */
     double *st = c->W; /* staging: W is free between steps */
     cudaStream_t s = c->stream;
     CK(cudaMemcpyAsync(st, zeta, n3 * 8, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(st + n3, Qx, n3 * 8, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(st + 2 * n3, Qy, n3 * 8, cudaMemcpyHostToDevice, s));
-    k_aos_to_planar<<<blocks(n, 256), 256, 0, s>>>(n, c->ldE, st, st + n3, st + 2 * n3, c->U + c->el_off[sc]);
+    k_aos_to_planar_nm<<<blocks(n, 256), 256, 0, s>>>(n, c->ldE, c->nm, st, st + n3, st + 2 * n3,
+                                                      c->U + c->el_off[sc]);
     c->launches++;
     /* the other scenarios' current flags must sit in WA as well before WA is marked current */
     if (c->wd_stepped && c->nscen > 1)
@@ -545,10 +611,11 @@ static int download_slice(dgr_ctx *c, int sc, double *zeta, double *Qx, double *
     if (!zeta || !Qx || !Qy || sc < 0 || sc >= c->nscen) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     const int n = c->el_off[sc + 1] - c->el_off[sc];
-    const size_t n3 = 3 * (size_t)n;
+    const size_t n3 = (size_t)c->nm * n;
     double *st = c->W;
     cudaStream_t s = c->stream;
-    k_planar_to_aos<<<blocks(n, 256), 256, 0, s>>>(n, c->ldE, c->U + c->el_off[sc], st, st + n3, st + 2 * n3);
+    k_planar_to_aos_nm<<<blocks(n, 256), 256, 0, s>>>(n, c->ldE, c->nm, c->U + c->el_off[sc], st, st + n3,
+                                                      st + 2 * n3);
     c->launches++;
     CK(cudaMemcpyAsync(zeta, st, n3 * 8, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(Qx, st + n3, n3 * 8, cudaMemcpyDeviceToHost, s));
@@ -678,9 +745,42 @@ static void launch_edge(dgr_ctx *c, const double *S, const int *wd, int lam_slot
                                                                       lam_slot, phase, c->p.g);
 }
 
+/* one RK stage of the p = 2 step: edge fluxes at the Gauss points, element update */
+static void launch_p2_stage(dgr_ctx *c, int stage, bool count)
+{
+    const StageIO io = stage_io(c, stage);
+    const MeshDev m = mesh_dev(c);
+    cudaStream_t s = c->stream;
+    k_p2_edge<128><<<blocks(c->nf, 128), 128, 0, s>>>(c->p2ref, m, c->p2g, io.S, c->bzeta, c->bqn, c->flux, c->clk,
+                                                      stage, 2 * stage, c->p.g);
+    const unsigned nb = blocks(c->ne, 128);
+    switch (io.mode) {
+    case MODE_STAGE1:
+        k_p2_element<MODE_STAGE1, 128><<<nb, 128, 0, s>>>(c->p2ref, m, c->p2g, io.S, c->U, c->flux, io.OUT, c->clk,
+                                                          c->p.g);
+        break;
+    case MODE_STAGE2:
+        k_p2_element<MODE_STAGE2, 128><<<nb, 128, 0, s>>>(c->p2ref, m, c->p2g, io.S, c->U, c->flux, io.OUT, c->clk,
+                                                          c->p.g);
+        break;
+    case MODE_RK3_2:
+        k_p2_element<MODE_RK3_2, 128><<<nb, 128, 0, s>>>(c->p2ref, m, c->p2g, io.S, c->U, c->flux, io.OUT, c->clk,
+                                                         c->p.g);
+        break;
+    default:
+        k_p2_element<MODE_RK3_3, 128><<<nb, 128, 0, s>>>(c->p2ref, m, c->p2g, io.S, c->U, c->flux, io.OUT, c->clk,
+                                                         c->p.g);
+    }
+    if (count) c->launches += 2;
+}
+
 /* one RK stage as four kernels (buffers of stage_io) */
 void launch_stage(dgr_ctx *c, int stage, bool count)
 {
+    if (c->p.order == 2) {
+        launch_p2_stage(c, stage, count);
+        return;
+    }
     const bool wd = c->p.wet_dry != 0;
     const StageIO io = stage_io(c, stage);
     int *dl = c->p.record_decisions ? c->dec + (size_t)(2 * stage) * c->ne : nullptr;
@@ -786,11 +886,11 @@ static cudaError_t launch_step(dgr_ctx *c)
     cudaStream_t s = c->stream;
     const PhysParams p = phys(c);
     const int ns = c->p.rk_stages;
-    if (c->fusion == 2) return launch_fused(c, 0, ns, 1);
+    if (c->fusion == 2 && c->p.order == 1) return launch_fused(c, 0, ns, 1);
     k_clock_begin<<<1, 256, 0, s>>>(c->clk, c->nscen, p, c->bnd_edges, c->bnd_type, c->bnd_sid, c->nbnd, c->bzeta,
                                     c->bqn);
     for (int st = 0; st < ns; ++st) {
-        if (c->fusion == 1) {
+        if (c->fusion == 1 && c->p.order == 1) {
             cudaError_t e = launch_fused(c, st, st + 1, 0);
             if (e != cudaSuccess) return e;
         } else {
@@ -804,6 +904,7 @@ static cudaError_t launch_step(dgr_ctx *c)
 static int kernels_per_step(const dgr_ctx *c)
 {
     const int ns = c->p.rk_stages;
+    if (c->p.order == 2) return 2 + 2 * ns;
     return c->fusion == 2 ? 1 : (c->fusion == 1 ? 2 + ns : 2 + 4 * ns);
 }
 
@@ -871,17 +972,26 @@ extern "C" int dgr_compute_L(dgr_ctx *c, double time, double *rz, double *rqx, d
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     k_clock_set<<<1, 1, 0, s>>>(c->clk, 0.0, 0.0);
-    const int *wd = wd_current(c);
-    launch_edge(c, c->U, wd, 0, 0);
-    k_element<MODE_RHS, 128><<<blocks(c->ne, 128), 128, 0, s>>>(mesh_dev(c), c->U, c->U, wd, c->flux, c->W, c->avg,
-                                                                c->clk, c->p.g);
+    if (c->p.order == 2) {
+        const MeshDev m = mesh_dev(c);
+        k_p2_edge<128><<<blocks(c->nf, 128), 128, 0, s>>>(c->p2ref, m, c->p2g, c->U, c->bzeta, c->bqn, c->flux,
+                                                          c->clk, 0, 0, c->p.g);
+        k_p2_element<MODE_RHS, 128><<<blocks(c->ne, 128), 128, 0, s>>>(c->p2ref, m, c->p2g, c->U, c->U, c->flux,
+                                                                       c->W, c->clk, c->p.g);
+    } else {
+        const int *wd = wd_current(c);
+        launch_edge(c, c->U, wd, 0, 0);
+        k_element<MODE_RHS, 128><<<blocks(c->ne, 128), 128, 0, s>>>(mesh_dev(c), c->U, c->U, wd, c->flux, c->W,
+                                                                    c->avg, c->clk, c->p.g);
+    }
     c->launches += 3;
     CK(cudaGetLastError());
     if (rz && rqx && rqy) {
-        const size_t n3 = 3 * (size_t)c->ne;
+        const size_t n3 = (size_t)c->nm * c->ne;
         double *tmp = nullptr; /* stream-ordered staging for the reference layout */
         CK(cudaMallocAsync((void **)&tmp, 3 * n3 * 8, s));
-        k_planar_to_aos<<<blocks(c->ne, 256), 256, 0, s>>>(c->ne, c->ldE, c->W, tmp, tmp + n3, tmp + 2 * n3);
+        k_planar_to_aos_nm<<<blocks(c->ne, 256), 256, 0, s>>>(c->ne, c->ldE, c->nm, c->W, tmp, tmp + n3,
+                                                              tmp + 2 * n3);
         c->launches++;
         CK(cudaMemcpyAsync(rz, tmp, n3 * 8, cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(rqx, tmp + n3, n3 * 8, cudaMemcpyDeviceToHost, s));
@@ -897,6 +1007,7 @@ extern "C" int dgr_compute_L(dgr_ctx *c, double time, double *rz, double *rqx, d
 extern "C" int dgr_get_fhat(dgr_ctx *c, double *f1, double *f2, double *f3)
 {
     if (!c || !f1 || !f2 || !f3 || c->nscen != 1) return DGR_ERR_INVALID;
+    if (c->p.order != 1) return DGR_ERR_INVALID; /* p = 1 operators */
     CK(cudaSetDevice(c->device));
     const size_t n3 = 3 * (size_t)c->ne;
     double *tmp = nullptr;
@@ -914,6 +1025,7 @@ extern "C" int dgr_get_fhat(dgr_ctx *c, double *f1, double *f2, double *f3)
 extern "C" int dgr_slope_limiter(dgr_ctx *c)
 {
     if (!c || c->nscen != 1) return DGR_ERR_INVALID;
+    if (c->p.order != 1) return DGR_ERR_INVALID; /* p = 1 operators */
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     const MeshDev m = mesh_dev(c);
@@ -933,6 +1045,7 @@ extern "C" int dgr_slope_limiter(dgr_ctx *c)
 extern "C" int dgr_pdop(dgr_ctx *c)
 {
     if (!c || c->nscen != 1) return DGR_ERR_INVALID;
+    if (c->p.order != 1) return DGR_ERR_INVALID; /* p = 1 operators */
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     k_clock_set<<<1, 1, 0, s>>>(c->clk, 0.0, 0.0);
@@ -951,6 +1064,7 @@ extern "C" int dgr_pdop(dgr_ctx *c)
 extern "C" int dgr_wet_dry_status(dgr_ctx *c)
 {
     if (!c || c->nscen != 1) return DGR_ERR_INVALID;
+    if (c->p.order != 1) return DGR_ERR_INVALID; /* p = 1 operators */
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     int *wd = c->wd_stepped ? wd_after_step(c) : c->wdA;
@@ -1086,6 +1200,7 @@ extern "C" int dgr_set_schedule(dgr_ctx *c, int block_size, int fusion)
 {
     if (!c || (block_size != 64 && block_size != 128 && block_size != 256) || fusion < 0 || fusion > 2)
         return DGR_ERR_INVALID;
+    if (c->p.order == 2 && fusion != 0) return DGR_ERR_INVALID; /* the p = 2 step has no fused kernel */
     c->bs = block_size;
     c->fusion = fusion;
     drop_graph(c);
@@ -1113,7 +1228,7 @@ extern "C" int dgr_autotune(dgr_ctx *c, int trial_steps, int *block_size, int *f
     if (!c || trial_steps <= 0) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
-    const size_t nU = 9 * (size_t)c->ldE;
+    const size_t nU = 3 * (size_t)c->nm * c->ldE;
     double *saveU = nullptr;
     int *saveWD = nullptr;
     CK(cudaMallocAsync((void **)&saveU, nU * 8, s));
@@ -1131,7 +1246,7 @@ extern "C" int dgr_autotune(dgr_ctx *c, int trial_steps, int *block_size, int *f
     int best_bs = c->bs, best_f = c->fusion;
     std::vector<double> t(c->nscen), d(c->nscen), fin(c->nscen, 1e300);
     for (int b = 0; b < 3; ++b)
-        for (int f = 0; f < 3; ++f) {
+        for (int f = 0; f < (c->p.order == 2 ? 1 : 3); ++f) {
             c->bs = bss[b];
             c->fusion = f;
             drop_graph(c);
@@ -1208,9 +1323,69 @@ extern "C" void dgr_host_free(void *p)
  * receive the average ms of one launch of: edge flux, element RHS+RK, node bounds,
  * limiter+PDop.
  */
+/* dgr_profile_step of the p = 2 step: kernel_ms[0] edge fluxes, [1] element update */
+static int profile_p2(dgr_ctx *c, int nsteps, double *kernel_ms)
+{
+    CK(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    cudaEvent_t ev[3];
+    for (int i = 0; i < 3; ++i) CK(cudaEventCreate(&ev[i]));
+    double acc[2] = {0, 0};
+    int r = read_clock(c);
+    if (r) return r;
+    for (int k = 0; k < c->nscen; ++k) {
+        if (!(c->h_clk[k].dt > 0)) c->h_clk[k].dt = c->p.dt0;
+        c->h_clk[k].done = 0;
+    }
+    r = write_clock(c);
+    if (r) return r;
+    const MeshDev m = mesh_dev(c);
+    int rc = DGR_OK;
+    for (int it = 0; it < nsteps && rc == DGR_OK; ++it)
+        for (int stage = 0; stage < c->p.rk_stages; ++stage) {
+            const StageIO io = stage_io(c, stage);
+            cudaEventRecord(ev[0], s);
+            k_p2_edge<128><<<blocks(c->nf, 128), 128, 0, s>>>(c->p2ref, m, c->p2g, io.S, c->bzeta, c->bqn, c->flux,
+                                                              c->clk, stage, 2 * stage, c->p.g);
+            cudaEventRecord(ev[1], s);
+            const unsigned nb = blocks(c->ne, 128);
+            if (io.mode == MODE_STAGE1)
+                k_p2_element<MODE_STAGE1, 128><<<nb, 128, 0, s>>>(c->p2ref, m, c->p2g, io.S, c->U, c->flux, io.OUT,
+                                                                  c->clk, c->p.g);
+            else if (io.mode == MODE_STAGE2)
+                k_p2_element<MODE_STAGE2, 128><<<nb, 128, 0, s>>>(c->p2ref, m, c->p2g, io.S, c->U, c->flux, io.OUT,
+                                                                  c->clk, c->p.g);
+            else if (io.mode == MODE_RK3_2)
+                k_p2_element<MODE_RK3_2, 128><<<nb, 128, 0, s>>>(c->p2ref, m, c->p2g, io.S, c->U, c->flux, io.OUT,
+                                                                 c->clk, c->p.g);
+            else
+                k_p2_element<MODE_RK3_3, 128><<<nb, 128, 0, s>>>(c->p2ref, m, c->p2g, io.S, c->U, c->flux, io.OUT,
+                                                                 c->clk, c->p.g);
+            cudaEventRecord(ev[2], s);
+            c->launches += 2;
+            if (cudaEventSynchronize(ev[2]) != cudaSuccess) {
+                rc = DGR_ERR_CUDA;
+                break;
+            }
+            for (int k = 0; k < 2; ++k) {
+                float ms = 0;
+                cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+                acc[k] += ms;
+            }
+        }
+    for (int i = 0; i < 3; ++i) cudaEventDestroy(ev[i]);
+    if (rc) return rc;
+    CK(cudaGetLastError());
+    kernel_ms[0] = acc[0] / ((double)c->p.rk_stages * nsteps);
+    kernel_ms[1] = acc[1] / ((double)c->p.rk_stages * nsteps);
+    kernel_ms[2] = kernel_ms[3] = 0.0;
+    return DGR_OK;
+}
+
 extern "C" int dgr_profile_step(dgr_ctx *c, int nsteps, double *kernel_ms, int n)
 {
     if (!c || nsteps <= 0 || !kernel_ms || n < 4) return DGR_ERR_INVALID;
+    if (c->p.order == 2) return profile_p2(c, nsteps, kernel_ms);
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     const bool wd = c->p.wet_dry != 0;
@@ -1271,6 +1446,33 @@ extern "C" int dgr_profile_step(dgr_ctx *c, int nsteps, double *kernel_ms, int n
     if (rc) return rc;
     CK(cudaGetLastError());
     for (int k = 0; k < 4; ++k) kernel_ms[k] = acc[k] / ((double)c->p.rk_stages * nsteps);
+    return DGR_OK;
+}
+
+extern "C" int dgr_p2_reference(double *t, int n)
+{
+    if (!t || n < 234) return DGR_ERR_INVALID;
+    const P2Ref R = make_p2_ref();
+    int i = 0;
+    for (int q = 0; q < P2_NQ; ++q) t[i++] = R.wq[q];
+    for (int q = 0; q < P2_NQ; ++q)
+        for (int k = 0; k < 3; ++k) t[i++] = R.lam[q][k];
+    for (int q = 0; q < P2_NQ; ++q)
+        for (int m = 0; m < P2_NM; ++m) t[i++] = R.phi[q][m];
+    for (int q = 0; q < P2_NQ; ++q)
+        for (int m = 0; m < P2_NM; ++m) t[i++] = R.dr[q][m];
+    for (int q = 0; q < P2_NQ; ++q)
+        for (int m = 0; m < P2_NM; ++m) t[i++] = R.ds[q][m];
+    for (int gp = 0; gp < P2_NGP; ++gp) t[i++] = R.te[gp];
+    for (int gp = 0; gp < P2_NGP; ++gp) t[i++] = R.wg[gp];
+    for (int k = 0; k < 3; ++k)
+        for (int gp = 0; gp < P2_NGP; ++gp)
+            for (int m = 0; m < P2_NM; ++m) t[i++] = R.phie[k][gp][m];
+    for (int m = 0; m < P2_NM; ++m) t[i++] = R.mass[m];
+    for (int q = 0; q < P2_NQ; ++q) {
+        t[i++] = -R.lam[q][0] + R.lam[q][1] - R.lam[q][2];
+        t[i++] = -R.lam[q][0] - R.lam[q][1] + R.lam[q][2];
+    }
     return DGR_OK;
 }
 

@@ -13,6 +13,7 @@
 
 #include "../../include/dgrain.h"
 #include "dgr_kernels.cuh"
+#include "dgr_p2.cuh"
 
 namespace dgr {
 struct AdjointState; /* dgr_adjoint.cu */
@@ -52,6 +53,10 @@ static inline int dalloc(T **p, size_t n)
 
 struct dgr_ctx {
     dgr_params p;
+    int nm;   /* state coefficients per element and variable: 3 (p = 1) or 6 (p = 2) */
+    int nfp;  /* flux planes per edge: 6 (p = 1: Fhat.n of both sides) or 9 (p = 2: 3 Gauss points) */
+    double *p2g;         /* p = 2 element geometry planes [P2G_N][ldE] */
+    dgr::P2Ref p2ref;    /* p = 2 reference-element tables */
     int device;
     int nscen;
     int ne, nn, nf, nbnd;

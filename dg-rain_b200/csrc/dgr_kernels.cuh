@@ -619,9 +619,13 @@ static __global__ void k_edge_setup(int nf, int ldE, int ldF, const int *__restr
     const double x0 = x[p0], x1 = x[p1], y0 = y[p0], y1 = y[p1];
     const double nx = sgn(jac) * (y1 - y0) / len;
     const double ny = sgn(jac) * (x0 - x1) / len;
+    /* bit 7: the "ex" element's local edge runs in the same direction as the "in" one (the
+     * p = 2 step pairs Gauss points by it; opposite for consistently oriented elements) */
+    const int ex_start = el2v_aos[3 * el_ex + k_ex];
+    const int same_dir = (el_ex != el_in && ex_start == p0) ? 1 : 0;
     e_in[i] = el_in;
     e_ex[i] = el_ex;
-    e_info[i] = k_in | (k_ex << 2) | ((bdry[i] & 7) << 4);
+    e_info[i] = k_in | (k_ex << 2) | ((bdry[i] & 7) << 4) | (same_dir << 7);
     e_geo[i] = nx;
     e_geo[ldF + i] = ny;
     e_geo[2 * ldF + i] = (z[v0] + z[v1]) / 2;
@@ -678,6 +682,30 @@ static __global__ void k_planar_to_aos(int ne, int ld, const double *__restrict_
     for (int v = 0; v < 3; ++v)
 #pragma unroll
         for (int k = 0; k < 3; ++k) dst[v][3 * el + k] = S[(3 * v + k) * ld + el];
+}
+
+/* the same transposes for nm coefficients per element and variable ([nm*el+k] <->
+ * planar [nm*v+k][ld]; nm = 3 for p = 1, 6 for p = 2) */
+static __global__ void __launch_bounds__(256) k_aos_to_planar_nm(int ne, int ld, int nm, const double *__restrict__ a0,
+                                                                 const double *__restrict__ a1,
+                                                                 const double *__restrict__ a2, double *__restrict__ S)
+{
+    const int el = blockIdx.x * blockDim.x + threadIdx.x;
+    if (el >= ne) return;
+    const double *src[3] = {a0, a1, a2};
+    for (int v = 0; v < 3; ++v)
+        for (int k = 0; k < nm; ++k) S[(size_t)(nm * v + k) * ld + el] = src[v][(size_t)nm * el + k];
+}
+
+static __global__ void __launch_bounds__(256) k_planar_to_aos_nm(int ne, int ld, int nm, const double *__restrict__ S,
+                                                                 double *__restrict__ a0, double *__restrict__ a1,
+                                                                 double *__restrict__ a2)
+{
+    const int el = blockIdx.x * blockDim.x + threadIdx.x;
+    if (el >= ne) return;
+    double *dst[3] = {a0, a1, a2};
+    for (int v = 0; v < 3; ++v)
+        for (int k = 0; k < nm; ++k) dst[v][(size_t)nm * el + k] = S[(size_t)(nm * v + k) * ld + el];
 }
 
 /* edge fluxes back into the reference's element slots Fhat[3*el+k] */

@@ -45,6 +45,7 @@ class DgrParams(C.Structure):
         ("device", C.c_int),
         ("record_decisions", C.c_int),
         ("rk_stages", C.c_int),
+        ("order", C.c_int),
     ]
 
 
@@ -152,6 +153,7 @@ SIGNATURES = [
     ("dgr_adjoint_dt", C.c_int, [C.c_void_p, dptr, dptr]),
     ("dgr_adjoint_timing", C.c_int, [C.c_void_p, dptr, dptr, dptr]),
     ("dgr_set_bathymetry", C.c_int, [C.c_void_p, dptr]),
+    ("dgr_p2_reference", C.c_int, [dptr, C.c_int]),
 ]
 
 _lib = None

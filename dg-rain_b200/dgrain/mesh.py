@@ -84,9 +84,10 @@ def _pairs(a) -> np.ndarray:
 
 def rectangle(nx: int, ny: int, lx: float = 10000.0, ly: float = 5000.0, jitter: float = 0.0,
               seed: int = 0, n_bumps: int = 8, manning: float = 0.03, connect: bool = True,
-              datum: float = 0.0) -> Mesh:
+              datum: float = 0.0, ocean: bool = True) -> Mesh:
     """The synthetic coastal rectangle; `datum` lowers the whole land surface by that many
-    metres (datum = 3 gives a basin that is under water everywhere)."""
+    metres (datum = 3 gives a basin that is under water everywhere); ocean = False closes
+    the x = 0 side (every boundary edge is land)."""
     rng = np.random.default_rng(seed)
     amp = rng.uniform(-0.5, 0.5, n_bumps)
     sig = rng.uniform(300.0, 800.0, n_bumps)
@@ -122,6 +123,8 @@ def rectangle(nx: int, ny: int, lx: float = 10000.0, ly: float = 5000.0, jitter:
     el2v[1::2] = np.stack([a, c, d], axis=1)
     jj_ = np.arange(ny)
     outflow = np.stack([node(0, jj_), node(0, jj_ + 1)], axis=1).astype(np.int32)
+    if not ocean:
+        outflow = _pairs([])
     m = Mesh(x=np.ascontiguousarray(x), y=np.ascontiguousarray(y), z=np.ascontiguousarray(z),
              nfric=np.ascontiguousarray(nfric), el2v=np.ascontiguousarray(el2v),
              inflow1=_pairs([]), inflow2=_pairs([]), outflow=np.ascontiguousarray(outflow))

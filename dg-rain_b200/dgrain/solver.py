@@ -45,6 +45,7 @@ class Solver:
         self.ctx = h
         self.ne = mesh.num_el
         self.nf = mesh.num_edges
+        self.nm = 6 if self.params.order == 2 else 3  # state coefficients per element and variable
 
     # ------------------------------------------------------------------ life ----
     def close(self) -> None:
@@ -89,15 +90,15 @@ class Solver:
         z = np.ascontiguousarray(zeta, dtype=np.float64)
         x = np.ascontiguousarray(qx, dtype=np.float64)
         y = np.ascontiguousarray(qy, dtype=np.float64)
-        assert z.shape == x.shape == y.shape == (3 * self.ne,)
+        assert z.shape == x.shape == y.shape == (self.nm * self.ne,)
         w = None if wd is None else np.ascontiguousarray(wd, dtype=np.int32)
         _lib.check(self.lib.dgr_upload_state(self.ctx, _dp(z), _dp(x), _dp(y), None if w is None else _ip(w)),
                    "dgr_upload_state")
 
     def download_state(self):
-        z = np.empty(3 * self.ne)
-        x = np.empty(3 * self.ne)
-        y = np.empty(3 * self.ne)
+        z = np.empty(self.nm * self.ne)
+        x = np.empty(self.nm * self.ne)
+        y = np.empty(self.nm * self.ne)
         w = np.empty(self.ne, dtype=np.int32)
         _lib.check(self.lib.dgr_download_state(self.ctx, _dp(z), _dp(x), _dp(y), _ip(w)), "dgr_download_state")
         return z, x, y, w
@@ -121,9 +122,9 @@ class Solver:
         _lib.check(rc, where)
 
     def compute2DL(self, time: float = 0.0):
-        rz = np.empty(3 * self.ne)
-        rx = np.empty(3 * self.ne)
-        ry = np.empty(3 * self.ne)
+        rz = np.empty(self.nm * self.ne)
+        rx = np.empty(self.nm * self.ne)
+        ry = np.empty(self.nm * self.ne)
         lam = C.c_double()
         self._status(self.lib.dgr_compute_L(self.ctx, time, _dp(rz), _dp(rx), _dp(ry), C.byref(lam)), "compute2DL")
         return rz, rx, ry, lam.value
@@ -221,6 +222,7 @@ class Ensemble:
         self.meshes = list(meshes)
         n = len(self.meshes)
         self.params = default_params(**common)
+        self.nm = 6 if self.params.order == 2 else 3  # state coefficients per element and variable
         self._views = (_lib.DgrMeshView * n)(*[m.view() for m in self.meshes])
         sp = (_lib.DgrScenarioParams * n)()
         self._keep = []
@@ -262,14 +264,14 @@ class Ensemble:
     def upload_state(self, s: int, zeta, qx, qy, wd=None) -> None:
         ne = self.meshes[s].num_el
         z, x, y = (np.ascontiguousarray(a, dtype=np.float64) for a in (zeta, qx, qy))
-        assert z.shape == x.shape == y.shape == (3 * ne,)
+        assert z.shape == x.shape == y.shape == (self.nm * ne,)
         w = None if wd is None else np.ascontiguousarray(wd, dtype=np.int32)
         _lib.check(self.lib.dgr_ensemble_upload_state(self.ctx, s, _dp(z), _dp(x), _dp(y),
                                                       None if w is None else _ip(w)), "dgr_ensemble_upload_state")
 
     def download_state(self, s: int):
         ne = self.meshes[s].num_el
-        z, x, y = np.empty(3 * ne), np.empty(3 * ne), np.empty(3 * ne)
+        z, x, y = np.empty(self.nm * ne), np.empty(self.nm * ne), np.empty(self.nm * ne)
         w = np.empty(ne, dtype=np.int32)
         _lib.check(self.lib.dgr_ensemble_download_state(self.ctx, s, _dp(z), _dp(x), _dp(y), _ip(w)),
                    "dgr_ensemble_download_state")

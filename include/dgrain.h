@@ -89,6 +89,11 @@ typedef struct dgr_params {
     int rk_stages;   /* 2: SSP-RK2 of 2DCode/time_evolution.c:10-246 (default).  3: SSP(3,3),
                         the coefficients of DG-SWEM src/prep_DG.F:1253-1270 (extension: the
                         limiter, PDop and status follow every stage as in the RK2 order). */
+    int order;       /* 1: 2DCode's p = 1 Crouzeix-Raviart step (default).  2: p = 2 modal DG with
+                        DG-SWEM's orthogonal basis (src/orthobasis_area.F) - an extension for
+                        flows that stay wet: wet_dry must be 0, there is no limiter, and the
+                        state is 6 modal coefficients per element and variable,
+                        zeta[6*el + m] etc. (see dgr_p2_reference). */
 } dgr_params;
 
 /* Mesh in the reference's arrays (2DCode/MeshAttributes.h:5-20), 0-based. */
@@ -321,6 +326,15 @@ DGR_API int dgr_adjoint_timing(const dgr_ctx *ctx, double *forward_ms, double *b
 /* Node depths z [num_nodes] (the fort.14 depth column): recomputes every depth-dependent
  * factor on the device. */
 DGR_API int dgr_set_bathymetry(dgr_ctx *ctx, const double *z);
+
+/* Reference-element tables of the p = 2 step, for projecting fields onto and evaluating
+ * them from the modal coefficients (n >= 234 doubles; no GPU needed):
+ *   [0..6]      area-rule weights (sum 1)      [7..27]     barycentric coordinates [7][3]
+ *   [28..69]    basis at the area points [7][6] [70..111]   d/dr [7][6]   [112..153] d/ds [7][6]
+ *   [154..156]  Gauss points on [-1, 1]        [157..159]  Gauss weights
+ *   [160..213]  basis at the Gauss points of local edge k [3][3][6]   [214..219] int phi_m^2
+ *   [220..233]  reference coordinates (r, s) of the 7 area points [7][2]. */
+DGR_API int dgr_p2_reference(double *tables, int n);
 
 /* Diagnostic: y[i] = x[i]^(4./3) as the kernels evaluate the Manning term of
  * 2DCode/2DInnerProducts.c:318 (correctly rounded; see dgr_device.cuh). */
