@@ -572,11 +572,13 @@ extern "C" int dgr_set_element_manning(dgr_ctx *c, const double *n_el)
 
 /* ------------------------------------------------------------------ state ---- */
 
-static int upload_slice(dgr_ctx *c, int sc, const double *zeta, const double *Qx, const double *Qy, const int *WD)
+/* state of scenarios [s0, s1) from the reference layout (their arrays concatenated) */
+int upload_scenarios(dgr_ctx *c, int s0, int s1, const double *zeta, const double *Qx, const double *Qy,
+                     const int *WD)
 {
-    if (!zeta || !Qx || !Qy || sc < 0 || sc >= c->nscen) return DGR_ERR_INVALID;
+    if (!zeta || !Qx || !Qy || s0 < 0 || s1 > c->nscen || s0 >= s1) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
-    const int n = c->el_off[sc + 1] - c->el_off[sc];
+    const int n = c->el_off[s1] - c->el_off[s0];
     const size_t n3 = (size_t)c->nm * n; /* coefficients per variable */
     double *st = c->W; /* staging: W is free between steps */
     cudaStream_t s = c->stream;
@@ -584,26 +586,33 @@ static int upload_slice(dgr_ctx *c, int sc, const double *zeta, const double *Qx
     CK(cudaMemcpyAsync(st + n3, Qx, n3 * 8, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(st + 2 * n3, Qy, n3 * 8, cudaMemcpyHostToDevice, s));
     k_aos_to_planar_nm<<<blocks(n, 256), 256, 0, s>>>(n, c->ldE, c->nm, st, st + n3, st + 2 * n3,
-                                                      c->U + c->el_off[sc]);
+                                                      c->U + c->el_off[s0]);
     c->launches++;
     /* the other scenarios' current flags must sit in WA as well before WA is marked current */
     if (c->wd_stepped && c->nscen > 1)
         for (int k = 0; k < c->nscen; ++k)
-            if (k != sc)
+            if (k < s0 || k >= s1)
                 CK(cudaMemcpyAsync(c->wdA + c->el_off[k], wd_after_step(c) + c->el_off[k],
                                    (size_t)(c->el_off[k + 1] - c->el_off[k]) * 4, cudaMemcpyDeviceToDevice, s));
-    if (WD) CK(cudaMemcpyAsync(c->wdA + c->el_off[sc], WD, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    if (WD) CK(cudaMemcpyAsync(c->wdA + c->el_off[s0], WD, (size_t)n * 4, cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
-    /* clear the scenario's error word and run state */
+    /* clear the scenarios' error words and run state */
     int r = read_clock(c);
     if (r) return r;
-    c->h_clk[sc].err = ~0ull;
-    c->h_clk[sc].done = 0;
+    for (int k = s0; k < s1; ++k) {
+        c->h_clk[k].err = ~0ull;
+        c->h_clk[k].done = 0;
+    }
     r = write_clock(c);
     if (r) return r;
     c->wd_fresh = 0;
     c->wd_stepped = 0;
     return DGR_OK;
+}
+
+static int upload_slice(dgr_ctx *c, int sc, const double *zeta, const double *Qx, const double *Qy, const int *WD)
+{
+    return upload_scenarios(c, sc, sc + 1, zeta, Qx, Qy, WD);
 }
 
 static int download_slice(dgr_ctx *c, int sc, double *zeta, double *Qx, double *Qy, int *WD)

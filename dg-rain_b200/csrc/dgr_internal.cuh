@@ -160,6 +160,8 @@ static inline int *wd_after_step(const dgr_ctx *c) { return c->p.rk_stages == 3 
 /* dgr_capi.cu */
 void drop_graph(dgr_ctx *c);
 int upload_geometry(dgr_ctx *c);                 /* element geometry planes from x, y, zn, n */
+int upload_scenarios(dgr_ctx *c, int s0, int s1, const double *zeta, const double *Qx, const double *Qy,
+                     const int *WD);             /* state of scenarios [s0, s1), reference layout */
 int read_clock(dgr_ctx *c);                      /* device clocks -> h_clk (synchronises) */
 int write_clock(dgr_ctx *c);                     /* h_clk -> device clocks (synchronises) */
 void launch_stage(dgr_ctx *c, int stage, bool count); /* one RK stage, four kernels */

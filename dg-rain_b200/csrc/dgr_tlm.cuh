@@ -129,34 +129,44 @@ __global__ void __launch_bounds__(128) k_limit_to(MeshDev m, const double *__res
     wd_out[el] = WD ? wd_status(w[0], zn, wd_in[el], h0) : wd_in[el];
 }
 
-/* Start of step n of a recorded run (single mesh): with replay, dt is the recorded one;
- * records the boundary-value time and dt of the step, then clock_begin_body. */
-static __global__ void __launch_bounds__(256) k_adj_clock_begin(DevClock *clk, PhysParams p, const int *__restrict__ bnd_edges,
-                                                         const int *__restrict__ bnd_type, int nbnd,
+/* Start of step n of a recorded run, every scenario: with replay, dt is the recorded one;
+ * records each scenario's boundary-value time and dt of the step (histories [step][nscen]),
+ * then clock_begin_body. */
+static __global__ void __launch_bounds__(256) k_adj_clock_begin(DevClock *clk, int nscen, PhysParams p,
+                                                         const int *__restrict__ bnd_edges,
+                                                         const int *__restrict__ bnd_type,
+                                                         const int *__restrict__ bnd_sid, int nbnd,
                                                          double *__restrict__ bzeta, double *__restrict__ bqn,
                                                          double *dt_hist, double *time_hist, int n, int replay)
 {
-    if (threadIdx.x == 0) {
+    const size_t row = (size_t)n * nscen;
+    for (int s = threadIdx.x; s < nscen; s += blockDim.x) {
         if (replay) {
-            clk->dt = dt_hist[n];
-            clk->dt_pending = 0;
+            clk[s].dt = dt_hist[row + s];
+            clk[s].dt_pending = 0;
         }
-        time_hist[n] = clk->time;
+        time_hist[row + s] = clk[s].time;
     }
     __syncthreads();
-    clock_begin_body(clk, 1, p, bnd_edges, bnd_type, nullptr, nbnd, bzeta, bqn);
-    if (threadIdx.x == 0 && !replay) dt_hist[n] = clk->dt;
+    clock_begin_body(clk, nscen, p, bnd_edges, bnd_type, bnd_sid, nbnd, bzeta, bqn);
+    /* thread s advanced scenario s's clock in clock_begin_body */
+    if (!replay)
+        for (int s = threadIdx.x; s < nscen; s += blockDim.x) dt_hist[row + s] = clk[s].dt;
 }
 
-/* boundary_conditions() at the recorded time of step n */
+/* boundary_conditions() at the recorded time of step n (each prescribed edge at its
+ * scenario's time) */
 static __global__ void __launch_bounds__(256) k_adj_forcing(const DevClock *clk, const double *__restrict__ time_hist, int n,
-                                                     const int *__restrict__ bnd_edges,
-                                                     const int *__restrict__ bnd_type, int nbnd,
+                                                     int nscen, const int *__restrict__ bnd_edges,
+                                                     const int *__restrict__ bnd_type,
+                                                     const int *__restrict__ bnd_sid, int nbnd,
                                                      double *__restrict__ bzeta, double *__restrict__ bqn)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nbnd) return;
-    const double zb2 = dgr_outflow_zeta(time_hist[n], clk->tide_on, clk->tide_amp, clk->tide_period);
+    const int sid = bnd_sid ? bnd_sid[j] : 0;
+    const DevClock *ck = clk + sid;
+    const double zb2 = dgr_outflow_zeta(time_hist[(size_t)n * nscen + sid], ck->tide_on, ck->tide_amp, ck->tide_period);
     const int e = bnd_edges[j];
     const int tt = bnd_type[j];
     double zb = 0, qn = 0;
@@ -168,13 +178,16 @@ static __global__ void __launch_bounds__(256) k_adj_forcing(const DevClock *clk,
 }
 
 /* Gauge residuals of the state after step n: r_g = sum_k w_gk zeta_k(el_g) - target_g
- * (target null: 0).  One warp; the objective is summed later in a fixed order. */
-static __global__ void k_misfit(const double *__restrict__ S, int ld, int ng, const int *__restrict__ g_el,
+ * (target null: 0), nw weights per gauge over the elevation planes 0..nw-1 (the three
+ * midpoint values at p = 1, the six modes at p = 2).  One warp; the objective is summed
+ * later in a fixed order. */
+static __global__ void k_misfit(const double *__restrict__ S, int ld, int nw, int ng, const int *__restrict__ g_el,
                          const double *__restrict__ g_w, const double *__restrict__ target, double *__restrict__ resid)
 {
     for (int g = threadIdx.x; g < ng; g += blockDim.x) {
         const int el = g_el[g];
-        const double z = g_w[3 * g] * S[el] + g_w[3 * g + 1] * S[ld + el] + g_w[3 * g + 2] * S[2 * ld + el];
+        double z = g_w[nw * g] * S[el];
+        for (int k = 1; k < nw; ++k) z += g_w[nw * g + k] * S[(size_t)k * ld + el];
         resid[g] = target ? z - target[g] : z;
     }
 }
@@ -195,27 +208,24 @@ static __global__ void k_misfit_sum(const double *__restrict__ resid, const doub
     out[1] = J2;
 }
 
-/* adjoint of the misfit of step n: lam(zeta) += 2 r_g w_gk at the gauges.  One thread per
+/* adjoint of the misfit of step n: lam(zeta_k) += 2 r_g w_gk at the gauges.  One thread per
  * gauge element (u_el, CSR u_ptr/u_g of its gauges in ascending order), so gauges that share
  * an element are added in a fixed order. */
-static __global__ void k_misfit_rev(double *__restrict__ lam, int ld, int nu, const int *__restrict__ u_el,
+static __global__ void k_misfit_rev(double *__restrict__ lam, int ld, int nw, int nu, const int *__restrict__ u_el,
                                     const int *__restrict__ u_ptr, const int *__restrict__ u_g,
                                     const double *__restrict__ g_w, const double *__restrict__ resid)
 {
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= nu) return;
     const int el = u_el[u];
-    double a0 = lam[el], a1 = lam[ld + el], a2 = lam[2 * ld + el];
-    for (int j = u_ptr[u]; j < u_ptr[u + 1]; ++j) {
-        const int g = u_g[j];
-        const double r2 = 2.0 * resid[g];
-        a0 += r2 * g_w[3 * g];
-        a1 += r2 * g_w[3 * g + 1];
-        a2 += r2 * g_w[3 * g + 2];
+    for (int k = 0; k < nw; ++k) {
+        double a = lam[(size_t)k * ld + el];
+        for (int j = u_ptr[u]; j < u_ptr[u + 1]; ++j) {
+            const int g = u_g[j];
+            a += 2.0 * resid[g] * g_w[nw * g + k];
+        }
+        lam[(size_t)k * ld + el] = a;
     }
-    lam[el] = a0;
-    lam[ld + el] = a1;
-    lam[2 * ld + el] = a2;
 }
 
 /* ==================================================================== tangent ==== */
@@ -274,11 +284,12 @@ __global__ void __launch_bounds__(128) k_tlm_element(MeshDev m, const double *__
                                                      const double *__restrict__ zx, const double *__restrict__ n_el,
                                                      const double *__restrict__ nelx, double *out, double *out_x,
                                                      double *__restrict__ avg, double *__restrict__ avg_x,
-                                                     const DevClock *clk, double g, const double *dt_hist, int n)
+                                                     const DevClock *clk, double g, const double *__restrict__ dt_n)
 {
     const int el = blockIdx.x * blockDim.x + threadIdx.x;
     if (el >= m.ne) return;
     const T *tag = nullptr;
+    const int sid = m.el_sid ? m.el_sid[el] : 0;
     const int ld = m.ldE;
     const double *G = m.geo + el;
     T F[3][3];
@@ -307,7 +318,7 @@ __global__ void __launch_bounds__(128) k_tlm_element(MeshDev m, const double *__
         return lane(tag, U[(3 * v + k) * ld + el], Ux[(3 * v + k) * ld + el]);
     };
     T w[3][3], a[3];
-    element_core<MODE, T>(F, zr, qxr, qyr, geo, zg, uin, local_g, clk->rain, dt_hist[n], w, a);
+    element_core<MODE, T>(F, zr, qxr, qyr, geo, zg, uin, local_g, clk[sid].rain, dt_n[sid], w, a);
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
 #pragma unroll
@@ -484,7 +495,7 @@ __global__ void __launch_bounds__(128, DGR_ADJ_MINB_ELEMENT) k_adj_element(MeshD
                                                      double *lamS, double *lamU, int u_accumulate,
                                                      double *__restrict__ fbar, double *__restrict__ zvb,
                                                      double *__restrict__ nbar, const double *__restrict__ n_el,
-                                                     double g, const double *__restrict__ dt_hist, int n)
+                                                     double g, const double *__restrict__ dt_n)
 {
     const int el = blockIdx.x * blockDim.x + threadIdx.x;
     if (el >= m.ne) return;
@@ -515,7 +526,7 @@ __global__ void __launch_bounds__(128, DGR_ADJ_MINB_ELEMENT) k_adj_element(MeshD
     const PlaneZGeo zg{G, ld};
     double Fb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Sb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     double midzb[3] = {0, 0, 0}, gnnb[3] = {0, 0, 0}, gradzb[2] = {0, 0};
-    element_core_rev<MODE>(wb, zr, qxr, qyr, geo, zg, local_g, dt_hist[n], Fb, Sb, midzb, gnnb, gradzb);
+    element_core_rev<MODE>(wb, zr, qxr, qyr, geo, zg, local_g, dt_n[m.el_sid ? m.el_sid[el] : 0], Fb, Sb, midzb, gnnb, gradzb);
     double cu, cs, cr;
     stage_coefficients(MODE, cu, cs, cr);
 #pragma unroll

@@ -4,7 +4,10 @@ tangent-linear directional derivatives, and a torch.autograd.Function over them.
 
 The objective of a run of nsteps steps from a given state is
     J = sum_n sum_g (zeta_g(u^{n+1}) - target[n, g])^2,
-zeta_g the Crouzeix-Raviart interpolation of the elevation at gauge g's point.  Derivatives
+zeta_g the elevation at gauge g's point: the Crouzeix-Raviart interpolation of the midpoint
+values at p = 1 (place_gauges), the modal expansion at p = 2 (p2.gauge_weights).  On an
+Ensemble the state, gauges and gradients use the flattened numbering (Ensemble.el_off /
+nd_off) and J sums over the scenarios.  Derivatives
 are those of the discrete scheme with its decisions and dt sequence frozen at the recorded
 forward run (the C ABI's dgr_adjoint_* / dgr_tlm); finite differences that should agree
 with them use the same dt sequence (forward(..., replay_dt=True)).
@@ -76,15 +79,18 @@ def intertidal_points(mesh: Mesh, n: int, amp: float, seed: int, max_tries: int 
 
 
 class GaugeMisfit:
-    """J and its derivatives for one Solver (single mesh) over nsteps steps, with a
-    checkpoint every ckpt_every steps."""
+    """J and its derivatives for one Solver or Ensemble over nsteps steps, with a checkpoint
+    every ckpt_every steps."""
 
-    def __init__(self, solver: Solver, nsteps: int, ckpt_every: int, gauge_el, gauge_w, target=None):
+    def __init__(self, solver, nsteps: int, ckpt_every: int, gauge_el, gauge_w, target=None):
         self.solver = solver
         self.lib = solver.lib
         self.nsteps = int(nsteps)
+        self.nm = solver.nm
+        self.ne = solver.ne
+        self.nn = solver.mesh.num_nodes if isinstance(solver, Solver) else solver.nn
         self.el = np.ascontiguousarray(gauge_el, dtype=np.int32)
-        self.w = np.ascontiguousarray(gauge_w, dtype=np.float64).reshape(-1, 3)
+        self.w = np.ascontiguousarray(gauge_w, dtype=np.float64).reshape(-1, self.nm)
         self.ng = int(self.el.shape[0])
         tgt = None if target is None else self._target(target)
         _lib.check(self.lib.dgr_adjoint_setup(solver.ctx, self.nsteps, int(ckpt_every), self.ng, _ip(self.el),
@@ -100,10 +106,10 @@ class GaugeMisfit:
         t = self._target(target)
         _lib.check(self.lib.dgr_adjoint_set_target(self.solver.ctx, _dp(t)), "dgr_adjoint_set_target")
 
-    @staticmethod
-    def _state(state):
+    def _state(self, state):
         z, x, y = (np.ascontiguousarray(a, dtype=np.float64) for a in state[:3])
-        wd = np.ascontiguousarray(state[3] if len(state) > 3 else np.full(z.shape[0] // 3, -1), dtype=np.int32)
+        assert z.shape == x.shape == y.shape == (self.nm * self.ne,)
+        wd = np.ascontiguousarray(state[3] if len(state) > 3 else np.full(self.ne, -1), dtype=np.int32)
         return z, x, y, wd
 
     def forward(self, state, time: float = -1.0, dt: float = 0.0, replay_dt: bool = False):
@@ -119,9 +125,9 @@ class GaugeMisfit:
 
     def backward(self) -> dict:
         """Gradient of the last forward run's J."""
-        ne, nn = self.solver.ne, self.solver.mesh.num_nodes
-        g = {"n_el": np.empty(ne), "z": np.empty(nn), "zeta0": np.empty(3 * ne), "qx0": np.empty(3 * ne),
-             "qy0": np.empty(3 * ne)}
+        ne, nn, nm = self.ne, self.nn, self.nm
+        g = {"n_el": np.empty(ne), "z": np.empty(nn), "zeta0": np.empty(nm * ne), "qx0": np.empty(nm * ne),
+             "qy0": np.empty(nm * ne)}
         self.solver._status(self.lib.dgr_adjoint_backward(self.solver.ctx, _dp(g["n_el"]), _dp(g["z"]),
                                                           _dp(g["zeta0"]), _dp(g["qx0"]), _dp(g["qy0"])),
                             "dgr_adjoint_backward")
@@ -152,10 +158,15 @@ class GaugeMisfit:
         return J.value, Jp.value
 
     def dt_history(self):
-        dt = np.empty(self.nsteps)
-        t = np.empty(self.nsteps)
+        """recorded dt and boundary time per step ([nsteps], or [nsteps, scenarios] for an
+        Ensemble)"""
+        nsc = getattr(self.solver, "n", 1) if not isinstance(self.solver, Solver) else 1
+        dt = np.empty(self.nsteps * nsc)
+        t = np.empty(self.nsteps * nsc)
         _lib.check(self.lib.dgr_adjoint_dt(self.solver.ctx, _dp(dt), _dp(t)), "dgr_adjoint_dt")
-        return dt, t
+        if nsc == 1:
+            return dt, t
+        return dt.reshape(self.nsteps, nsc), t.reshape(self.nsteps, nsc)
 
     def timing(self):
         """device ms of the last forward, backward and tangent-linear runs"""
@@ -170,24 +181,25 @@ def _torch_function():
 
     class MisfitFunction(torch.autograd.Function):
         """J(n_el, z) of a GaugeMisfit from a fixed initial state; backward is the discrete
-        adjoint.  Each backward must follow its own forward (the adjoint replays the last
-        recorded run)."""
+        adjoint.  z None keeps the depths (the only choice on an Ensemble).  Each backward
+        must follow its own forward (the adjoint replays the last recorded run)."""
 
         @staticmethod
         def forward(ctx, n_el, z, misfit, state, time, dt):
             s = misfit.solver
             s.set_element_manning(n_el.detach().cpu().numpy().astype(np.float64))
-            s.set_bathymetry(z.detach().cpu().numpy().astype(np.float64))
+            if z is not None:
+                s.set_bathymetry(z.detach().cpu().numpy().astype(np.float64))
             J, _ = misfit.forward(state, time, dt)
             ctx.misfit = misfit
-            ctx.dev = (n_el.device, z.device)
+            ctx.dev = (n_el.device, None if z is None else z.device)
             return torch.tensor(J, dtype=torch.float64, device=n_el.device)
 
         @staticmethod
         def backward(ctx, gJ):
             g = ctx.misfit.backward()
             gn = torch.from_numpy(g["n_el"]).to(ctx.dev[0]) * gJ
-            gz = torch.from_numpy(g["z"]).to(ctx.dev[1]) * gJ
+            gz = None if ctx.dev[1] is None else torch.from_numpy(g["z"]).to(ctx.dev[1]) * gJ
             return gn, gz, None, None, None, None
 
     return MisfitFunction
@@ -197,7 +209,8 @@ _FN = None
 
 
 def gauge_misfit(n_el, z, misfit: GaugeMisfit, state, time: float = -1.0, dt: float = 0.0):
-    """torch scalar J(n_el, z) differentiable with respect to the two float64 tensors."""
+    """torch scalar J(n_el, z) differentiable with respect to the float64 tensors n_el
+    (per element) and z (per node, or None to keep the depths)."""
     global _FN
     if _FN is None:
         _FN = _torch_function()

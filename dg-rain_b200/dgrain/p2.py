@@ -21,6 +21,34 @@ def reference() -> dict:
             "phie": t[160:214].reshape(3, 3, 6), "mass": t[214:220], "rs": t[220:234].reshape(7, 2)}
 
 
+def basis(r, s) -> np.ndarray:
+    """the six basis functions [..., 6] at reference coordinates (r, s) (closed forms of
+    DG-SWEM src/orthobasis_area.F:18-175 at p = 2, hierarchical order)"""
+    r, s = np.asarray(r, dtype=np.float64), np.asarray(s, dtype=np.float64)
+    A = r + (1.0 + s) / 2
+    B = (1.0 - s) / 2
+    return np.stack([np.ones_like(r), (3 * s + 1) / 2, A, (5 * s * s + 2 * s - 1) / 2, A * (5 * s + 3) / 2,
+                     (3 * A * A - B * B) / 2], axis=-1)
+
+
+def gauge_weights(mesh: Mesh, points) -> tuple[np.ndarray, np.ndarray]:
+    """elements and weights [ng, 6] of gauge points [(x, y), ...]: the basis at the point, so
+    that sum_m w_m zeta_m is the p = 2 elevation there"""
+    from .adjoint import barycentric
+
+    els, ws = [], []
+    for px, py in points:
+        e, lam = barycentric(mesh, px, py)
+        if e < 0:
+            raise ValueError(f"gauge ({px}, {py}) lies outside the mesh")
+        # vertices (-1,-1), (1,-1), (-1,1) of the reference triangle
+        r = -lam[0] + lam[1] - lam[2]
+        s = -lam[0] - lam[1] + lam[2]
+        els.append(e)
+        ws.append(basis(r, s))
+    return np.asarray(els, dtype=np.int32), np.ascontiguousarray(np.asarray(ws, dtype=np.float64))
+
+
 def quadrature_points(mesh: Mesh, ref: dict | None = None):
     """physical coordinates [ne, 7] of every element's area quadrature points and the weights
     [ne, 7] of the physical integral (2 |J| w_q)"""

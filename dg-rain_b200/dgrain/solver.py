@@ -243,6 +243,11 @@ class Ensemble:
                    "dgr_ensemble_create")
         self.ctx = h
         self.n = n
+        # flattened numbering: scenario s's element i is el_off[s] + i (nodes likewise)
+        self.el_off = np.concatenate([[0], np.cumsum([m.num_el for m in self.meshes])]).astype(np.int64)
+        self.nd_off = np.concatenate([[0], np.cumsum([m.num_nodes for m in self.meshes])]).astype(np.int64)
+        self.ne = int(self.el_off[-1])
+        self.nn = int(self.nd_off[-1])
 
     def close(self) -> None:
         if self.ctx:
@@ -292,6 +297,34 @@ class Ensemble:
                         raise StepError(code, index, step, f"ensemble scenario {s}")
             _lib.check(rc, "dgr_ensemble_run")
         return t, d, steps
+
+    def set_element_manning(self, n_el) -> None:
+        """per-element Manning n of every scenario, flattened (scenario order); None: the
+        node-averaged n of each mesh"""
+        if n_el is None:
+            _lib.check(self.lib.dgr_set_element_manning(self.ctx, None), "dgr_set_element_manning")
+            return
+        a = np.ascontiguousarray(n_el, dtype=np.float64)
+        assert a.shape == (self.ne,)
+        _lib.check(self.lib.dgr_set_element_manning(self.ctx, _dp(a)), "dgr_set_element_manning")
+
+    def flatten_states(self, states):
+        """one state per scenario -> the flattened (zeta, Qx, Qy, WD) of the whole ensemble"""
+        parts = [[np.asarray(st[v]) for st in states] for v in range(3)]
+        wd = [np.asarray(st[3], dtype=np.int32) if len(st) > 3 else np.full(m.num_el, -1, dtype=np.int32)
+              for st, m in zip(states, self.meshes)]
+        return tuple(np.ascontiguousarray(np.concatenate(p), dtype=np.float64) for p in parts) + \
+            (np.ascontiguousarray(np.concatenate(wd)),)
+
+    def _status(self, rc: int, where: str) -> None:
+        if rc == _lib.DGR_OK:
+            return
+        if 1 <= rc <= 6:
+            for s in range(self.n):
+                code, index, step = self.last_error(s)
+                if code:
+                    raise StepError(code, index, step, f"{where}, ensemble scenario {s}")
+        _lib.check(rc, where)
 
     def last_error(self, s: int):
         code, index, step = C.c_int(), C.c_int(), C.c_int()

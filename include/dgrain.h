@@ -279,19 +279,25 @@ DGR_API int dgr_profile_step(dgr_ctx *ctx, int nsteps, double *kernel_ms, int n)
 DGR_API int dgr_slope_limiter_noalloc(int num_el, int num_nodes, const int *d_EltoVert, const double *d_z,
                                       double *d_zeta, double *d_Qx, double *d_Qy, double H0, void *stream);
 
-/* ---- discrete adjoint and tangent-linear model (single mesh) ----------------------
+/* ---- discrete adjoint and tangent-linear model (one mesh or an ensemble) ----------
  * Extension: the reference has no derivatives.  Objective over a run of nsteps steps:
  *   J = sum_n sum_g (zeta_g(u^{n+1}) - target[n*ngauges + g])^2,
- *   zeta_g(u) = w[3g] zeta_0 + w[3g+1] zeta_1 + w[3g+2] zeta_2 of element gauge_el[g]
- * (midpoint values; the Crouzeix-Raviart interpolation at a point is such a functional).
+ *   zeta_g(u) = sum_k w[nm*g + k] zeta_k of element gauge_el[g]
+ * with nm = 3 at p = 1 (midpoint values; the Crouzeix-Raviart interpolation at a point is
+ * such a functional) and nm = 6 at p = 2 (modes; the basis at the point).
  * Derivatives are those of the discrete scheme with every decision (wet/dry flags,
  * limiter clamps and redistribution, PDop branches, entropy-fix selections, node max/min
  * elements) and the CFL dt sequence frozen at the recorded forward run.  Parameters: the
  * per-element Manning n (dgr_set_element_manning; required for its gradient), the node
- * depth z (dgr_set_bathymetry) and the initial state. */
+ * depth z (dgr_set_bathymetry, single mesh) and the initial state.
+ * On an ensemble context every scenario runs nsteps steps with its own dt; element and
+ * node indices, states and gradients use the flattened numbering (scenario s's element i
+ * is the sum of the earlier scenarios' element counts plus i; nodes likewise) and J sums
+ * over all scenarios' gauges. */
 
 /* Allocates the adjoint storage: a checkpoint every ckpt_every steps plus a recompute
- * store of ckpt_every steps (about 390 B per element and step); target may be NULL (0). */
+ * store of ckpt_every steps (about 390 B per element and step at p = 1 with RK2, 144 B per
+ * element and stage at p = 2); target may be NULL (0). */
 DGR_API int dgr_adjoint_setup(dgr_ctx *ctx, int nsteps, int ckpt_every, int ngauges, const int *gauge_el,
                               const double *gauge_w, const double *target);
 DGR_API int dgr_adjoint_set_target(dgr_ctx *ctx, const double *target);
@@ -319,7 +325,7 @@ DGR_API int dgr_tlm(dgr_ctx *ctx, const double *zeta, const double *Qx, const do
 DGR_API int dgr_fd_frozen(dgr_ctx *ctx, const double *zeta, const double *Qx, const double *Qy, const int *WD,
                           const double *zeta_p, const double *Qx_p, const double *Qy_p, const double *n_el_p,
                           const double *z_p, double *J, double *J_p);
-/* dt and boundary-value time of every step of the last forward run [nsteps]. */
+/* dt and boundary-value time of every step of the last forward run [nsteps][scenarios]. */
 DGR_API int dgr_adjoint_dt(dgr_ctx *ctx, double *dt, double *time);
 /* Device time in ms of the last forward, backward and tangent-linear runs. */
 DGR_API int dgr_adjoint_timing(const dgr_ctx *ctx, double *forward_ms, double *backward_ms, double *tlm_ms);

@@ -39,3 +39,18 @@ def test_projection_is_exact_for_quadratics(dgrain):
     c = dgrain.p2.project(m, f)
     assert dgrain.p2.l2_error(m, c, f) <= 1e-11 * np.sqrt(1e4 * 5e3)
     assert abs(dgrain.p2.volume(m, dgrain.p2.project(m, lambda x, y: np.ones_like(x))) - 5e7) < 1e-6
+
+
+def test_gauge_weights_are_the_basis_at_the_point(dgrain):
+    """p2.gauge_weights evaluates the basis at a physical point: at an element's area
+    quadrature points it reproduces the kernels' table, and the modal elevation there"""
+    m = dgrain.rectangle(6, 3, jitter=0.2, seed=4)
+    R = dgrain.p2.reference()
+    np.testing.assert_allclose(dgrain.p2.basis(R["rs"][:, 0], R["rs"][:, 1]), R["phi"], atol=1e-15)
+    X, Y, _ = dgrain.p2.quadrature_points(m, R)
+    e = 7
+    el, w = dgrain.p2.gauge_weights(m, list(zip(X[e], Y[e])))
+    assert (el == e).all()
+    np.testing.assert_allclose(w, R["phi"], atol=1e-12)
+    c = dgrain.p2.project(m, lambda x, y: 1 + x / 1e4 - (y / 1e4) ** 2)
+    np.testing.assert_allclose((w * c.reshape(-1, 6)[el]).sum(axis=1), dgrain.p2.evaluate(m, c, R)[e], atol=1e-12)
