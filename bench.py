@@ -324,6 +324,66 @@ def adjoint_bench(steps: int, ckpt: int, fd_dirs: int, device: int = 0, nx: int 
                         "the land film for the depth, best of the two"}
 
 
+def calibration_bench(nscen: int, steps: int, ckpt: int, iterations: int, device: int = 0):
+    """Batched p = 2 SSP(3,3) adjoint calibration workload: nscen submerged basins of
+    log-uniform [20k, 150k] triangles (10 km x 5 km, datum 7 m, tide 0.5 m, a 1 m hump per
+    basin), 32 gauges each, a shared 16-zone Manning field.  Times the plain ensemble device
+    loop, the recorded forward run and the backward sweep of one gradient of the summed
+    misfit (n = 0.04 everywhere, target from the generating field) over `steps` steps with a
+    checkpoint every `ckpt`, checks the zone gradient against the tangent-linear model, and
+    runs `iterations` L-BFGS iterations (0: none)."""
+    import torch
+
+    import dgrain
+    from dgrain import calibration as cb
+
+    t0 = time.perf_counter()
+    meshes, params, states, gauges, zones, n_true = cb.ensemble_workload(nscen)
+    e = dgrain.Ensemble(meshes, params, order=2, wet_dry=0, cfl=0.1, rk_stages=3, device=device)
+    log(f"[bench] calibration: {nscen} p=2 meshes, {e.ne} triangles, built in {time.perf_counter() - t0:.1f} s")
+    for k, st in enumerate(states):
+        e.upload_state(k, *st)
+    n0 = np.full(16, 0.04)
+    cal = cb.setup(e, states, gauges, zones, steps, ckpt)
+    e.set_element_manning(cal.n_elements(n0))
+    e.run(3)
+    for k, st in enumerate(states):
+        e.upload_state(k, *st)
+    torch.cuda.synchronize()
+    _, _, n = e.run(steps)
+    run_ms = e.last_device_ms()
+    if not (n == steps).all():
+        raise RuntimeError("calibration ensemble stopped early")
+    cal.set_target_from(n_true)
+    e.set_element_manning(cal.n_elements(n0))
+    J, _ = cal.misfit.forward(cal.state)
+    g = cal.misfit.backward()
+    fwd_ms, bwd_ms, _ = cal.misfit.timing()
+    gz = np.bincount(cal.zones.numpy(), weights=g["n_el"], minlength=16)
+    rng = np.random.default_rng(1)
+    dzone = rng.normal(size=16)
+    cal.misfit.forward(cal.state)
+    _, dJ = cal.misfit.tlm(cal.state, dn_el=dzone[cal.zones.numpy()])
+    out = {"scenarios": nscen, "triangles": e.ne, "steps": steps, "checkpoint_every": ckpt, "J": J,
+           "plain_run_ms": run_ms, "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+           "adjoint_over_forward": bwd_ms / run_ms,
+           "forward_element_stage_updates_per_s": e.ne * 3 * steps / (run_ms / 1e3),
+           "backward_element_stage_updates_per_s": e.ne * 3 * steps / (bwd_ms / 1e3),
+           "zone_tlm_vs_adjoint": abs(float(gz @ dzone) - dJ) / abs(dJ),
+           "workload": f"{nscen} submerged basins 10 km x 5 km, log-uniform 20k-150k triangles, p=2 modal, "
+                       "SSP(3,3), Roe at 3 Gauss points, CFL 0.1, tide 0.5 m, 1 m hump, 32 gauges each, shared "
+                       "16-zone Manning n (4x4 tiling of normalised coordinates), target from the generating "
+                       "field, gradient at n = 0.04"}
+    if iterations > 0:
+        hist: list = []
+        n_fit = cal.fit(n0, iterations, hist)
+        out.update({"lbfgs_iterations": cal.iterations, "lbfgs_evaluations": cal.evals,
+                    "n_error_initial": cb.relative_error(n0, n_true), "n_error": cb.relative_error(n_fit, n_true),
+                    "J_final": hist[-1][0], "lbfgs_adjoint_to_forward": cal.bwd_ms / cal.fwd_ms})
+    e.close()
+    return out
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -361,6 +421,11 @@ def main():
     ap.add_argument("--adjoint-ckpt", type=int, default=100)
     ap.add_argument("--adjoint-fd", type=int, default=4)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--calib-scenarios", type=int, default=64)
+    ap.add_argument("--calib-steps", type=int, default=200)
+    ap.add_argument("--calib-ckpt", type=int, default=50)
+    ap.add_argument("--calib-iterations", type=int, default=0)
+    ap.add_argument("--no-calibration", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -494,6 +559,12 @@ def main():
         solver.close()
         adj = adjoint_bench(args.adjoint_steps, args.adjoint_ckpt, args.adjoint_fd, device=local)
 
+    cal = None
+    if not args.no_calibration and args.calib_scenarios > 0:
+        solver.close()
+        cal = calibration_bench(args.calib_scenarios, args.calib_steps, args.calib_ckpt, args.calib_iterations,
+                                device=local)
+
     if rank == 0:
         cs = clocks.summary()
         line = {
@@ -515,6 +586,7 @@ def main():
             "clocks": cs,
             "ensemble": ens,
             "adjoint": adj,
+            "calibration": cal,
         }
         print(json.dumps(line), flush=True)
     solver.close()

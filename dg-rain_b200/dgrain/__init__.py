@@ -7,9 +7,10 @@ from .mesh import (Mesh, build_connectivity, initial_state, read_fort14, rectang
                    rectangle_with_elements, write_fort14)
 from .solver import Ensemble, Solver, StepError, default_params
 from .adjoint import GaugeMisfit, cr_weights, gauge_misfit, intertidal_points, place_gauges
+from . import calibration
 
 __all__ = [
-    "_lib", "p2", "DgrError", "load", "Mesh", "build_connectivity", "initial_state", "read_fort14",
+    "_lib", "p2", "calibration", "DgrError", "load", "Mesh", "build_connectivity", "initial_state", "read_fort14",
     "rectangle", "rectangle_with_elements", "write_fort14", "Ensemble", "Solver", "StepError", "default_params",
     "GaugeMisfit", "cr_weights", "gauge_misfit", "intertidal_points", "place_gauges",
 ]
