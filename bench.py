@@ -514,6 +514,7 @@ def main():
         bq = np.zeros(m.num_edges)
         typ = m.bdry
         nbnd = int((typ != 0).sum())
+        tidal = np.nonzero(typ == 2)[0]  # the edges boundary_conditions() rewrites each step
         from dgrain.mesh import _dp, _ip
 
         barrier()
@@ -523,7 +524,7 @@ def main():
         lam = C.c_double()
         for _ in range(args.e2e_steps):
             zb = AMP * np.sin(2 * np.pi * tt / PERIOD)   # boundary_conditions() with the tide
-            bz[typ == 2], bq[typ == 2] = zb, 1e6
+            bz[tidal], bq[tidal] = zb, 1e6
             lib.dgr_set_boundary(solver.ctx, _dp(bz), _dp(bq))
             tt = tt + dtt
             rc = lib.dgr_step(solver.ctx, tt, dtt, C.byref(lam))

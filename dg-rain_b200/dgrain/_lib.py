@@ -103,8 +103,12 @@ SIGNATURES = [
     ("dgr_count_edges", C.c_int, [C.c_int, C.c_int, iptr, iptr]),
     ("dgr_build_connectivity", C.c_int,
      [C.c_int, C.c_int, iptr, dptr, dptr, C.c_int, iptr, C.c_int, iptr, C.c_int, iptr, iptr, iptr, iptr, dptr]),
+    ("dgr_build_connectivity_device", C.c_int,
+     [C.c_int, C.c_int, iptr, dptr, dptr, C.c_int, iptr, C.c_int, iptr, C.c_int, iptr, iptr, iptr, iptr, dptr]),
     ("dgr_initial_state", C.c_int, [C.c_int, iptr, dptr, dptr, dptr, dptr, iptr]),
     ("dgr_write_dat", C.c_int, [C.c_char_p, C.c_int, dptr]),
+    ("dgr_write_state_dat", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p]),
+    ("dgr_ensemble_write_state_dat", C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_char_p, C.c_char_p]),
     ("dgr_host_alloc", C.c_void_p, [C.c_size_t]),
     ("dgr_host_free", None, [C.c_void_p]),
     ("dgr_params_default", C.c_int, [C.POINTER(DgrParams)]),

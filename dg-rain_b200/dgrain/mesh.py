@@ -133,18 +133,23 @@ def rectangle(nx: int, ny: int, lx: float = 10000.0, ly: float = 5000.0, jitter:
     return m
 
 
-def build_connectivity(m: Mesh) -> Mesh:
+def build_connectivity(m: Mesh, device: bool = False) -> Mesh:
     """EdgtoVert/EdgtoEls/BdryPrescribed/minEdgLength exactly as
-    2DCode/extract_mesh_attributes.c:143-361 numbers them (native, hashed)."""
+    2DCode/extract_mesh_attributes.c:143-361 numbers them (native, hashed; device=True:
+    sorted on the current GPU, same arrays)."""
     lib = _lib.load()
-    nf = C.c_int(0)
-    _lib.check(lib.dgr_count_edges(m.num_el, m.num_nodes, _ip(m.el2v), C.byref(nf)), "dgr_count_edges")
-    nf = nf.value
+    if device:
+        nf = m.num_nodes + m.num_el - 1  # Euler's relation, checked by the builder
+    else:
+        nf = C.c_int(0)
+        _lib.check(lib.dgr_count_edges(m.num_el, m.num_nodes, _ip(m.el2v), C.byref(nf)), "dgr_count_edges")
+        nf = nf.value
     ed2v = np.zeros((nf, 2), dtype=np.int32)
     ed2el = np.zeros((nf, 2), dtype=np.int32)
     bdry = np.zeros(nf, dtype=np.int32)
     me = C.c_double(0.0)
-    _lib.check(lib.dgr_build_connectivity(
+    fn = lib.dgr_build_connectivity_device if device else lib.dgr_build_connectivity
+    _lib.check(fn(
         m.num_el, m.num_nodes, _ip(m.el2v), _dp(m.x), _dp(m.y),
         len(m.inflow1), _ip(m.inflow1), len(m.inflow2), _ip(m.inflow2), len(m.outflow), _ip(m.outflow),
         _ip(ed2v), _ip(ed2el), _ip(bdry), C.byref(me)), "dgr_build_connectivity")

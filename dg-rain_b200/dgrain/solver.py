@@ -103,6 +103,12 @@ class Solver:
         _lib.check(self.lib.dgr_download_state(self.ctx, _dp(z), _dp(x), _dp(y), _ip(w)), "dgr_download_state")
         return z, x, y, w
 
+    def write_state_dat(self, zeta_path=None, qx_path=None, qy_path=None) -> None:
+        """the current state as the reference's .dat snapshot files, formatted on the device"""
+        enc = lambda p: None if p is None else str(p).encode()  # noqa: E731
+        _lib.check(self.lib.dgr_write_state_dat(self.ctx, enc(zeta_path), enc(qx_path), enc(qy_path)),
+                   "dgr_write_state_dat")
+
     def set_boundary(self, bzeta, bqn) -> None:
         bz = np.ascontiguousarray(bzeta, dtype=np.float64)
         bq = np.ascontiguousarray(bqn, dtype=np.float64)
@@ -297,6 +303,12 @@ class Ensemble:
                         raise StepError(code, index, step, f"ensemble scenario {s}")
             _lib.check(rc, "dgr_ensemble_run")
         return t, d, steps
+
+    def write_state_dat(self, s: int, zeta_path=None, qx_path=None, qy_path=None) -> None:
+        """scenario s's current state as .dat snapshot files, formatted on the device"""
+        enc = lambda p: None if p is None else str(p).encode()  # noqa: E731
+        _lib.check(self.lib.dgr_ensemble_write_state_dat(self.ctx, s, enc(zeta_path), enc(qx_path), enc(qy_path)),
+                   "dgr_ensemble_write_state_dat")
 
     def set_element_manning(self, n_el) -> None:
         """per-element Manning n of every scenario, flattened (scenario order); None: the

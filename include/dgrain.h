@@ -153,6 +153,13 @@ DGR_API int dgr_build_connectivity(int num_el, int num_nodes, const int *EltoVer
                            int num_outflow, const int *outflow,
                            int *EdgtoVert, int *EdgtoEls, int *BdryPrescribed,
                            double *minEdgLength);
+/* The same arrays, bit for bit, built on the current CUDA device by sorting (mesh ingest on
+ * the GPU; same arguments, host arrays in and out).  Every element must have three
+ * distinct vertices (else DGR_ERR_MESH) and 6 x num_el must stay below 2^31. */
+DGR_API int dgr_build_connectivity_device(int num_el, int num_nodes, const int *EltoVert, const double *x,
+                                          const double *y, int n_inflow1, const int *inflow1, int n_inflow2,
+                                          const int *inflow2, int n_outflow, const int *outflow, int *EdgtoVert,
+                                          int *EdgtoEls, int *BdryPrescribed, double *minEdgLength);
 
 /* initialize (2DCode/initialize.c:117-126): nodal elevations averaged onto the edge
  * midpoints, zero discharge, WD = -1.  zeta_nodal == NULL gives the reference's 0.1. */
@@ -162,6 +169,16 @@ DGR_API int dgr_initial_state(int num_el, const int *EltoVert, const double *zet
 /* Writes one .dat file in the reference format (time_evolution.c:284-306,363-386):
  * one element per line, its three values as "%1.15f\t\t". */
 DGR_API int dgr_write_dat(const char *path, int num_el, const double *values);
+
+/* The context's current state as .dat files in the same format, formatted on the device
+ * (the reference's snapshot writer, time_evolution.c:324-390, runs printf on the host):
+ * zeta_path / qx_path / qy_path (any may be NULL) receive one element per line, its values
+ * as "%1.15f\t\t", byte-identical to dgr_write_dat of the downloaded arrays.  At p = 2 a
+ * line holds the element's six modal coefficients.  A value of magnitude >= 2^63 is not
+ * formatted: DGR_ERR_INVALID, and that file is removed. */
+DGR_API int dgr_write_state_dat(dgr_ctx *ctx, const char *zeta_path, const char *qx_path, const char *qy_path);
+DGR_API int dgr_ensemble_write_state_dat(dgr_ctx *ctx, int scenario, const char *zeta_path, const char *qx_path,
+                                         const char *qy_path);
 
 /* Page-locked host memory for fast copies (cudaHostAlloc); NULL on failure. */
 DGR_API void *dgr_host_alloc(size_t bytes);
