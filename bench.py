@@ -384,6 +384,46 @@ def calibration_bench(nscen: int, steps: int, ckpt: int, iterations: int, device
     return out
 
 
+def io_bench(m, solver, outdir: str):
+    """Mesh ingest and snapshot output on the bench mesh: connectivity by the host builder
+    (hashed, O(E)) and by the GPU builder (sorted), identical arrays required; the three
+    .dat snapshot files of the current state written by the device formatter and by the host
+    writer (download + printf), identical bytes required."""
+    import copy
+
+    import dgrain
+
+    base = copy.deepcopy(m)
+    t0 = time.perf_counter()
+    a = dgrain.build_connectivity(copy.deepcopy(base))
+    host_s = time.perf_counter() - t0
+    dgrain.build_connectivity(copy.deepcopy(base), device=True)  # first call: module load
+    t0 = time.perf_counter()
+    b = dgrain.build_connectivity(copy.deepcopy(base), device=True)
+    dev_s = time.perf_counter() - t0
+    same_mesh = all(np.array_equal(getattr(a, k), getattr(b, k)) for k in ("ed2v", "ed2el", "bdry")) and \
+        a.min_edge == b.min_edge
+    os.makedirs(outdir, exist_ok=True)
+    paths = [os.path.join(outdir, f"dev_{v}.dat") for v in ("H", "Qx", "Qy")]
+    t0 = time.perf_counter()
+    solver.write_state_dat(*paths)
+    dev_w = time.perf_counter() - t0
+    lib = dgrain.load()
+    t0 = time.perf_counter()
+    st = solver.download_state()
+    hpaths = [os.path.join(outdir, f"host_{v}.dat") for v in ("H", "Qx", "Qy")]
+    for p, v in zip(hpaths, st[:3]):
+        lib.dgr_write_dat(p.encode(), m.num_el, v.ctypes.data_as(dgrain._lib.dptr))
+    host_w = time.perf_counter() - t0
+    same_dat = all(open(p, "rb").read() == open(q, "rb").read() for p, q in zip(paths, hpaths))
+    nbytes = sum(os.path.getsize(p) for p in paths)
+    for p in paths + hpaths:
+        os.remove(p)
+    return {"triangles": m.num_el, "connectivity_host_s": host_s, "connectivity_device_s": dev_s,
+            "connectivity_identical": bool(same_mesh), "dat_device_s": dev_w, "dat_host_s": host_w,
+            "dat_bytes": nbytes, "dat_identical": bool(same_dat)}
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -426,6 +466,7 @@ def main():
     ap.add_argument("--calib-ckpt", type=int, default=50)
     ap.add_argument("--calib-iterations", type=int, default=0)
     ap.add_argument("--no-calibration", action="store_true")
+    ap.add_argument("--io", action="store_true", help="add the mesh-ingest and .dat-writer comparison")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -546,6 +587,8 @@ def main():
             lib.dgr_host_free(C.c_void_p(host[k].ctypes.data))
         lib.dgr_host_free(C.c_void_p(wdp))
 
+    io = io_bench(m, solver, os.path.join("gpurun_out", "io_tmp")) if args.io and rank == 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_reference(m, st)
@@ -572,7 +615,8 @@ def main():
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "coastal rectangle 2000x1000 cells (10 km x 5 km), 4,000,000 triangles, "
+            "config": {"workload": f"coastal rectangle {args.nx}x{args.ny} cells (10 km x 5 km), "
+                                   f"{m.num_el:,} triangles, "
                                    "jitter 0.1, p=1 CR/RT0, SSP-RK2, Roe, vertex limiter, wet/dry on, "
                                    "tide 0.5 m / 12.42 h, Manning 0.03, CFL 0.3, FP64",
                        "num_el": m.num_el, "num_edges": m.num_edges, "parallelism": f"replicas x{world}",
@@ -588,6 +632,7 @@ def main():
             "ensemble": ens,
             "adjoint": adj,
             "calibration": cal,
+            "io": io,
         }
         print(json.dumps(line), flush=True)
     solver.close()

@@ -25,6 +25,15 @@
 
 namespace dgr {
 
+/* Minimum resident blocks per SM requested for the p = 2 kernels (register caps 65536 /
+ * (block size x blocks)); overridable at build time for tuning sweeps. */
+#ifndef DGR_P2_MINB_EDGE
+#define DGR_P2_MINB_EDGE 1
+#endif
+#ifndef DGR_P2_MINB_ELEMENT
+#define DGR_P2_MINB_ELEMENT 1
+#endif
+
 constexpr int P2_NM = 6;       /* modes per variable */
 constexpr int P2_NQ = 7;       /* area quadrature points */
 constexpr int P2_NGP = 3;      /* Gauss points per edge */
@@ -217,7 +226,7 @@ struct P2PlaneZ {
 /* --------------------------------------------------------------- kernels ---- */
 
 template <int BS>
-__global__ void __launch_bounds__(BS) k_p2_edge(P2Ref ref, MeshDev m, const double *__restrict__ p2g,
+__global__ void __launch_bounds__(BS, DGR_P2_MINB_EDGE) k_p2_edge(P2Ref ref, MeshDev m, const double *__restrict__ p2g,
                                                 const double *__restrict__ S, const double *__restrict__ bzeta,
                                                 const double *__restrict__ bqn, double *__restrict__ flux,
                                                 DevClock *clk, int lam_slot, int phase, double g)
@@ -275,7 +284,7 @@ DGR_HD void p2_gather_flux(const MeshDev &m, int el, const FluxLoad &fl, T F[3][
 }
 
 template <int MODE, int BS>
-__global__ void __launch_bounds__(BS) k_p2_element(P2Ref ref, MeshDev m, const double *__restrict__ p2g,
+__global__ void __launch_bounds__(BS, DGR_P2_MINB_ELEMENT) k_p2_element(P2Ref ref, MeshDev m, const double *__restrict__ p2g,
                                                    const double *__restrict__ S, const double *__restrict__ U,
                                                    const double *__restrict__ flux, double *__restrict__ out,
                                                    const DevClock *clk, double g)

@@ -20,6 +20,14 @@
 #include "dgr_p2.cuh"
 #include "dgr_tlm.cuh"
 
+/* minimum resident blocks per SM of the p = 2 reverse kernels (see dgr_p2.cuh) */
+#ifndef DGR_P2_MINB_ADJ_ELEMENT
+#define DGR_P2_MINB_ADJ_ELEMENT 1
+#endif
+#ifndef DGR_P2_MINB_ADJ_EDGE
+#define DGR_P2_MINB_ADJ_EDGE 1
+#endif
+
 namespace dgr {
 
 /* ==================================================================== tangent ==== */
@@ -240,7 +248,7 @@ DGR_HD void p2_dz_rev(double rx, double ry, double sx, double sy, const double d
  * stage): every element reads its own columns before writing them.
  */
 template <int MODE>
-__global__ void __launch_bounds__(128) k_p2_adj_element(P2Ref ref, MeshDev m, const double *__restrict__ p2g,
+__global__ void __launch_bounds__(128, DGR_P2_MINB_ADJ_ELEMENT) k_p2_adj_element(P2Ref ref, MeshDev m, const double *__restrict__ p2g,
                                                         const double *__restrict__ S, const double *lamO, double *lamS,
                                                         double *lamU, int u_accumulate, double *__restrict__ fbar,
                                                         double *__restrict__ zvb, double *__restrict__ nbar,
@@ -326,7 +334,7 @@ __global__ void __launch_bounds__(128) k_p2_adj_element(P2Ref ref, MeshDev m, co
  * the flux adjoints in fbar, and the adjoints of the Gauss-point depths go to the edge's
  * end vertices (zeb).
  */
-static __global__ void __launch_bounds__(128) k_p2_adj_edge(P2Ref ref, MeshDev m, const double *__restrict__ p2g,
+static __global__ void __launch_bounds__(128, DGR_P2_MINB_ADJ_EDGE) k_p2_adj_edge(P2Ref ref, MeshDev m, const double *__restrict__ p2g,
                                                             const double *__restrict__ S,
                                                             const double *__restrict__ bzeta,
                                                             const double *__restrict__ bqn, double *__restrict__ fbar,
