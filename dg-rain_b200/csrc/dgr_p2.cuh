@@ -26,12 +26,14 @@
 namespace dgr {
 
 /* Minimum resident blocks per SM requested for the p = 2 kernels (register caps 65536 /
- * (block size x blocks)); overridable at build time for tuning sweeps. */
+ * (block size x blocks): 128 for the element kernel, 102 for the edge kernel at 128
+ * threads).  Chosen by a measured sweep (1.3 M triangles, SSP(3,3): 14 % faster than the
+ * uncapped 242 / 150 registers despite the spills); overridable at build time. */
 #ifndef DGR_P2_MINB_EDGE
-#define DGR_P2_MINB_EDGE 1
+#define DGR_P2_MINB_EDGE 5
 #endif
 #ifndef DGR_P2_MINB_ELEMENT
-#define DGR_P2_MINB_ELEMENT 1
+#define DGR_P2_MINB_ELEMENT 4
 #endif
 
 constexpr int P2_NM = 6;       /* modes per variable */
