@@ -78,7 +78,8 @@ static void release(dgr_ctx *c)
     void *ptrs[] = {c->x, c->y, c->zn, c->nfric, c->n_el, c->el2v_aos, c->el2v, c->elem_edge, c->e_in,
                     c->e_ex, c->e_info, c->n2e_ptr, c->n2e, c->bnd_edges, c->bnd_type, c->bnd_sid, c->bdry,
                     c->el_sid, c->ed_sid, c->e_geo, c->geo, c->U, c->W, c->flux, c->avg, c->bounds, c->bzeta,
-                    c->bqn, c->bstage, c->wdA, c->wdB, c->wdC, c->dec, c->bar, c->clk, c->p2g};
+                    c->bqn, c->bstage, c->wdA, c->wdB, c->wdC, c->dec, c->bar, c->clk, c->p2g,
+                    c->gauge_el, c->gauge_sid, c->gauge_w, c->gauge_series};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     adjoint_release(c);
@@ -895,26 +896,35 @@ static cudaError_t launch_step(dgr_ctx *c)
     cudaStream_t s = c->stream;
     const PhysParams p = phys(c);
     const int ns = c->p.rk_stages;
-    if (c->fusion == 2 && c->p.order == 1) return launch_fused(c, 0, ns, 1);
-    k_clock_begin<<<1, 256, 0, s>>>(c->clk, c->nscen, p, c->bnd_edges, c->bnd_type, c->bnd_sid, c->nbnd, c->bzeta,
-                                    c->bqn);
-    for (int st = 0; st < ns; ++st) {
-        if (c->fusion == 1 && c->p.order == 1) {
-            cudaError_t e = launch_fused(c, st, st + 1, 0);
-            if (e != cudaSuccess) return e;
-        } else {
-            launch_stage(c, st, false);
+    if (c->fusion == 2 && c->p.order == 1) {
+        cudaError_t e = launch_fused(c, 0, ns, 1);
+        if (e != cudaSuccess) return e;
+    } else {
+        k_clock_begin<<<1, 256, 0, s>>>(c->clk, c->nscen, p, c->bnd_edges, c->bnd_type, c->bnd_sid, c->nbnd,
+                                        c->bzeta, c->bqn);
+        for (int st = 0; st < ns; ++st) {
+            if (c->fusion == 1 && c->p.order == 1) {
+                cudaError_t e = launch_fused(c, st, st + 1, 0);
+                if (e != cudaSuccess) return e;
+            } else {
+                launch_stage(c, st, false);
+            }
         }
+        k_clock_end<<<blocks(c->nscen, 256), 256, 0, s>>>(c->clk, c->nscen);
     }
-    k_clock_end<<<blocks(c->nscen, 256), 256, 0, s>>>(c->clk, c->nscen);
+    if (c->gauge_n)
+        k_gauge_record<<<blocks(c->gauge_n, 128), 128, 0, s>>>(c->U, c->ldE, c->nm, c->gauge_n, c->gauge_el,
+                                                               c->gauge_sid, c->gauge_w, c->clk, c->gauge_cap,
+                                                               c->gauge_series);
     return cudaGetLastError();
 }
 
 static int kernels_per_step(const dgr_ctx *c)
 {
     const int ns = c->p.rk_stages;
-    if (c->p.order == 2) return 2 + 2 * ns;
-    return c->fusion == 2 ? 1 : (c->fusion == 1 ? 2 + ns : 2 + 4 * ns);
+    const int rec = c->gauge_n ? 1 : 0;
+    if (c->p.order == 2) return 2 + 2 * ns + rec;
+    return rec + (c->fusion == 2 ? 1 : (c->fusion == 1 ? 2 + ns : 2 + 4 * ns));
 }
 
 int decode_err(unsigned long long key, int *code, int *index, int *step)
@@ -1501,5 +1511,53 @@ extern "C" int dgr_pow43_batch(const double *x, double *y, int n, int device)
         snprintf(dgr_cuda_err_buffer(), 256, "pow43: %s", cudaGetErrorString(e));
         return DGR_ERR_CUDA;
     }
+    return DGR_OK;
+}
+
+/* --------------------------------------------------------------- gauges ---- */
+
+extern "C" int dgr_set_gauges(dgr_ctx *c, int ngauges, const int *gauge_el, const double *gauge_w, int capacity)
+{
+    if (!c || ngauges < 0 || (ngauges > 0 && (!gauge_el || !gauge_w || capacity <= 0))) return DGR_ERR_INVALID;
+    for (int g = 0; g < ngauges; ++g)
+        if (gauge_el[g] < 0 || gauge_el[g] >= c->ne) return DGR_ERR_INVALID;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    drop_graph(c); /* the step graph gains or loses the recording kernel */
+    int *ptrs_i[2] = {c->gauge_el, c->gauge_sid};
+    for (int *q : ptrs_i)
+        if (q) cudaFree(q);
+    if (c->gauge_w) cudaFree(c->gauge_w);
+    if (c->gauge_series) cudaFree(c->gauge_series);
+    c->gauge_el = c->gauge_sid = nullptr;
+    c->gauge_w = c->gauge_series = nullptr;
+    c->gauge_n = c->gauge_cap = 0;
+    if (ngauges == 0) return DGR_OK;
+    std::vector<int> sid(ngauges);
+    for (int g = 0; g < ngauges; ++g) {
+        int k = 0;
+        while (k + 1 < c->nscen && gauge_el[g] >= c->el_off[k + 1]) ++k;
+        sid[g] = k;
+    }
+    int r = 0;
+    if ((r = dalloc(&c->gauge_el, ngauges)) || (r = dalloc(&c->gauge_sid, ngauges)) ||
+        (r = dalloc(&c->gauge_w, (size_t)ngauges * c->nm)) ||
+        (r = dalloc(&c->gauge_series, (size_t)ngauges * capacity)))
+        return r;
+    CK(cudaMemcpy(c->gauge_el, gauge_el, (size_t)ngauges * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->gauge_sid, sid.data(), (size_t)ngauges * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->gauge_w, gauge_w, (size_t)ngauges * c->nm * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemset(c->gauge_series, 0, (size_t)ngauges * capacity * 8));
+    c->gauge_n = ngauges;
+    c->gauge_cap = capacity;
+    return DGR_OK;
+}
+
+extern "C" int dgr_get_gauge_series(dgr_ctx *c, double *values)
+{
+    if (!c || !values || !c->gauge_n) return DGR_ERR_INVALID;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaMemcpy(values, c->gauge_series, (size_t)c->gauge_n * c->gauge_cap * 8, cudaMemcpyDeviceToHost));
     return DGR_OK;
 }

@@ -90,6 +90,10 @@ struct dgr_ctx {
     cudaGraph_t graph;
     cudaGraphExec_t graph_exec;
     dgr::AdjointState *adj; /* discrete adjoint storage, created on first use */
+    /* gauge series recorded by the device loop (dgr_set_gauges) */
+    int gauge_n, gauge_cap;
+    int *gauge_el, *gauge_sid;
+    double *gauge_w, *gauge_series; /* weights [n][nm], series [cap][n] */
 };
 
 static inline dgr::MeshDev mesh_dev(const dgr_ctx *c)

@@ -440,6 +440,23 @@ static __global__ void k_clock_finish(DevClock *clk, int nscen, PhysParams p)
     }
 }
 
+/* Gauge values after a step of the device loop: row (step - 1) of the series holds
+ * zeta_g = sum_k w[nm g + k] zeta_k(el_g) for the step count of the gauge's scenario (a
+ * finished scenario rewrites its last row with the same state). */
+static __global__ void k_gauge_record(const double *__restrict__ S, int ld, int nm, int ng, const int *__restrict__ g_el,
+                                      const int *__restrict__ g_sid, const double *__restrict__ g_w,
+                                      const DevClock *clk, int cap, double *__restrict__ series)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ng) return;
+    const int step = clk[g_sid[g]].step;
+    if (step < 1 || step > cap) return;
+    const int el = g_el[g];
+    double z = g_w[nm * g] * S[el];
+    for (int k = 1; k < nm; ++k) z += g_w[nm * g + k] * S[(size_t)k * ld + el];
+    series[(size_t)(step - 1) * ng + g] = z;
+}
+
 /* Host-driven step (oneTimeStep2D, single mesh): set the step's dt, clear per-step words. */
 static __global__ void k_clock_set(DevClock *clk, double time, double dt)
 {

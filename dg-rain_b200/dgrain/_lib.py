@@ -108,6 +108,8 @@ SIGNATURES = [
     ("dgr_initial_state", C.c_int, [C.c_int, iptr, dptr, dptr, dptr, dptr, iptr]),
     ("dgr_write_dat", C.c_int, [C.c_char_p, C.c_int, dptr]),
     ("dgr_write_state_dat", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p]),
+    ("dgr_set_gauges", C.c_int, [C.c_void_p, C.c_int, iptr, dptr, C.c_int]),
+    ("dgr_get_gauge_series", C.c_int, [C.c_void_p, dptr]),
     ("dgr_ensemble_write_state_dat", C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_char_p, C.c_char_p]),
     ("dgr_host_alloc", C.c_void_p, [C.c_size_t]),
     ("dgr_host_free", None, [C.c_void_p]),

@@ -103,6 +103,25 @@ class Solver:
         _lib.check(self.lib.dgr_download_state(self.ctx, _dp(z), _dp(x), _dp(y), _ip(w)), "dgr_download_state")
         return z, x, y, w
 
+    def set_gauges(self, gauge_el, gauge_w, capacity: int) -> None:
+        """record the elevation at the gauges after every step of the device loop (up to
+        `capacity` steps per run); gauge_el None removes them"""
+        if gauge_el is None:
+            _lib.check(self.lib.dgr_set_gauges(self.ctx, 0, None, None, 0), "dgr_set_gauges")
+            self._gauges = None
+            return
+        el = np.ascontiguousarray(gauge_el, dtype=np.int32)
+        w = np.ascontiguousarray(gauge_w, dtype=np.float64).reshape(len(el), self.nm)
+        _lib.check(self.lib.dgr_set_gauges(self.ctx, len(el), _ip(el), _dp(w), int(capacity)), "dgr_set_gauges")
+        self._gauges = (len(el), int(capacity))
+
+    def gauge_series(self) -> np.ndarray:
+        """[capacity, ngauges] values recorded by the last run"""
+        ng, cap = self._gauges
+        out = np.empty((cap, ng))
+        _lib.check(self.lib.dgr_get_gauge_series(self.ctx, _dp(out)), "dgr_get_gauge_series")
+        return out
+
     def write_state_dat(self, zeta_path=None, qx_path=None, qy_path=None) -> None:
         """the current state as the reference's .dat snapshot files, formatted on the device"""
         enc = lambda p: None if p is None else str(p).encode()  # noqa: E731
@@ -303,6 +322,25 @@ class Ensemble:
                         raise StepError(code, index, step, f"ensemble scenario {s}")
             _lib.check(rc, "dgr_ensemble_run")
         return t, d, steps
+
+    def set_gauges(self, gauge_el, gauge_w, capacity: int) -> None:
+        """record the elevation at the gauges after every step of the device loop (up to
+        `capacity` steps per run); gauge_el None removes them"""
+        if gauge_el is None:
+            _lib.check(self.lib.dgr_set_gauges(self.ctx, 0, None, None, 0), "dgr_set_gauges")
+            self._gauges = None
+            return
+        el = np.ascontiguousarray(gauge_el, dtype=np.int32)
+        w = np.ascontiguousarray(gauge_w, dtype=np.float64).reshape(len(el), self.nm)
+        _lib.check(self.lib.dgr_set_gauges(self.ctx, len(el), _ip(el), _dp(w), int(capacity)), "dgr_set_gauges")
+        self._gauges = (len(el), int(capacity))
+
+    def gauge_series(self) -> np.ndarray:
+        """[capacity, ngauges] values recorded by the last run"""
+        ng, cap = self._gauges
+        out = np.empty((cap, ng))
+        _lib.check(self.lib.dgr_get_gauge_series(self.ctx, _dp(out)), "dgr_get_gauge_series")
+        return out
 
     def write_state_dat(self, s: int, zeta_path=None, qx_path=None, qy_path=None) -> None:
         """scenario s's current state as .dat snapshot files, formatted on the device"""

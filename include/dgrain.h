@@ -180,6 +180,17 @@ DGR_API int dgr_write_state_dat(dgr_ctx *ctx, const char *zeta_path, const char 
 DGR_API int dgr_ensemble_write_state_dat(dgr_ctx *ctx, int scenario, const char *zeta_path, const char *qx_path,
                                          const char *qy_path);
 
+/* Gauge time series recorded by the device loop (dgr_run / dgr_ensemble_run): after each
+ * step, for gauge g in element gauge_el[g] (flattened numbering on an ensemble),
+ * zeta_g = sum_k gauge_w[nm*g + k] zeta_k (nm = 3 midpoint values at p = 1, 6 modes at
+ * p = 2) is stored in row (step - 1) of a device series [capacity][ngauges], step being the
+ * gauge's scenario's step count in the current run; steps past capacity are not recorded.
+ * ngauges = 0 removes the gauges.  The state never leaves the device for them. */
+DGR_API int dgr_set_gauges(dgr_ctx *ctx, int ngauges, const int *gauge_el, const double *gauge_w, int capacity);
+/* The recorded series [capacity][ngauges]: rows below the steps each scenario took in the
+ * last run are that run's values. */
+DGR_API int dgr_get_gauge_series(dgr_ctx *ctx, double *values);
+
 /* Page-locked host memory for fast copies (cudaHostAlloc); NULL on failure. */
 DGR_API void *dgr_host_alloc(size_t bytes);
 DGR_API void dgr_host_free(void *p);
