@@ -324,27 +324,33 @@ def adjoint_bench(steps: int, ckpt: int, fd_dirs: int, device: int = 0, nx: int 
                         "the land film for the depth, best of the two"}
 
 
-def calibration_bench(nscen: int, steps: int, ckpt: int, iterations: int, device: int = 0):
+def calibration_bench(nscen: int, steps: int, ckpt: int, iterations: int, device: int = 0, dist=None):
     """Batched p = 2 SSP(3,3) adjoint calibration workload: nscen submerged basins of
     log-uniform [20k, 150k] triangles (10 km x 5 km, datum 7 m, tide 0.5 m, a 1 m hump per
     basin), 32 gauges each, a shared 16-zone Manning field.  Times the plain ensemble device
     loop, the recorded forward run and the backward sweep of one gradient of the summed
     misfit (n = 0.04 everywhere, target from the generating field) over `steps` steps with a
     checkpoint every `ckpt`, checks the zone gradient against the tangent-linear model, and
-    runs `iterations` L-BFGS iterations (0: none)."""
+    runs `iterations` L-BFGS iterations (0: none).  With several ranks (dist), each owns a
+    share of the scenarios balanced by element count; J and the zone gradient are summed
+    over the ranks (NCCL all-reduce), times are the maximum over ranks."""
     import torch
 
     import dgrain
     from dgrain import calibration as cb
 
+    world = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
     t0 = time.perf_counter()
-    meshes, params, states, gauges, zones, n_true = cb.ensemble_workload(nscen)
+    share = cb.partition(cb.workload_counts(nscen), world)[rank]
+    meshes, params, states, gauges, zones, n_true = cb.ensemble_workload(nscen, subset=share)
     e = dgrain.Ensemble(meshes, params, order=2, wet_dry=0, cfl=0.1, rk_stages=3, device=device)
     log(f"[bench] calibration: {nscen} p=2 meshes, {e.ne} triangles, built in {time.perf_counter() - t0:.1f} s")
     for k, st in enumerate(states):
         e.upload_state(k, *st)
     n0 = np.full(16, 0.04)
-    cal = cb.setup(e, states, gauges, zones, steps, ckpt)
+    group = dist.group.WORLD if dist is not None else None
+    cal = cb.setup(e, states, gauges, zones, steps, ckpt, group=group)
     e.set_element_manning(cal.n_elements(n0))
     e.run(3)
     for k, st in enumerate(states):
@@ -364,16 +370,28 @@ def calibration_bench(nscen: int, steps: int, ckpt: int, iterations: int, device
     dzone = rng.normal(size=16)
     cal.misfit.forward(cal.state)
     _, dJ = cal.misfit.tlm(cal.state, dn_el=dzone[cal.zones.numpy()])
-    out = {"scenarios": nscen, "triangles": e.ne, "steps": steps, "checkpoint_every": ckpt, "J": J,
+    local = np.array([J, float(gz @ dzone), dJ, float(e.ne)])
+    times = np.array([run_ms, fwd_ms, bwd_ms])
+    if dist is not None:
+        t = torch.tensor(local, dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        local = t.cpu().numpy()
+        t = torch.tensor(times, dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        times = t.cpu().numpy()
+    J, adj, dJ, ne = local
+    run_ms, fwd_ms, bwd_ms = times
+    ne = int(ne)
+    out = {"scenarios": nscen, "ranks": world, "triangles": ne, "steps": steps, "checkpoint_every": ckpt, "J": J,
            "plain_run_ms": run_ms, "forward_ms": fwd_ms, "backward_ms": bwd_ms,
            "adjoint_over_forward": bwd_ms / run_ms,
-           "forward_element_stage_updates_per_s": e.ne * 3 * steps / (run_ms / 1e3),
-           "backward_element_stage_updates_per_s": e.ne * 3 * steps / (bwd_ms / 1e3),
-           "zone_tlm_vs_adjoint": abs(float(gz @ dzone) - dJ) / abs(dJ),
+           "forward_element_stage_updates_per_s": ne * 3 * steps / (run_ms / 1e3),
+           "backward_element_stage_updates_per_s": ne * 3 * steps / (bwd_ms / 1e3),
+           "zone_tlm_vs_adjoint": abs(adj - dJ) / abs(dJ),
            "workload": f"{nscen} submerged basins 10 km x 5 km, log-uniform 20k-150k triangles, p=2 modal, "
                        "SSP(3,3), Roe at 3 Gauss points, CFL 0.1, tide 0.5 m, 1 m hump, 32 gauges each, shared "
                        "16-zone Manning n (4x4 tiling of normalised coordinates), target from the generating "
-                       "field, gradient at n = 0.04"}
+                       "field, gradient at n = 0.04; scenarios sharded over the ranks by element count"}
     if iterations > 0:
         hist: list = []
         n_fit = cal.fit(n0, iterations, hist)
@@ -382,46 +400,6 @@ def calibration_bench(nscen: int, steps: int, ckpt: int, iterations: int, device
                     "J_final": hist[-1][0], "lbfgs_adjoint_to_forward": cal.bwd_ms / cal.fwd_ms})
     e.close()
     return out
-
-
-def io_bench(m, solver, outdir: str):
-    """Mesh ingest and snapshot output on the bench mesh: connectivity by the host builder
-    (hashed, O(E)) and by the GPU builder (sorted), identical arrays required; the three
-    .dat snapshot files of the current state written by the device formatter and by the host
-    writer (download + printf), identical bytes required."""
-    import copy
-
-    import dgrain
-
-    base = copy.deepcopy(m)
-    t0 = time.perf_counter()
-    a = dgrain.build_connectivity(copy.deepcopy(base))
-    host_s = time.perf_counter() - t0
-    dgrain.build_connectivity(copy.deepcopy(base), device=True)  # first call: module load
-    t0 = time.perf_counter()
-    b = dgrain.build_connectivity(copy.deepcopy(base), device=True)
-    dev_s = time.perf_counter() - t0
-    same_mesh = all(np.array_equal(getattr(a, k), getattr(b, k)) for k in ("ed2v", "ed2el", "bdry")) and \
-        a.min_edge == b.min_edge
-    os.makedirs(outdir, exist_ok=True)
-    paths = [os.path.join(outdir, f"dev_{v}.dat") for v in ("H", "Qx", "Qy")]
-    t0 = time.perf_counter()
-    solver.write_state_dat(*paths)
-    dev_w = time.perf_counter() - t0
-    lib = dgrain.load()
-    t0 = time.perf_counter()
-    st = solver.download_state()
-    hpaths = [os.path.join(outdir, f"host_{v}.dat") for v in ("H", "Qx", "Qy")]
-    for p, v in zip(hpaths, st[:3]):
-        lib.dgr_write_dat(p.encode(), m.num_el, v.ctypes.data_as(dgrain._lib.dptr))
-    host_w = time.perf_counter() - t0
-    same_dat = all(open(p, "rb").read() == open(q, "rb").read() for p, q in zip(paths, hpaths))
-    nbytes = sum(os.path.getsize(p) for p in paths)
-    for p in paths + hpaths:
-        os.remove(p)
-    return {"triangles": m.num_el, "connectivity_host_s": host_s, "connectivity_device_s": dev_s,
-            "connectivity_identical": bool(same_mesh), "dat_device_s": dev_w, "dat_host_s": host_w,
-            "dat_bytes": nbytes, "dat_identical": bool(same_dat)}
 
 
 def run_reference_arm(args):
@@ -607,7 +585,7 @@ def main():
     if not args.no_calibration and args.calib_scenarios > 0:
         solver.close()
         cal = calibration_bench(args.calib_scenarios, args.calib_steps, args.calib_ckpt, args.calib_iterations,
-                                device=local)
+                                device=local, dist=dist)
 
     if rank == 0:
         cs = clocks.summary()
