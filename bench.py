@@ -172,38 +172,49 @@ def cpu_baseline_reference(m, st, steps: int = 2, warmup: int = 1, max_seconds: 
                       f"{el:.1f} s, gcc -O2 build, one host core"}
 
 
-def ensemble_workload(nscen: int, seed: int = 7, lo: int = 5000, hi: int = 80000):
+def ensemble_workload(nscen: int, seed: int = 7, lo: int = 5000, hi: int = 80000, subset=None):
     """The batched-ensemble configuration: nscen coastal basins of log-uniform size in
     [lo, hi] triangles at 5 m resolution, lowered 7 m below datum so that every point is at
     least 1 m under water (the 8 bumps add at most 4 m; the reference wet/dry scheme stops
     within tens of steps once rain falls on dry land), each with its own tide amplitude
-    U(0.2, 1.5) m (period 12.42 h), rain U(0, 100) mm/h and Manning n U(0.02, 0.06)."""
+    U(0.2, 1.5) m (period 12.42 h), rain U(0, 100) mm/h and Manning n U(0.02, 0.06).
+    subset: the scenarios to build (one rank's share); returns their meshes, parameters and
+    states, and the size targets of all scenarios."""
     import dgrain
 
     rng = np.random.default_rng(seed)
     sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), nscen))
+    draws = [(float(rng.uniform(0.2, 1.5)), float(rng.uniform(0.0, 100.0) / 3.6e6), float(rng.uniform(0.02, 0.06)))
+             for _ in range(nscen)]
     meshes, params, states = [], [], []
-    for k, n in enumerate(sizes):
-        m = dgrain.rectangle_with_elements(n, seed=1000 + k, cell=5.0, datum=7.0)
-        p = dict(tide_on=1, tide_amp=float(rng.uniform(0.2, 1.5)), tide_period=PERIOD,
-                 rain=float(rng.uniform(0.0, 100.0) / 3.6e6),
-                 n_el=np.full(m.num_el, float(rng.uniform(0.02, 0.06))))
+    for k in (range(nscen) if subset is None else subset):
+        m = dgrain.rectangle_with_elements(sizes[k], seed=1000 + k, cell=5.0, datum=7.0)
+        amp, rain, n = draws[k]
+        p = dict(tide_on=1, tide_amp=amp, tide_period=PERIOD, rain=rain, n_el=np.full(m.num_el, n))
         meshes.append(m)
         params.append(p)
         states.append(dgrain.initial_state(m, np.maximum(0.0, LAND_FILM - m.z)))
-    return meshes, params, states
+    return meshes, params, states, sizes
 
 
-def ensemble_bench(nscen: int, steps: int, warmup: int, device: int = 0):
+def ensemble_bench(nscen: int, steps: int, warmup: int, device: int = 0, dist=None):
     """Batched ensemble (one context, every launch advances all scenarios, schedule picked
     by the autotuner) against the plain GPU step looped over the same scenarios (one
-    context each, its own device loop); same steps, bit-identical results required."""
+    context each, its own device loop); same steps, bit-identical results required.  With
+    several ranks (dist) each owns a share of the scenarios balanced by size (independent
+    units, no data exchange); rates are all ranks' updates over the slowest rank's time."""
     import torch
 
     import dgrain
+    from dgrain.calibration import partition
 
+    world = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
     t0 = time.perf_counter()
-    meshes, params, states = ensemble_workload(nscen)
+    sizes = ensemble_workload(nscen, subset=[])[3]
+    share = partition(sizes, world)[rank]
+    meshes, params, states, _ = ensemble_workload(nscen, subset=share)
+    nscen_local = len(share)
     tot_el = sum(m.num_el for m in meshes)
     log(f"[bench] ensemble: {nscen} meshes, {tot_el} triangles, built in {time.perf_counter() - t0:.1f} s")
     e = dgrain.Ensemble(meshes, params, wet_dry=1, cfl=CFL, device=device)
@@ -218,7 +229,7 @@ def ensemble_bench(nscen: int, steps: int, warmup: int, device: int = 0):
     launches = e.kernel_launches() - l0
     if not (n == steps).all():
         raise RuntimeError("ensemble scenario stopped early")
-    batched = [e.download_state(k) for k in range(nscen)]
+    batched = [e.download_state(k) for k in range(nscen_local)]
     e.close()
 
     solvers = []
@@ -240,16 +251,24 @@ def ensemble_bench(nscen: int, steps: int, warmup: int, device: int = 0):
                for k, s in enumerate(solvers))
     for s in solvers:
         s.close()
+    if dist is not None:
+        t = torch.tensor([float(tot_el), 0.0 if same else 1.0, float(launches)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        tot_el, same, launches = int(t[0].item()), t[1].item() == 0.0, int(t[2].item())
+        t = torch.tensor([batched_ms, looped_wall, looped_dev], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        batched_ms, looped_wall, looped_dev = (float(v) for v in t.cpu().numpy())
     units = tot_el * 2 * steps
-    return {"scenarios": nscen, "triangles": tot_el, "steps": steps, "warmup": warmup,
+    return {"scenarios": nscen, "ranks": world, "triangles": tot_el, "steps": steps, "warmup": warmup,
             "batched": units / (batched_ms / 1e3), "looped": units / (looped_wall / 1e3),
             "looped_device_only": units / (looped_dev / 1e3),
             "speedup": looped_wall / batched_ms, "unit": METRIC, "bit_identical": bool(same),
             "schedule": {"block_size": bs, "fusion": fusion,
                          "trials_ms_per_step": {f"{b}/{f}": round(v, 4) for (b, f), v in table.items()}},
             "batched_ms_per_step": batched_ms / steps, "gpu_launches": launches,
-            "workload": "256 coastal basins 5k-80k triangles (log-uniform), 5 m cells, 7 m below datum, "
-                        "tide 0.2-1.5 m, rain 0-100 mm/h, Manning 0.02-0.06, per-scenario CFL dt"}
+            "workload": f"{nscen} coastal basins 5k-80k triangles (log-uniform), 5 m cells, 7 m below datum, "
+                        "tide 0.2-1.5 m, rain 0-100 mm/h, Manning 0.02-0.06, per-scenario CFL dt; scenarios "
+                        "sharded over the ranks by size"}
 
 
 def adjoint_bench(steps: int, ckpt: int, fd_dirs: int, device: int = 0, nx: int = 447, ny: int = 224):
@@ -574,7 +593,7 @@ def main():
     ens = None
     if not args.no_ensemble and args.ensemble_scenarios > 0:
         solver.close()
-        ens = ensemble_bench(args.ensemble_scenarios, args.ensemble_steps, 3, device=local)
+        ens = ensemble_bench(args.ensemble_scenarios, args.ensemble_steps, 3, device=local, dist=dist)
 
     adj = None
     if not args.no_adjoint and args.adjoint_steps > 0:
