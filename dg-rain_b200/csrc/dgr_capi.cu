@@ -235,7 +235,7 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     if (c->p.rk_stages == 0) c->p.rk_stages = 2; /* a zero-filled struct means the reference's RK2 */
     if (c->p.order == 0) c->p.order = 1;
     if ((c->p.rk_stages != 2 && c->p.rk_stages != 3) || (c->p.order != 1 && c->p.order != 2) ||
-        (c->p.order == 2 && c->p.wet_dry)) {
+        (c->p.order == 2 && c->p.wet_dry) || (c->p.flux != 0 && c->p.flux != 1)) {
         delete c;
         return DGR_ERR_INVALID;
     }
@@ -516,7 +516,7 @@ extern "C" int dgr_set_params(dgr_ctx *c, const dgr_params *p)
 {
     if (!c || !p) return DGR_ERR_INVALID;
     if (p->g != c->p.g || p->H0 != c->p.H0 || p->VELZERO != c->p.VELZERO || p->wet_dry != c->p.wet_dry ||
-        p->device != c->p.device || (p->order == 0 ? 1 : p->order) != c->p.order)
+        p->device != c->p.device || (p->order == 0 ? 1 : p->order) != c->p.order || p->flux != c->p.flux)
         return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     c->p.rain = p->rain;

@@ -129,6 +129,49 @@ DGR_HD T roe_flux(T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy
     return m;
 }
 
+/* Local Lax-Friedrichs flux (DG-SWEM src/numerical_flux.F:887-1141, LLF_FLUX, in its
+ * nonlinear Cartesian form): the mean of the two traces' normal fluxes (the normal-flux
+ * expressions of roe_flux) minus half the largest wave speed of either trace, |u.n| + c
+ * over both, times the jump ex - in.  Returns that speed, the max |lambda| of roe_flux, in
+ * the same order.  local_g scales the pressure term only; g sets the wave speeds.  An
+ * extension: 2DCode has the Roe flux only (dgr_params.flux = 1 selects this one). */
+template <class T>
+DGR_HD T llf_flux(T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy_ex, T z_edge, double nx,
+                  double ny, double local_g, double g)
+{
+    const T h_in = zeta_in + z_edge;
+    const T h_ex = zeta_ex + z_edge;
+    const T u_in = qx_in / h_in, u_ex = qx_ex / h_ex;
+    const T v_in = qy_in / h_in, v_ex = qy_ex / h_ex;
+    const T p_in = 0.5 * local_g * (h_in * h_in - z_edge * z_edge);
+    const T p_ex = 0.5 * local_g * (h_ex * h_ex - z_edge * z_edge);
+    const T huv_in = h_in * u_in * v_in, huv_ex = h_ex * u_ex * v_ex;
+    const T fn_in[3] = {h_in * u_in * nx + h_in * v_in * ny, (h_in * u_in * u_in + p_in) * nx + huv_in * ny,
+                        huv_in * nx + (h_in * v_in * v_in + p_in) * ny};
+    const T fn_ex[3] = {h_ex * u_ex * nx + h_ex * v_ex * ny, (h_ex * u_ex * u_ex + p_ex) * nx + huv_ex * ny,
+                        huv_ex * nx + (h_ex * v_ex * v_ex + p_ex) * ny};
+    const T un_in = u_in * nx + v_in * ny, un_ex = u_ex * nx + v_ex * ny;
+    const T c_in = sqrt(g * h_in), c_ex = sqrt(g * h_ex);
+    T m = rmax(fabs(un_in - c_in), fabs(un_ex - c_ex));
+    m = rmax(m, fabs(un_in));
+    m = rmax(m, fabs(un_ex));
+    m = rmax(m, fabs(un_in + c_in));
+    m = rmax(m, fabs(un_ex + c_ex));
+    const T jump[3] = {zeta_ex - zeta_in, qx_ex - qx_in, qy_ex - qy_in};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) fh[k] = 0.5 * (fn_in[k] + fn_ex[k]) - 0.5 * m * jump[k];
+    return m;
+}
+
+/* numerical flux of kind `type` (0: Roe, 2DCode; 1: local Lax-Friedrichs, DG-SWEM) */
+template <class T>
+DGR_HD T numerical_flux(int type, T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy_ex, T z_edge,
+                        double nx, double ny, double local_g, double g)
+{
+    if (type == 1) return llf_flux<T>(fh, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g);
+    return roe_flux<T>(fh, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g);
+}
+
 /*
  * x^p for p = 4./3 (the double nearest 4/3, used by the Manning term
  * pow(H[e], 4./3) of 2DCode/2DInnerProducts.c:318), correctly rounded.

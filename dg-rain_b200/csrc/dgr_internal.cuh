@@ -117,6 +117,7 @@ static inline dgr::MeshDev mesh_dev(const dgr_ctx *c)
     m.zn = c->zn;
     m.el_sid = c->el_sid;
     m.ed_sid = c->ed_sid;
+    m.flux = c->p.flux;
     return m;
 }
 

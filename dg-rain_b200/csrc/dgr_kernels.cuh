@@ -77,6 +77,7 @@ struct MeshDev {
     const double *zn;     /* node depth [nn] */
     const int *el_sid;    /* scenario of each element, NULL for a single mesh */
     const int *ed_sid;    /* scenario of each edge, NULL for a single mesh */
+    int flux;             /* numerical flux: 0 Roe (2DCode), 1 local Lax-Friedrichs (DG-SWEM) */
 };
 
 struct PhysParams {
@@ -114,7 +115,7 @@ DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, 
         const int wdi = WD ? ldm<COH>(&wd[el_in]) : 1, wde = WD ? ldm<COH>(&wd[el_ex]) : 1;
         double fin[3], fex[3];
         int code;
-        lam = flux_core<double, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code);
+        lam = flux_core<double, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code, m.flux);
         if (code) atomicMin(&ck->err, err_key(ldm<COH>(&ck->step), phase, code, i - ck->ed_off));
         const int lf = m.ldF;
         flux[i] = fin[0];

@@ -83,7 +83,8 @@ DGR_HD int p2_match_point(int info, int g) { return (info & 128) ? g : P2_NGP - 
  * (tangents / perturbed values) for the two-lane arithmetics, unused for T = double. */
 template <class T, class Load>
 DGR_HD T p2_edge_core(const P2Ref &ref, const Load &st, int el_in, int el_ex, int info, double nx, double ny,
-                      const T &za, const T &zb, double bz, double bq, double g, T fh[P2_NGP][3], int &code)
+                      const T &za, const T &zb, double bz, double bq, double g, T fh[P2_NGP][3], int &code,
+                      int ftype = 0)
 {
     const int k_in = info & 3, k_ex = (info >> 2) & 3, bd = (info >> 4) & 7;
     const bool boundary = bd || el_in == el_ex;
@@ -114,7 +115,7 @@ DGR_HD T p2_edge_core(const P2Ref &ref, const Load &st, int el_in, int el_ex, in
                 ue[v] = a;
             }
         }
-        const T l = roe_flux<T>(fh[gp], ui[0], ue[0], ui[1], ue[1], ui[2], ue[2], z_g, nx, ny, g, g);
+        const T l = numerical_flux<T>(ftype, fh[gp], ui[0], ue[0], ui[1], ue[1], ui[2], ue[2], z_g, nx, ny, g, g);
         if (isnan(fh[gp][0]) || isnan(fh[gp][1]) || isnan(fh[gp][2])) code = 1;
         lam = rmax(lam, l);
     }
@@ -251,7 +252,7 @@ __global__ void __launch_bounds__(BS, DGR_P2_MINB_EDGE) k_p2_edge(P2Ref ref, Mes
             double fh[P2_NGP][3];
             int code;
             lam = p2_edge_core<double>(ref, st, el_in, el_ex, info, nx, ny, za, zb, bd ? bzeta[i] : 0.0,
-                                       bd ? bqn[i] : 0.0, g, fh, code);
+                                       bd ? bqn[i] : 0.0, g, fh, code, m.flux);
             if (code) atomicMin(&ck->err, err_key(ck->step, phase, code, i - ck->ed_off));
 #pragma unroll
             for (int gp = 0; gp < P2_NGP; ++gp)

@@ -83,7 +83,8 @@ __global__ void __launch_bounds__(128) k_p2_tlm_edge(P2Ref ref, MeshDev m, const
     const auto st = [S, Sx, ld, tag](int plane, int el) { return lane(tag, S[plane * ld + el], Sx[plane * ld + el]); };
     T fh[P2_NGP][3];
     int code;
-    p2_edge_core<T>(ref, st, el_in, el_ex, info, nx, ny, za, zb, bd ? bzeta[i] : 0.0, bd ? bqn[i] : 0.0, g, fh, code);
+    p2_edge_core<T>(ref, st, el_in, el_ex, info, nx, ny, za, zb, bd ? bzeta[i] : 0.0, bd ? bqn[i] : 0.0, g, fh, code,
+                    m.flux);
     const int lf = m.ldF;
 #pragma unroll
     for (int gp = 0; gp < P2_NGP; ++gp)
@@ -381,7 +382,7 @@ static __global__ void __launch_bounds__(128, DGR_P2_MINB_ADJ_EDGE) k_p2_adj_edg
         for (int v = 0; v < 3; ++v)
             fhb[v] = fbar[(3 * gp + v) * lf + i] + (boundary ? 0.0 : fbar[(9 + 3 * gp + v) * lf + i]);
         RoeBar b = {0, 0, 0, 0, 0, 0, 0};
-        roe_flux_rev(fhb, ui[0], ue[0], ui[1], ue[1], ui[2], ue[2], z_g, nx, ny, g, g, b);
+        numerical_flux_rev(m.flux, fhb, ui[0], ue[0], ui[1], ue[1], ui[2], ue[2], z_g, nx, ny, g, g, b);
         if (boundary) ghost_state_rev(bd, nx, ny, bz, bq, b.zex, b.qxex, b.qyex, b.zin, b.qxin, b.qyin);
         fbar[(3 * gp) * lf + i] = b.zin;
         fbar[(3 * gp + 1) * lf + i] = b.qxin;

@@ -186,6 +186,74 @@ DGR_HD void roe_flux_rev(const double fhb[3], double zeta_in, double zeta_ex, do
     b.zed += zb + hib + heb;
 }
 
+/* Reverse of llf_flux: fhb = adjoint of Fhat.n.  The selected wave speed is the one the
+ * forward's rmax chain keeps (ties to the later operand), |x| differentiated with the sign
+ * of x (+ at 0), sqrt with derivative 0 at 0. */
+DGR_HD void llf_flux_rev(const double fhb[3], double zeta_in, double zeta_ex, double qx_in, double qx_ex, double qy_in,
+                         double qy_ex, double z_edge, double nx, double ny, double local_g, double g, RoeBar &b)
+{
+    const double h_in = zeta_in + z_edge, h_ex = zeta_ex + z_edge;
+    const double u_in = qx_in / h_in, u_ex = qx_ex / h_ex;
+    const double v_in = qy_in / h_in, v_ex = qy_ex / h_ex;
+    const double un_in = u_in * nx + v_in * ny, un_ex = u_ex * nx + v_ex * ny;
+    const double c_in = sqrt(g * h_in), c_ex = sqrt(g * h_ex);
+    const double x[6] = {un_in - c_in, un_ex - c_ex, un_in, un_ex, un_in + c_in, un_ex + c_ex};
+    int s = 0;
+    double m = fabs(x[0]);
+#pragma unroll
+    for (int i = 1; i < 6; ++i) {
+        const double a = fabs(x[i]);
+        if (!(m > a)) {
+            m = a;
+            s = i;
+        }
+    }
+    const double jump[3] = {zeta_ex - zeta_in, qx_ex - qx_in, qy_ex - qy_in};
+    /* fh = 0.5 (fn_in + fn_ex) - 0.5 m jump */
+    const double fnb[3] = {0.5 * fhb[0], 0.5 * fhb[1], 0.5 * fhb[2]};
+    const double mb = -0.5 * (fhb[0] * jump[0] + fhb[1] * jump[1] + fhb[2] * jump[2]);
+    const double jb[3] = {-0.5 * m * fhb[0], -0.5 * m * fhb[1], -0.5 * m * fhb[2]};
+    const double xb = x[s] < 0 ? -mb : mb;
+    double un_in_b = 0, un_ex_b = 0, c_in_b = 0, c_ex_b = 0;
+    if (s == 0 || s == 2 || s == 4) un_in_b = xb;
+    else un_ex_b = xb;
+    if (s == 0) c_in_b = -xb;
+    else if (s == 4) c_in_b = xb;
+    else if (s == 1) c_ex_b = -xb;
+    else if (s == 5) c_ex_b = xb;
+    double uib = nx * un_in_b, vib = ny * un_in_b, ueb = nx * un_ex_b, veb = ny * un_ex_b;
+    double hib = c_in == 0.0 ? 0.0 : c_in_b * g / (2.0 * c_in);
+    double heb = c_ex == 0.0 ? 0.0 : c_ex_b * g / (2.0 * c_ex);
+    double zb = 0.0;
+    normal_flux_rev(fnb, h_in, u_in, v_in, z_edge, nx, ny, local_g, hib, uib, vib, zb);
+    normal_flux_rev(fnb, h_ex, u_ex, v_ex, z_edge, nx, ny, local_g, heb, ueb, veb, zb);
+    const double ihi = 1.0 / h_in, ihe = 1.0 / h_ex;
+    b.qxin += uib * ihi;
+    b.qyin += vib * ihi;
+    hib -= (uib * u_in + vib * v_in) * ihi;
+    b.qxex += ueb * ihe;
+    b.qyex += veb * ihe;
+    heb -= (ueb * u_ex + veb * v_ex) * ihe;
+    b.zin += hib - jb[0];
+    b.zex += heb + jb[0];
+    b.qxin -= jb[1];
+    b.qxex += jb[1];
+    b.qyin -= jb[2];
+    b.qyex += jb[2];
+    b.zed += zb + hib + heb;
+}
+
+/* reverse of numerical_flux */
+DGR_HD void numerical_flux_rev(int type, const double fhb[3], double zeta_in, double zeta_ex, double qx_in,
+                               double qx_ex, double qy_in, double qy_ex, double z_edge, double nx, double ny,
+                               double local_g, double g, RoeBar &b)
+{
+    if (type == 1)
+        llf_flux_rev(fhb, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g, b);
+    else
+        roe_flux_rev(fhb, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g, b);
+}
+
 /* Reverse of the reflection (qx, qy) -> ghost discharge with the normal part negated and
  * the tangential part kept (2DCode/compute2DL.c:175-191). */
 DGR_HD void reflect_rev(double nx, double ny, double oxb, double oyb, double &qxb, double &qyb)
@@ -226,7 +294,8 @@ DGR_HD void ghost_state_rev(int bd, double nx, double ny, double bz, double bq, 
 /* Reverse of flux_core: finb/fexb = adjoints of the stored Fhat.n of the two sides. */
 template <bool WD>
 DGR_HD void flux_core_rev(double zi, double qxi, double qyi, double ze, double qxe, double qye, double z_edge, double nx,
-                          double ny, int wdi, int wde, double g, const double finb[3], const double fexb[3], EdgeBar &b)
+                          double ny, int wdi, int wde, double g, const double finb[3], const double fexb[3], EdgeBar &b,
+                          int ftype = 0)
 {
     const double tx = -ny, ty = nx;
     if (WD && wdi == 0 && wde == 0) {
@@ -237,7 +306,7 @@ DGR_HD void flux_core_rev(double zi, double qxi, double qyi, double ze, double q
         const double qxe_ref = (ty * qn_ex - ny * qt_ex) * d;
         const double qye_ref = (-tx * qn_ex + nx * qt_ex) * d;
         RoeBar r = {0, 0, 0, 0, 0, 0, 0};
-        roe_flux_rev(finb, zi, zi, qxi, qxe_ref, qyi, qye_ref, z_edge, nx, ny, 0.0, g, r);
+        numerical_flux_rev(ftype, finb, zi, zi, qxi, qxe_ref, qyi, qye_ref, z_edge, nx, ny, 0.0, g, r);
         b.zi += r.zin + r.zex;
         b.qxi += r.qxin;
         b.qyi += r.qyin;
@@ -250,7 +319,7 @@ DGR_HD void flux_core_rev(double zi, double qxi, double qyi, double ze, double q
         const double qxi_ref = (ty * qn_in - ny * qt_in) * d;
         const double qyi_ref = (-tx * qn_in + nx * qt_ex) * d;
         RoeBar s = {0, 0, 0, 0, 0, 0, 0};
-        roe_flux_rev(fexb, ze, ze, qxi_ref, qxe, qyi_ref, qye, z_edge, nx, ny, 0.0, g, s);
+        numerical_flux_rev(ftype, fexb, ze, ze, qxi_ref, qxe, qyi_ref, qye, z_edge, nx, ny, 0.0, g, s);
         b.ze += s.zin + s.zex;
         b.qxe += s.qxex;
         b.qye += s.qyex;
@@ -267,10 +336,10 @@ DGR_HD void flux_core_rev(double zi, double qxi, double qyi, double ze, double q
             if (in_shared) fhb[k] += finb[k];
             if (ex_shared) fhb[k] += fexb[k];
         }
-        roe_flux_rev(fhb, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, g, g, r);
+        numerical_flux_rev(ftype, fhb, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, g, g, r);
     }
-    if (!in_shared) roe_flux_rev(finb, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g, r);
-    if (!ex_shared) roe_flux_rev(fexb, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g, r);
+    if (!in_shared) numerical_flux_rev(ftype, finb, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g, r);
+    if (!ex_shared) numerical_flux_rev(ftype, fexb, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g, r);
     b.zi += r.zin;
     b.ze += r.zex;
     b.qxi += r.qxin;

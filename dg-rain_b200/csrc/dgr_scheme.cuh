@@ -185,7 +185,7 @@ DGR_HD void ghost_state(int bd, double nx, double ny, const T &zi, const T &qxi,
 template <class T, bool WD>
 DGR_HD T flux_core(const T &zi, const T &qxi, const T &qyi, const T &ze, const T &qxe, const T &qye,
                    const T &z_edge, double nx, double ny, int wdi, int wde, double g, T fin[3], T fex[3],
-                   int &code)
+                   int &code, int ftype = 0)
 {
     const double tx = -ny, ty = nx;
     T lam = 0.0;
@@ -197,25 +197,25 @@ DGR_HD T flux_core(const T &zi, const T &qxi, const T &qyi, const T &ze, const T
         const double d = 1. / (nx * ty - ny * tx);
         const T qxe_ref = (ty * qn_ex - ny * qt_ex) * d;
         const T qye_ref = (-tx * qn_ex + nx * qt_ex) * d;
-        const T lam_in = roe_flux<T>(fin, zi, zi, qxi, qxe_ref, qyi, qye_ref, z_edge, nx, ny, 0.0, g);
+        const T lam_in = numerical_flux<T>(ftype, fin, zi, zi, qxi, qxe_ref, qyi, qye_ref, z_edge, nx, ny, 0.0, g);
         qn_ex = qxe * nx + qye * ny;
         qt_ex = qxe * tx + qye * ty;
         qn_in = -qn_ex;
         qt_in = qt_ex;
         const T qxi_ref = (ty * qn_in - ny * qt_in) * d;
         const T qyi_ref = (-tx * qn_in + nx * qt_ex) * d;
-        const T lam_ex = roe_flux<T>(fex, ze, ze, qxi_ref, qxe, qyi_ref, qye, z_edge, nx, ny, 0.0, g);
+        const T lam_ex = numerical_flux<T>(ftype, fex, ze, ze, qxi_ref, qxe, qyi_ref, qye, z_edge, nx, ny, 0.0, g);
         lam = rmax(lam_in, lam_ex);
     } else {
         T fh[3];
-        lam = roe_flux<T>(fh, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, g, g);
+        lam = numerical_flux<T>(ftype, fh, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, g, g);
         if (isnan(fh[0]) || isnan(fh[1]) || isnan(fh[2])) code = 1;
         if (!WD || wdi == 1) {
             fin[0] = fh[0];
             fin[1] = fh[1];
             fin[2] = fh[2];
         } else {
-            const T l2 = roe_flux<T>(fin, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g);
+            const T l2 = numerical_flux<T>(ftype, fin, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g);
             if (!code && (isnan(fin[0]) || isnan(fin[1]) || isnan(fin[2]))) code = 2;
             lam = rmax(lam, l2);
         }
@@ -224,7 +224,7 @@ DGR_HD T flux_core(const T &zi, const T &qxi, const T &qyi, const T &ze, const T
             fex[1] = fh[1];
             fex[2] = fh[2];
         } else {
-            const T l2 = roe_flux<T>(fex, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g);
+            const T l2 = numerical_flux<T>(ftype, fex, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g);
             if (!code && (isnan(fex[0]) || isnan(fex[1]) || isnan(fex[2]))) code = 3;
             lam = rmax(lam, l2);
         }

@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(256) k_tlm_edge(MeshDev m, const double *__res
     const int wdi = WD ? wd[el_in] : 1, wde = WD ? wd[el_ex] : 1;
     T fin[3], fex[3];
     int code;
-    flux_core<T, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code);
+    flux_core<T, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code, m.flux);
     const int lf = m.ldF;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -589,7 +589,7 @@ __global__ void __launch_bounds__(256, DGR_ADJ_MINB_EDGE) k_adj_edge(MeshDev m, 
         fexb[k] = boundary ? 0.0 : fbar[(3 + k) * lf + i]; /* no element gathers a boundary edge's ex side */
     }
     EdgeBar b = {0, 0, 0, 0, 0, 0, 0};
-    flux_core_rev<WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, finb, fexb, b);
+    flux_core_rev<WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, finb, fexb, b, m.flux);
     if (boundary) {
         ghost_state_rev(bd, nx, ny, bz, bq, b.ze, b.qxe, b.qye, b.zi, b.qxi, b.qyi);
     } else {

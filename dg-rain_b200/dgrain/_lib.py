@@ -46,6 +46,7 @@ class DgrParams(C.Structure):
         ("record_decisions", C.c_int),
         ("rk_stages", C.c_int),
         ("order", C.c_int),
+        ("flux", C.c_int),
     ]
 
 

@@ -94,6 +94,9 @@ typedef struct dgr_params {
                         flows that stay wet: wet_dry must be 0, there is no limiter, and the
                         state is 6 modal coefficients per element and variable,
                         zeta[6*el + m] etc. (see dgr_p2_reference). */
+    int flux;        /* numerical flux at edges: 0 the Roe flux of 2DCode/numericalFlux2D.c:6-108
+                        (default); 1 the local Lax-Friedrichs flux of DG-SWEM
+                        src/numerical_flux.F:887-1141 (extension).  Fixed at creation. */
 } dgr_params;
 
 /* Mesh in the reference's arrays (2DCode/MeshAttributes.h:5-20), 0-based. */

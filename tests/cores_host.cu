@@ -25,7 +25,11 @@ struct DualZ {
 
 }  // namespace
 
+static int g_ftype = 0; /* numerical flux of the edge cases: 0 Roe, 1 local Lax-Friedrichs */
+
 extern "C" {
+
+void dgr_t_set_flux(int type) { g_ftype = type; }
 
 /* x = zin, zex, qxin, qxex, qyin, qyex, zedge */
 int dgr_t_roe(const double *x, double nx, double ny, double lg, double g, const double *xd, const double *yb,
@@ -34,13 +38,13 @@ int dgr_t_roe(const double *x, double nx, double ny, double lg, double g, const 
     Dual in[7];
     for (int i = 0; i < 7; ++i) in[i] = Dual(x[i], xd[i]);
     Dual fh[3];
-    roe_flux<Dual>(fh, in[0], in[1], in[2], in[3], in[4], in[5], in[6], nx, ny, lg, g);
+    numerical_flux<Dual>(g_ftype, fh, in[0], in[1], in[2], in[3], in[4], in[5], in[6], nx, ny, lg, g);
     for (int k = 0; k < 3; ++k) {
         y[k] = fh[k].v;
         yd[k] = fh[k].d;
     }
     RoeBar b = {0, 0, 0, 0, 0, 0, 0};
-    roe_flux_rev(yb, x[0], x[1], x[2], x[3], x[4], x[5], x[6], nx, ny, lg, g, b);
+    numerical_flux_rev(g_ftype, yb, x[0], x[1], x[2], x[3], x[4], x[5], x[6], nx, ny, lg, g, b);
     const double o[7] = {b.zin, b.zex, b.qxin, b.qxex, b.qyin, b.qyex, b.zed};
     for (int i = 0; i < 7; ++i) xb[i] = o[i];
     return 0;
@@ -66,9 +70,10 @@ int dgr_t_edge(int wd_on, int kind, int bd, int wdi, int wde, double bz, double 
     Dual fin[3], fex[3];
     int code;
     if (wd_on)
-        flux_core<Dual, true>(in[0], in[1], in[2], ze, qxe, qye, in[6], nx, ny, wdi, wde, g, fin, fex, code);
+        flux_core<Dual, true>(in[0], in[1], in[2], ze, qxe, qye, in[6], nx, ny, wdi, wde, g, fin, fex, code, g_ftype);
     else
-        flux_core<Dual, false>(in[0], in[1], in[2], ze, qxe, qye, in[6], nx, ny, wdi, wde, g, fin, fex, code);
+        flux_core<Dual, false>(in[0], in[1], in[2], ze, qxe, qye, in[6], nx, ny, wdi, wde, g, fin, fex, code,
+                               g_ftype);
     for (int k = 0; k < 3; ++k) {
         y[k] = fin[k].v;
         yd[k] = fin[k].d;
@@ -80,9 +85,9 @@ int dgr_t_edge(int wd_on, int kind, int bd, int wdi, int wde, double bz, double 
     if (kind) ghost_state<double>(kind == 2 ? bd : 0, nx, ny, x[0], x[1], x[2], bz, bq, x[0], zev, qxev, qyev);
     EdgeBar b = {0, 0, 0, 0, 0, 0, 0};
     if (wd_on)
-        flux_core_rev<true>(x[0], x[1], x[2], zev, qxev, qyev, x[6], nx, ny, wdi, wde, g, yb, yb + 3, b);
+        flux_core_rev<true>(x[0], x[1], x[2], zev, qxev, qyev, x[6], nx, ny, wdi, wde, g, yb, yb + 3, b, g_ftype);
     else
-        flux_core_rev<false>(x[0], x[1], x[2], zev, qxev, qyev, x[6], nx, ny, wdi, wde, g, yb, yb + 3, b);
+        flux_core_rev<false>(x[0], x[1], x[2], zev, qxev, qyev, x[6], nx, ny, wdi, wde, g, yb, yb + 3, b, g_ftype);
     for (int i = 0; i < 7; ++i) xb[i] = 0;
     if (kind) {
         ghost_state_rev(kind == 2 ? bd : 0, nx, ny, bz, bq, b.ze, b.qxe, b.qye, b.zi, b.qxi, b.qyi);

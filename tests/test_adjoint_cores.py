@@ -44,6 +44,7 @@ def cores():
     _build()
     lib = C.CDLL(LIB)
     d = C.c_double
+    lib.dgr_t_set_flux.argtypes = [C.c_int]
     lib.dgr_t_roe.argtypes = [dp, d, d, d, d, dp, dp, dp, dp, dp]
     lib.dgr_t_edge.argtypes = [C.c_int] * 5 + [d, d, dp, d, d, d, dp, dp, dp, dp, dp]
     lib.dgr_t_element.argtypes = ([C.c_int, dp, dp, dp, d, d, d, d, d] + [dp] * 7 + [d, dp, dp, dp, dp, dp, dp, dp,
@@ -79,8 +80,17 @@ def _roe(cores, x, nx, ny, lg, xd=None, yb=None):
     return y, yd, xb
 
 
+@pytest.fixture(params=[0, 1], ids=["roe", "llf"])
+def flux(request, cores):
+    """numerical flux of the edge cases: the Roe flux of 2DCode, the local Lax-Friedrichs
+    flux of DG-SWEM"""
+    cores.dgr_t_set_flux(request.param)
+    yield request.param
+    cores.dgr_t_set_flux(0)
+
+
 @pytest.mark.parametrize("lg", [G, 0.0])
-def test_roe_dot_product(cores, lg):
+def test_roe_dot_product(cores, flux, lg):
     rng = np.random.default_rng(1)
     for _ in range(400):
         x, nx, ny = _roe_inputs(rng)
@@ -104,7 +114,7 @@ def _fd_check(f, x, xd, yd, rel=1e-6, h=1e-6):
     return np.max(np.abs(cen - yd)) <= rel * scale + noise
 
 
-def test_roe_tangent_matches_finite_differences(cores):
+def test_roe_tangent_matches_finite_differences(cores, flux):
     rng = np.random.default_rng(2)
     checked = 0
     for _ in range(200):
@@ -154,7 +164,7 @@ def _edge_inputs(rng):
 
 
 @pytest.mark.parametrize("case", EDGE_CASES)
-def test_edge_dot_product_and_fd(cores, case):
+def test_edge_dot_product_and_fd(cores, flux, case):
     rng = np.random.default_rng(3)
     checked = 0
     for _ in range(150):
