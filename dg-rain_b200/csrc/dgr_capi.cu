@@ -235,7 +235,7 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     if (c->p.rk_stages == 0) c->p.rk_stages = 2; /* a zero-filled struct means the reference's RK2 */
     if (c->p.order == 0) c->p.order = 1;
     if ((c->p.rk_stages != 2 && c->p.rk_stages != 3) || (c->p.order != 1 && c->p.order != 2) ||
-        (c->p.order == 2 && c->p.wet_dry) || (c->p.flux != 0 && c->p.flux != 1)) {
+        (c->p.order == 2 && c->p.wet_dry) || (c->p.flux < 0 || c->p.flux > 2)) {
         delete c;
         return DGR_ERR_INVALID;
     }

@@ -163,12 +163,70 @@ DGR_HD T llf_flux(T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy
     return m;
 }
 
-/* numerical flux of kind `type` (0: Roe, 2DCode; 1: local Lax-Friedrichs, DG-SWEM) */
+/* HLLC flux (DG-SWEM src/numerical_flux.F:1154-1400, HLLC_FLUX, nonlinear Cartesian
+ * form): wave speeds S_in = un_in - c_in l_in, S_ex = un_ex + c_ex l_ex with the
+ * shock/rarefaction factors l = sqrt((h* h* + h* h) / (2 h h)) when h* > h (else 1),
+ * h* = (0.5 (c_in + c_ex) + 0.25 (un_in - un_ex))^2 / g, the contact speed S*, and the
+ * four branches: the in trace's normal flux for S_in >= 0, the in star state for
+ * S_in <= 0 <= S*, the ex star state for S* <= 0 <= S_ex, the ex trace's flux otherwise;
+ * star-state corrections S (Q* - Q) in normal/tangential components rotated back.  The
+ * normal fluxes are roe_flux's expressions (local_g in the pressure); returns max |lambda|
+ * of the two traces as roe_flux does (for the CFL dt).  An extension (flux = 2). */
+template <class T>
+DGR_HD T hllc_flux(T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy_ex, T z_edge, double nx,
+                   double ny, double local_g, double g)
+{
+    const T h_in = zeta_in + z_edge;
+    const T h_ex = zeta_ex + z_edge;
+    const T u_in = qx_in / h_in, u_ex = qx_ex / h_ex;
+    const T v_in = qy_in / h_in, v_ex = qy_ex / h_ex;
+    const T un_in = u_in * nx + v_in * ny, un_ex = u_ex * nx + v_ex * ny;
+    const T ut_in = -u_in * ny + v_in * nx, ut_ex = -u_ex * ny + v_ex * nx;
+    const T c_in = sqrt(g * h_in), c_ex = sqrt(g * h_ex);
+    const T P = 0.5 * (c_in + c_ex) + 0.25 * (un_in - un_ex);
+    const T hs = 1.0 / g * P * P;
+    T l_in = 1.0, l_ex = 1.0;
+    if (hs > h_ex) l_ex = sqrt((hs * hs + hs * h_ex) / (2.0 * h_ex * h_ex));
+    if (hs > h_in) l_in = sqrt((hs * hs + hs * h_in) / (2.0 * h_in * h_in));
+    const T s_in = un_in - c_in * l_in;
+    const T s_ex = un_ex + c_ex * l_ex;
+    const T A = un_ex - s_ex, B = un_in - s_in;
+    const T s_st = (s_in * h_ex * A - s_ex * h_in * B) / (h_ex * A - h_in * B);
+    /* DG-SWEM's branch order: S_in >= 0; S* >= 0; S_ex >= 0; otherwise */
+    const int branch = s_in >= 0.0 ? 0 : (s_st >= 0.0 ? 1 : (s_ex >= 0.0 ? 2 : 3));
+    const bool use_in = branch <= 1;
+    const T h = use_in ? h_in : h_ex, u = use_in ? u_in : u_ex, v = use_in ? v_in : v_ex;
+    const T p = 0.5 * local_g * (h * h - z_edge * z_edge);
+    const T huv = h * u * v;
+    fh[0] = h * u * nx + h * v * ny;
+    fh[1] = (h * u * u + p) * nx + huv * ny;
+    fh[2] = huv * nx + (h * v * v + p) * ny;
+    if (branch == 1 || branch == 2) { /* a star state */
+        const T S = use_in ? s_in : s_ex, un = use_in ? un_in : un_ex, ut = use_in ? ut_in : ut_ex;
+        const T qx = use_in ? qx_in : qx_ex, qy = use_in ? qy_in : qy_ex;
+        const T q1 = h * ((S - un) / (S - s_st));
+        const T d1 = q1 - h;
+        const T d2 = q1 * s_st - (qx * nx + qy * ny);
+        const T d3 = q1 * ut - (-qx * ny + qy * nx);
+        fh[0] = fh[0] + S * d1;
+        fh[1] = fh[1] + S * (d2 * nx - d3 * ny);
+        fh[2] = fh[2] + S * (d2 * ny + d3 * nx);
+    }
+    T m = rmax(fabs(un_in - c_in), fabs(un_ex - c_ex));
+    m = rmax(m, fabs(un_in));
+    m = rmax(m, fabs(un_ex));
+    m = rmax(m, fabs(un_in + c_in));
+    m = rmax(m, fabs(un_ex + c_ex));
+    return m;
+}
+
+/* numerical flux of kind `type` (0: Roe, 2DCode; 1: local Lax-Friedrichs, 2: HLLC, DG-SWEM) */
 template <class T>
 DGR_HD T numerical_flux(int type, T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy_ex, T z_edge,
                         double nx, double ny, double local_g, double g)
 {
     if (type == 1) return llf_flux<T>(fh, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g);
+    if (type == 2) return hllc_flux<T>(fh, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g);
     return roe_flux<T>(fh, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g);
 }
 

@@ -77,7 +77,7 @@ struct MeshDev {
     const double *zn;     /* node depth [nn] */
     const int *el_sid;    /* scenario of each element, NULL for a single mesh */
     const int *ed_sid;    /* scenario of each edge, NULL for a single mesh */
-    int flux;             /* numerical flux: 0 Roe (2DCode), 1 local Lax-Friedrichs (DG-SWEM) */
+    int flux;             /* numerical flux: 0 Roe (2DCode), 1 local Lax-Friedrichs, 2 HLLC (DG-SWEM) */
 };
 
 struct PhysParams {

@@ -243,6 +243,146 @@ DGR_HD void llf_flux_rev(const double fhb[3], double zeta_in, double zeta_ex, do
     b.zed += zb + hib + heb;
 }
 
+/* Reverse of hllc_flux with its branch and shock factors frozen at the forward's (the
+ * branch by the forward's comparisons; sqrt with derivative 0 at 0). */
+DGR_HD void hllc_flux_rev(const double fhb[3], double zeta_in, double zeta_ex, double qx_in, double qx_ex,
+                          double qy_in, double qy_ex, double z_edge, double nx, double ny, double local_g, double g,
+                          RoeBar &b)
+{
+    /* forward values, hllc_flux's expressions */
+    const double h_in = zeta_in + z_edge, h_ex = zeta_ex + z_edge;
+    const double u_in = qx_in / h_in, u_ex = qx_ex / h_ex;
+    const double v_in = qy_in / h_in, v_ex = qy_ex / h_ex;
+    const double un_in = u_in * nx + v_in * ny, un_ex = u_ex * nx + v_ex * ny;
+    const double ut_in = -u_in * ny + v_in * nx, ut_ex = -u_ex * ny + v_ex * nx;
+    const double c_in = sqrt(g * h_in), c_ex = sqrt(g * h_ex);
+    const double P = 0.5 * (c_in + c_ex) + 0.25 * (un_in - un_ex);
+    const double hs = 1.0 / g * P * P;
+    const bool sh_ex = hs > h_ex, sh_in = hs > h_in;
+    const double l_ex = sh_ex ? sqrt((hs * hs + hs * h_ex) / (2.0 * h_ex * h_ex)) : 1.0;
+    const double l_in = sh_in ? sqrt((hs * hs + hs * h_in) / (2.0 * h_in * h_in)) : 1.0;
+    const double s_in = un_in - c_in * l_in;
+    const double s_ex = un_ex + c_ex * l_ex;
+    const double A = un_ex - s_ex, B = un_in - s_in;
+    const double N = s_in * h_ex * A - s_ex * h_in * B, D = h_ex * A - h_in * B;
+    const double s_st = N / D;
+    const int branch = s_in >= 0.0 ? 0 : (s_st >= 0.0 ? 1 : (s_ex >= 0.0 ? 2 : 3));
+    const bool use_in = branch <= 1;
+    const double h = use_in ? h_in : h_ex, u = use_in ? u_in : u_ex, v = use_in ? v_in : v_ex;
+
+    /* adjoints of the chosen trace (h, u, v, un, ut, qx, qy) and of the speeds */
+    double hb = 0, ub = 0, vb = 0, unb = 0, utb = 0, qxb = 0, qyb = 0;
+    double s_inb = 0, s_exb = 0, s_stb = 0, zb = 0;
+    normal_flux_rev(fhb, h, u, v, z_edge, nx, ny, local_g, hb, ub, vb, zb);
+    if (branch == 1 || branch == 2) {
+        const double S = use_in ? s_in : s_ex, un = use_in ? un_in : un_ex, ut = use_in ? ut_in : ut_ex;
+        const double qx = use_in ? qx_in : qx_ex, qy = use_in ? qy_in : qy_ex;
+        const double R = (S - un) / (S - s_st);
+        const double q1 = h * R;
+        const double d1 = q1 - h;
+        const double d2 = q1 * s_st - (qx * nx + qy * ny);
+        const double d3 = q1 * ut - (-qx * ny + qy * nx);
+        const double Sb = fhb[0] * d1 + fhb[1] * (d2 * nx - d3 * ny) + fhb[2] * (d2 * ny + d3 * nx);
+        const double d1b = S * fhb[0];
+        const double d2b = S * (fhb[1] * nx + fhb[2] * ny);
+        const double d3b = S * (-fhb[1] * ny + fhb[2] * nx);
+        const double q1b = d1b + d2b * s_st + d3b * ut;
+        s_stb += d2b * q1;
+        utb += d3b * q1;
+        hb -= d1b;
+        qxb -= d2b * nx - d3b * ny;
+        qyb -= d2b * ny + d3b * nx;
+        hb += q1b * R;
+        const double Rb = q1b * h;
+        const double numb = Rb / (S - s_st);
+        const double denb = -Rb * R / (S - s_st);
+        const double Sbt = Sb + numb + denb;
+        unb -= numb;
+        s_stb -= denb;
+        if (use_in)
+            s_inb += Sbt;
+        else
+            s_exb += Sbt;
+    }
+    /* per-side adjoints */
+    double h_inb = 0, h_exb = 0, un_inb = 0, un_exb = 0, ut_inb = 0, ut_exb = 0, c_inb = 0, c_exb = 0;
+    double u_inb = 0, v_inb = 0, u_exb = 0, v_exb = 0;
+    if (use_in) {
+        h_inb += hb;
+        u_inb += ub;
+        v_inb += vb;
+        un_inb += unb;
+        ut_inb += utb;
+        b.qxin += qxb;
+        b.qyin += qyb;
+    } else {
+        h_exb += hb;
+        u_exb += ub;
+        v_exb += vb;
+        un_exb += unb;
+        ut_exb += utb;
+        b.qxex += qxb;
+        b.qyex += qyb;
+    }
+    /* s* = N / D */
+    if (s_stb != 0.0) {
+        const double Nb = s_stb / D, Db = -s_stb * s_st / D;
+        double Ab = Nb * s_in * h_ex + Db * h_ex;
+        double Bb = -Nb * s_ex * h_in - Db * h_in;
+        s_inb += Nb * h_ex * A;
+        h_exb += Nb * s_in * A + Db * A;
+        s_exb -= Nb * h_in * B;
+        h_inb -= Nb * s_ex * B + Db * B;
+        un_exb += Ab;
+        s_exb -= Ab;
+        un_inb += Bb;
+        s_inb -= Bb;
+    }
+    /* s_in = un_in - c_in l_in, s_ex = un_ex + c_ex l_ex */
+    un_inb += s_inb;
+    c_inb -= s_inb * l_in;
+    const double l_inb = -s_inb * c_in;
+    un_exb += s_exb;
+    c_exb += s_exb * l_ex;
+    const double l_exb = s_exb * c_ex;
+    /* l = sqrt(W), W = (hs hs + hs h) / (2 h h) */
+    double hsb = 0;
+    if (sh_in && l_inb != 0.0) {
+        const double Wb = l_inb / (2.0 * l_in);
+        hsb += Wb * (2.0 * hs + h_in) / (2.0 * h_in * h_in);
+        h_inb += Wb * (hs / (2.0 * h_in * h_in) - (hs * hs + hs * h_in) / (h_in * h_in * h_in));
+    }
+    if (sh_ex && l_exb != 0.0) {
+        const double Wb = l_exb / (2.0 * l_ex);
+        hsb += Wb * (2.0 * hs + h_ex) / (2.0 * h_ex * h_ex);
+        h_exb += Wb * (hs / (2.0 * h_ex * h_ex) - (hs * hs + hs * h_ex) / (h_ex * h_ex * h_ex));
+    }
+    /* hs = P P / g */
+    const double Pb = hsb * 2.0 * P / g;
+    c_inb += 0.5 * Pb;
+    c_exb += 0.5 * Pb;
+    un_inb += 0.25 * Pb;
+    un_exb -= 0.25 * Pb;
+    /* c = sqrt(g h) */
+    h_inb += c_in == 0.0 ? 0.0 : c_inb * g / (2.0 * c_in);
+    h_exb += c_ex == 0.0 ? 0.0 : c_exb * g / (2.0 * c_ex);
+    /* un = u nx + v ny, ut = -u ny + v nx */
+    u_inb += un_inb * nx - ut_inb * ny;
+    v_inb += un_inb * ny + ut_inb * nx;
+    u_exb += un_exb * nx - ut_exb * ny;
+    v_exb += un_exb * ny + ut_exb * nx;
+    /* u = qx / h, v = qy / h */
+    b.qxin += u_inb / h_in;
+    b.qyin += v_inb / h_in;
+    h_inb -= (u_inb * u_in + v_inb * v_in) / h_in;
+    b.qxex += u_exb / h_ex;
+    b.qyex += v_exb / h_ex;
+    h_exb -= (u_exb * u_ex + v_exb * v_ex) / h_ex;
+    b.zin += h_inb;
+    b.zex += h_exb;
+    b.zed += zb + h_inb + h_exb;
+}
+
 /* reverse of numerical_flux */
 DGR_HD void numerical_flux_rev(int type, const double fhb[3], double zeta_in, double zeta_ex, double qx_in,
                                double qx_ex, double qy_in, double qy_ex, double z_edge, double nx, double ny,
@@ -250,6 +390,8 @@ DGR_HD void numerical_flux_rev(int type, const double fhb[3], double zeta_in, do
 {
     if (type == 1)
         llf_flux_rev(fhb, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g, b);
+    else if (type == 2)
+        hllc_flux_rev(fhb, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g, b);
     else
         roe_flux_rev(fhb, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g, b);
 }

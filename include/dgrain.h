@@ -96,7 +96,8 @@ typedef struct dgr_params {
                         zeta[6*el + m] etc. (see dgr_p2_reference). */
     int flux;        /* numerical flux at edges: 0 the Roe flux of 2DCode/numericalFlux2D.c:6-108
                         (default); 1 the local Lax-Friedrichs flux of DG-SWEM
-                        src/numerical_flux.F:887-1141 (extension).  Fixed at creation. */
+                        src/numerical_flux.F:887-1141; 2 DG-SWEM's HLLC flux (:1154-1400)
+                        (extensions, for flows that stay wet).  Fixed at creation. */
 } dgr_params;
 
 /* Mesh in the reference's arrays (2DCode/MeshAttributes.h:5-20), 0-based. */

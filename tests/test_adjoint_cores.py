@@ -80,10 +80,10 @@ def _roe(cores, x, nx, ny, lg, xd=None, yb=None):
     return y, yd, xb
 
 
-@pytest.fixture(params=[0, 1], ids=["roe", "llf"])
+@pytest.fixture(params=[0, 1, 2], ids=["roe", "llf", "hllc"])
 def flux(request, cores):
     """numerical flux of the edge cases: the Roe flux of 2DCode, the local Lax-Friedrichs
-    flux of DG-SWEM"""
+    and HLLC fluxes of DG-SWEM"""
     cores.dgr_t_set_flux(request.param)
     yield request.param
     cores.dgr_t_set_flux(0)
@@ -309,3 +309,29 @@ def test_limiter_dot_product_and_fd(cores, pdop):
         for b in (1, 2):
             assert any(s[1] == b for s in seen), seen  # PDop mass branches
             assert any(s[2] == b for s in seen), seen  # PDop momentum branches
+
+
+def _hllc_branch(x, nx, ny, g=G):
+    """HLLC branch of DG-SWEM's order (0 in, 1 in star, 2 ex star, 3 ex) for x = (zin, zex,
+    qxin, qxex, qyin, qyex, zedge)"""
+    h_in, h_ex = x[0] + x[6], x[1] + x[6]
+    un_in = (x[2] * nx + x[4] * ny) / h_in
+    un_ex = (x[3] * nx + x[5] * ny) / h_ex
+    c_in, c_ex = np.sqrt(g * h_in), np.sqrt(g * h_ex)
+    hs = (0.5 * (c_in + c_ex) + 0.25 * (un_in - un_ex)) ** 2 / g
+    l_in = np.sqrt((hs * hs + hs * h_in) / (2 * h_in * h_in)) if hs > h_in else 1.0
+    l_ex = np.sqrt((hs * hs + hs * h_ex) / (2 * h_ex * h_ex)) if hs > h_ex else 1.0
+    s_in, s_ex = un_in - c_in * l_in, un_ex + c_ex * l_ex
+    a, b = un_ex - s_ex, un_in - s_in
+    s_st = (s_in * h_ex * a - s_ex * h_in * b) / (h_ex * a - h_in * b)
+    return 0 if s_in >= 0 else (1 if s_st >= 0 else (2 if s_ex >= 0 else 3))
+
+
+def test_hllc_inputs_cover_every_branch():
+    """the random inputs of the flux tests reach all four HLLC branches"""
+    rng = np.random.default_rng(1)
+    seen = set()
+    for _ in range(400):
+        x, nx, ny = _roe_inputs(rng)
+        seen.add(_hllc_branch(x, nx, ny))
+    assert seen == {0, 1, 2, 3}, seen

@@ -1,5 +1,6 @@
-"""The local Lax-Friedrichs flux (dgr_params.flux = 1; DG-SWEM src/numerical_flux.F:887-1141,
-an extension with no 2DCode counterpart, so checked by the scheme's properties):
+"""DG-SWEM's local Lax-Friedrichs (dgr_params.flux = 1, src/numerical_flux.F:887-1141) and
+HLLC (flux = 2, :1154-1400) fluxes, extensions with no 2DCode counterpart, so checked by the
+scheme's properties, each flux:
   * a lake at rest stays at rest and a closed basin conserves its volume (p = 1 and p = 2);
   * a submerged tidal basin stays finite with positive depths and differs from the Roe run
     by a discretisation-sized amount;
@@ -28,11 +29,16 @@ def midpoint_field(m, f):
     return np.ascontiguousarray(f(mx, my).reshape(-1))
 
 
-def test_p1_lake_at_rest_and_volume(dgrain):
+@pytest.fixture(params=[1, 2], ids=["llf", "hllc"])
+def flux(request):
+    return request.param
+
+
+def test_p1_lake_at_rest_and_volume(dgrain, flux):
     m = dgrain.rectangle(24, 12, jitter=0.15, seed=4, datum=7.0, ocean=False)
     zero = np.zeros(3 * m.num_el)
     rest = (np.full(3 * m.num_el, 0.1), zero, zero.copy())
-    with dgrain.Solver(m, wet_dry=0, cfl=0.3, tide_on=0, flux=1) as s:
+    with dgrain.Solver(m, wet_dry=0, cfl=0.3, tide_on=0, flux=flux) as s:
         s.upload_state(*rest)
         s.time_evolution(1e300, 50)
         z, qx, qy, _ = s.download_state()
@@ -47,14 +53,14 @@ def test_p1_lake_at_rest_and_volume(dgrain):
     assert np.abs(qx).max() > 1e-3 and abs(v1 - v0) <= 1e-12 * abs(v0)
 
 
-def test_p1_tidal_basin_llf_vs_roe(dgrain):
+def test_p1_tidal_basin_vs_roe(dgrain, flux):
     """a submerged tidal basin (wet/dry on, every element wet): finite, positive depths,
     and within a discretisation-sized distance of the Roe run"""
     m = dgrain.rectangle(40, 20, jitter=0.1, seed=3, datum=7.0)
     st = dgrain.initial_state(m, np.zeros(m.num_nodes))
     out = []
-    for flux in (0, 1):
-        with dgrain.Solver(m, wet_dry=1, cfl=0.3, tide_on=1, tide_amp=0.5, flux=flux) as s:
+    for f in (0, flux):
+        with dgrain.Solver(m, wet_dry=1, cfl=0.3, tide_on=1, tide_amp=0.5, flux=f) as s:
             s.upload_state(*st)
             t, dt, n = s.time_evolution(1e300, 300)
             assert n == 300
@@ -67,11 +73,11 @@ def test_p1_tidal_basin_llf_vs_roe(dgrain):
     assert 0 < d < 0.05 * np.abs(z0).max(), (d, np.abs(z0).max())
 
 
-def test_p2_llf_well_balanced_and_convergent(dgrain):
+def test_p2_well_balanced_and_convergent(dgrain, flux):
     m = dgrain.rectangle(16, 8, jitter=0.15, seed=2, datum=7.0, ocean=False)
     c = dgrain.p2.project(m, lambda x, y: np.full_like(x, 0.1))
     zero = np.zeros_like(c)
-    with dgrain.Solver(m, order=2, wet_dry=0, cfl=0.1, rk_stages=3, tide_on=0, flux=1) as s:
+    with dgrain.Solver(m, order=2, wet_dry=0, cfl=0.1, rk_stages=3, tide_on=0, flux=flux) as s:
         s.upload_state(c, zero, zero.copy(), np.zeros(m.num_el, dtype=np.int32))
         s.time_evolution(1e300, 50)
         z, qx, qy, _ = s.download_state()
@@ -85,7 +91,7 @@ def test_p2_llf_well_balanced_and_convergent(dgrain):
         w = k * np.sqrt(9.81 * 10.0)
         c0 = dgrain.p2.project(mm, lambda x, y: 1e-5 * np.cos(k * x))
         zz = np.zeros_like(c0)
-        with dgrain.Solver(mm, order=2, wet_dry=0, cfl=0.1, rk_stages=3, tide_on=0, flux=1) as s:
+        with dgrain.Solver(mm, order=2, wet_dry=0, cfl=0.1, rk_stages=3, tide_on=0, flux=flux) as s:
             s.upload_state(c0, zz, zz.copy(), np.zeros(mm.num_el, dtype=np.int32))
             t, _, _ = s.time_evolution(250.0, 10 ** 6)
             z = s.download_state()[0]
@@ -96,7 +102,7 @@ def test_p2_llf_well_balanced_and_convergent(dgrain):
 
 
 @pytest.mark.parametrize("order", [1, 2])
-def test_llf_adjoint_is_transpose_of_tlm(dgrain, order):
+def test_adjoint_is_transpose_of_tlm(dgrain, flux, order):
     rng = np.random.default_rng(8)
     if order == 1:
         m = dgrain.rectangle(32, 16, jitter=0.1, seed=7)
@@ -113,7 +119,7 @@ def test_llf_adjoint_is_transpose_of_tlm(dgrain, order):
         el, w = dgrain.p2.gauge_weights(m, list(zip(rng.uniform(500, 9500, 6), rng.uniform(500, 4500, 6))))
         nm = 6
     n_el = rng.uniform(0.02, 0.05, m.num_el)
-    with dgrain.Solver(m, tide_on=1, tide_amp=0.5, flux=1, **kw) as s:
+    with dgrain.Solver(m, tide_on=1, tide_amp=0.5, flux=flux, **kw) as s:
         mis = dgrain.GaugeMisfit(s, 24, 8, el, w)
         s.set_element_manning(n_el * np.exp(rng.normal(0.0, 0.2, m.num_el)))
         _, vals = mis.forward(st)
