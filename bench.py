@@ -197,6 +197,54 @@ def ensemble_workload(nscen: int, seed: int = 7, lo: int = 5000, hi: int = 80000
     return meshes, params, states, sizes
 
 
+def _reference_ensemble_worker(job):
+    """one host process of the ensemble's CPU baseline: the reference C step (oracle/_ref)
+    on each of its scenarios in turn, `steps` timed steps after one warm-up step each;
+    returns (element-stage updates, seconds of the timed steps)"""
+    indices, nscen, steps = job
+    from oracle import oracle as O
+
+    meshes, params, states, _ = ensemble_workload(nscen, subset=indices)
+    updates, secs = 0, 0.0
+    for m, p, st in zip(meshes, params, states):
+        r = O.Reference(wet_dry=True)
+        r.set_mesh(m)
+        r.initialize()
+        r.set_state(*st)
+        rc, t, dt, n, _ = r.run(1, 1e9, CFL, tide_on=1, amp=p["tide_amp"], period=PERIOD, time=-1.0, dt=0.0)
+        t0 = time.perf_counter()
+        rc, t, dt, n, _ = r.run(steps, 1e9, CFL, tide_on=1, amp=p["tide_amp"], period=PERIOD, time=t, dt=dt)
+        secs += time.perf_counter() - t0
+        updates += m.num_el * 2 * n
+    return updates, secs
+
+
+def cpu_baseline_ensemble(nscen: int, steps: int = 2, max_workers: int = 64):
+    """The ensemble's CPU baseline: the scenarios as independent reference processes across
+    the host's cores (scenarios dealt out by size, largest first to the least loaded
+    process); aggregate rate = all updates / the slowest process's stepping time."""
+    import multiprocessing as mp
+
+    from dgrain.calibration import partition
+    from oracle import oracle as O
+
+    if not O.have_reference():
+        return None
+    workers = max(1, min(max_workers, os.cpu_count() or 1, nscen))
+    sizes = ensemble_workload(nscen, subset=[])[3]
+    shares = [s for s in partition(sizes, workers) if s]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(len(shares)) as pool:
+        res = pool.map(_reference_ensemble_worker, [(s, nscen, steps) for s in shares])
+    wall = time.perf_counter() - t0
+    updates = sum(u for u, _ in res)
+    slowest = max(s for _, s in res)
+    return {"value": updates / slowest, "unit": METRIC, "cores": len(shares), "kind": "reference",
+            "sample": f"all {nscen} scenarios, {steps} time steps each after one warm-up step, as {len(shares)} "
+                      f"independent processes of the unmodified 2DCode step (gcc -O2, wet/dry build; the reference "
+                      f"has no rain or per-element n, so those extensions are off), {wall:.1f} s wall"}
+
+
 def ensemble_bench(nscen: int, steps: int, warmup: int, device: int = 0, dist=None):
     """Batched ensemble (one context, every launch advances all scenarios, schedule picked
     by the autotuner) against the plain GPU step looped over the same scenarios (one
@@ -259,7 +307,9 @@ def ensemble_bench(nscen: int, steps: int, warmup: int, device: int = 0, dist=No
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         batched_ms, looped_wall, looped_dev = (float(v) for v in t.cpu().numpy())
     units = tot_el * 2 * steps
+    cpu = cpu_baseline_ensemble(nscen) if rank == 0 and world == 1 else None
     return {"scenarios": nscen, "ranks": world, "triangles": tot_el, "steps": steps, "warmup": warmup,
+            "cpu_baseline": cpu,
             "batched": units / (batched_ms / 1e3), "looped": units / (looped_wall / 1e3),
             "looped_device_only": units / (looped_dev / 1e3),
             "speedup": looped_wall / batched_ms, "unit": METRIC, "bit_identical": bool(same),
