@@ -141,13 +141,15 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline_reference(m, st, steps: int = 2, warmup: int = 1, max_seconds: float = 60.0):
+def cpu_baseline_reference(m, st, steps: int = 2, warmup: int = 1, max_seconds: float = 60.0,
+                           optimised: bool = False):
     """The reference C step (oracle/_ref, unmodified 2DCode compiled with gcc -O2) on this
-    host, one core, on the same mesh and state; falls back to the oracle restatement."""
+    host, one core, on the same mesh and state; falls back to the oracle restatement.
+    optimised: the -O3 -march=x86-64-v3 build of the same sources (timing only)."""
     from oracle import oracle as O
 
     if O.have_reference():
-        r = O.Reference(wet_dry=True)
+        r = O.Reference(wet_dry=True, optimised=optimised)
         r.set_mesh(m)
         r.initialize()
         r.set_state(*st)
@@ -167,9 +169,13 @@ def cpu_baseline_reference(m, st, steps: int = 2, warmup: int = 1, max_seconds: 
         done += 1
     el = time.perf_counter() - t0
     value = m.num_el * 2 * done / el if done else 0.0
-    return {"value": value, "unit": METRIC, "cores": 1, "kind": kind,
-            "sample": f"{done} time steps of the {m.num_el}-triangle workload after {warmup} warm-up step(s), "
-                      f"{el:.1f} s, gcc -O2 build, one host core"}
+    out = {"value": value, "unit": METRIC, "cores": 1, "kind": kind,
+           "sample": f"{done} time steps of the {m.num_el}-triangle workload after {warmup} warm-up step(s), "
+                     f"{el:.1f} s, gcc {'-O3 -march=x86-64-v3' if optimised else '-O2'} build, one host core"}
+    if kind == "reference" and not optimised and os.path.exists(O.REF_LIB_WD_O3):
+        o3 = cpu_baseline_reference(m, st, steps=steps, warmup=warmup, max_seconds=max_seconds, optimised=True)
+        out["o3_x86_64_v3"] = {"value": o3["value"], "sample": o3["sample"]}
+    return out
 
 
 def ensemble_workload(nscen: int, seed: int = 7, lo: int = 5000, hi: int = 80000, subset=None):

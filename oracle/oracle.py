@@ -19,6 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref2d.so")
 REF_LIB_WD = os.path.join(HERE, "_ref", "libref2d_wd.so")
+REF_LIB_WD_O3 = os.path.join(HERE, "_ref", "libref2d_wd_o3.so")  # -O3 -march=x86-64-v3, timing only
 
 dptr = C.POINTER(C.c_double)
 iptr = C.POINTER(C.c_int)
@@ -198,8 +199,8 @@ class Reference:
 
     _libs: dict = {}
 
-    def __init__(self, wet_dry: bool):
-        path = REF_LIB_WD if wet_dry else REF_LIB
+    def __init__(self, wet_dry: bool, optimised: bool = False):
+        path = (REF_LIB_WD_O3 if optimised else REF_LIB_WD) if wet_dry else REF_LIB
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} not built (the reference tree was not available)")
         if path not in Reference._libs:
