@@ -43,3 +43,17 @@ def test_p2_and_ensemble_dat(dgrain, tmp_path):
     for name, v in (("z", z), ("qx", qx)):
         want = "".join("".join("%1.15f\t\t" % x for x in row) + "\n" for row in v.reshape(-1, 6))
         assert (tmp_path / f"{name}.dat").read_text() == want, name
+
+
+def test_unformattable_value_is_refused(dgrain, tmp_path):
+    """a value of magnitude >= 2^63 is refused with DGR_ERR_INVALID and its file removed"""
+    m = dgrain.rectangle(6, 3, seed=1)
+    z = np.zeros(3 * m.num_el)
+    qx = z.copy()
+    qx[4] = 1e19
+    with dgrain.Solver(m, wet_dry=0) as s:
+        s.upload_state(z, qx, z.copy())
+        with pytest.raises(dgrain.DgrError) as ei:
+            s.write_state_dat(tmp_path / "z.dat", tmp_path / "qx.dat")
+        assert ei.value.code == dgrain._lib.DGR_ERR_INVALID
+    assert (tmp_path / "z.dat").exists() and not (tmp_path / "qx.dat").exists()
