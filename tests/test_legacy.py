@@ -70,3 +70,29 @@ def test_legacy_program_matches_reference_program(dgrain, tmp_path, manning):
         else:
             x, y = np.loadtxt(outs["ref"][0] / f"{f}.dat"), np.loadtxt(outs["gpu"][0] / f"{f}.dat")
             assert np.abs(x - y).max() <= 1e-11 * max(np.abs(x).max(), 1e-300), f
+
+
+@needs_bins
+@pytest.mark.gpu
+@pytest.mark.parametrize("manning", [0.0, 0.03])
+def test_legacy_program_config1_length(dgrain, tmp_path, manning):
+    """The same comparison on the 1,600-triangle rectangle (40 x 20 cells, no jitter) over
+    more than 2,000 steps of the reference program as shipped (submerged, so that the
+    build without wet/dry handling runs)."""
+    outs = {}
+    for name, binary in (("ref", BIN_REF), ("gpu", BIN_GPU)):
+        d = tmp_path / name
+        d.mkdir()
+        m = dgrain.rectangle(40, 20, jitter=0.0, seed=5, datum=7.0, manning=manning)
+        dgrain.write_fort14(m, str(d / "fort.14"))
+        rc, out = run(binary, d, 5000.0)
+        assert rc == 0, out[-2000:]
+        outs[name] = (d, out)
+    lines = {k: [ln for ln in v[1].splitlines() if ln.startswith(("dt =", "time ="))] for k, v in outs.items()}
+    assert len(lines["ref"]) >= 2 * 2000 and lines["gpu"] == lines["ref"], len(lines["ref"])
+    for f in ("001_H", "001_Qx", "001_Qy"):
+        if manning == 0.0:
+            assert (outs["ref"][0] / f"{f}.dat").read_text() == (outs["gpu"][0] / f"{f}.dat").read_text(), f
+        else:
+            x, y = np.loadtxt(outs["ref"][0] / f"{f}.dat"), np.loadtxt(outs["gpu"][0] / f"{f}.dat")
+            assert np.abs(x - y).max() <= 1e-11 * max(np.abs(x).max(), 1e-300), f
