@@ -78,7 +78,11 @@ def test_legacy_program_matches_reference_program(dgrain, tmp_path, manning):
 def test_legacy_program_config1_length(dgrain, tmp_path, manning):
     """The same comparison on the 1,600-triangle rectangle (40 x 20 cells, no jitter) over
     more than 2,000 steps of the reference program as shipped (submerged, so that the
-    build without wet/dry handling runs)."""
+    build without wet/dry handling runs).  Without friction the text is identical; with
+    friction the correctly rounded H^(4/3) of the device and glibc's pow (not correctly
+    rounded for about 0.1 % of arguments) differ by an ulp now and then, and over 2,250
+    steps those ulps add up to 1.5e-11 of the field's maximum (measured): the bound here is
+    3e-11, the per-step one (120-150 steps, the other tests) stays 1e-11."""
     outs = {}
     for name, binary in (("ref", BIN_REF), ("gpu", BIN_GPU)):
         d = tmp_path / name
@@ -95,4 +99,4 @@ def test_legacy_program_config1_length(dgrain, tmp_path, manning):
             assert (outs["ref"][0] / f"{f}.dat").read_text() == (outs["gpu"][0] / f"{f}.dat").read_text(), f
         else:
             x, y = np.loadtxt(outs["ref"][0] / f"{f}.dat"), np.loadtxt(outs["gpu"][0] / f"{f}.dat")
-            assert np.abs(x - y).max() <= 1e-11 * max(np.abs(x).max(), 1e-300), f
+            assert np.abs(x - y).max() <= 3e-11 * max(np.abs(x).max(), 1e-300), f
