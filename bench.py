@@ -504,7 +504,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--ny", type=int, default=NY)
-    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--e2e-steps", type=int, default=-1,
+                    help="steps of the end-to-end run (default: --steps, the workload's length; 0: none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=90.0)
     ap.add_argument("--ensemble-scenarios", type=int, default=256)
@@ -521,6 +522,8 @@ def main():
     ap.add_argument("--no-calibration", action="store_true")
     ap.add_argument("--io", action="store_true", help="add the mesh-ingest and .dat-writer comparison")
     args = ap.parse_args()
+    if args.e2e_steps < 0:
+        args.e2e_steps = args.steps
     if args.impl == "reference":
         return run_reference_arm(args)
 
