@@ -477,6 +477,46 @@ def calibration_bench(nscen: int, steps: int, ckpt: int, iterations: int, device
     return out
 
 
+def io_bench(m, solver, outdir: str):
+    """Mesh ingest and snapshot output on the bench mesh: connectivity by the host builder
+    (hashed, O(E)) and by the GPU builder (sorted), identical arrays required; the three
+    .dat snapshot files of the current state written by the device formatter and by the host
+    writer (download + printf), identical bytes required."""
+    import copy
+
+    import dgrain
+
+    base = copy.deepcopy(m)
+    t0 = time.perf_counter()
+    a = dgrain.build_connectivity(copy.deepcopy(base))
+    host_s = time.perf_counter() - t0
+    dgrain.build_connectivity(copy.deepcopy(base), device=True)  # first call: module load
+    t0 = time.perf_counter()
+    b = dgrain.build_connectivity(copy.deepcopy(base), device=True)
+    dev_s = time.perf_counter() - t0
+    same_mesh = all(np.array_equal(getattr(a, k), getattr(b, k)) for k in ("ed2v", "ed2el", "bdry")) and \
+        a.min_edge == b.min_edge
+    os.makedirs(outdir, exist_ok=True)
+    paths = [os.path.join(outdir, f"dev_{v}.dat") for v in ("H", "Qx", "Qy")]
+    t0 = time.perf_counter()
+    solver.write_state_dat(*paths)
+    dev_w = time.perf_counter() - t0
+    lib = dgrain.load()
+    t0 = time.perf_counter()
+    st = solver.download_state()
+    hpaths = [os.path.join(outdir, f"host_{v}.dat") for v in ("H", "Qx", "Qy")]
+    for p, v in zip(hpaths, st[:3]):
+        lib.dgr_write_dat(p.encode(), m.num_el, v.ctypes.data_as(dgrain._lib.dptr))
+    host_w = time.perf_counter() - t0
+    same_dat = all(open(p, "rb").read() == open(q, "rb").read() for p, q in zip(paths, hpaths))
+    nbytes = sum(os.path.getsize(p) for p in paths)
+    for p in paths + hpaths:
+        os.remove(p)
+    return {"triangles": m.num_el, "connectivity_host_s": host_s, "connectivity_device_s": dev_s,
+            "connectivity_identical": bool(same_mesh), "dat_device_s": dev_w, "dat_host_s": host_w,
+            "dat_bytes": nbytes, "dat_identical": bool(same_dat)}
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:

@@ -290,7 +290,7 @@ extern "C" int dgr_adjoint_forward(dgr_ctx *c, const double *zeta, const double 
         clock_begin_step(c, n, replay_dt);
         for (int st = 0; st < c->p.rk_stages; ++st) launch_stage(c, st, true);
         k_clock_end<<<blocks(nsc, 128), 128, 0, s>>>(c->clk, nsc);
-        k_misfit<<<1, 32, 0, s>>>(c->U, c->ldE, a->nw, a->ng, a->g_el, a->g_w, a->target + (size_t)n * a->ng,
+        k_misfit<<<blocks(a->ng, 128), 128, 0, s>>>(c->U, c->ldE, a->nw, a->ng, a->g_el, a->g_w, a->target + (size_t)n * a->ng,
                                   a->resid + (size_t)n * a->ng);
         c->launches += 3;
     }
@@ -705,9 +705,9 @@ static int run_lanes(dgr_ctx *c, double *J, double *out2)
                 lanes_stage_p1<T>(c, n, stage);
         }
         /* residuals of the base lane and of the second lane (a tangent has target 0) */
-        k_misfit<<<1, 32, 0, s>>>(c->U, c->ldE, a->nw, a->ng, a->g_el, a->g_w, a->target + (size_t)n * a->ng,
+        k_misfit<<<blocks(a->ng, 128), 128, 0, s>>>(c->U, c->ldE, a->nw, a->ng, a->g_el, a->g_w, a->target + (size_t)n * a->ng,
                                   a->rt + (size_t)n * a->ng);
-        k_misfit<<<1, 32, 0, s>>>(a->Ud, c->ldE, a->nw, a->ng, a->g_el, a->g_w,
+        k_misfit<<<blocks(a->ng, 128), 128, 0, s>>>(a->Ud, c->ldE, a->nw, a->ng, a->g_el, a->g_w,
                                   pert ? a->target + (size_t)n * a->ng : nullptr, a->rd + (size_t)n * a->ng);
         c->launches += 2;
     }

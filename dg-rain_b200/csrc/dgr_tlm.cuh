@@ -179,12 +179,12 @@ static __global__ void __launch_bounds__(256) k_adj_forcing(const DevClock *clk,
 
 /* Gauge residuals of the state after step n: r_g = sum_k w_gk zeta_k(el_g) - target_g
  * (target null: 0), nw weights per gauge over the elevation planes 0..nw-1 (the three
- * midpoint values at p = 1, the six modes at p = 2).  One warp; the objective is summed
- * later in a fixed order. */
+ * midpoint values at p = 1, the six modes at p = 2).  One thread per gauge; the objective
+ * is summed later in a fixed order. */
 static __global__ void k_misfit(const double *__restrict__ S, int ld, int nw, int ng, const int *__restrict__ g_el,
                          const double *__restrict__ g_w, const double *__restrict__ target, double *__restrict__ resid)
 {
-    for (int g = threadIdx.x; g < ng; g += blockDim.x) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
         const int el = g_el[g];
         double z = g_w[nw * g] * S[el];
         for (int k = 1; k < nw; ++k) z += g_w[nw * g + k] * S[(size_t)k * ld + el];
