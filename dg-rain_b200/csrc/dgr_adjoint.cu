@@ -368,12 +368,7 @@ static void recorded_stage(dgr_ctx *c, int j, int stage, const double *S, double
     }
     const bool wd = c->p.wet_dry != 0;
     double *R = seg_R(c, j, stage), *avg = seg_avg(c, j, stage), *bnd = seg_B(c, j, stage);
-    if (wd)
-        k_edge_flux<true><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, c->flux, c->clk, stage,
-                                                             2 * stage, c->p.g);
-    else
-        k_edge_flux<false><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, c->flux, c->clk,
-                                                              stage, 2 * stage, c->p.g);
+    launch_edge(c, S, wd_in, stage, 2 * stage);
     if (mode == MODE_STAGE1)
         k_element<MODE_STAGE1, 128><<<nb, 128, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
     else if (mode == MODE_STAGE2)
@@ -464,10 +459,20 @@ static void reverse_stage(dgr_ctx *c, int j, int n, int stage)
     else
         ADJ_EL(MODE_RK3_3);
 #undef ADJ_EL
-    if (wd)
-        k_adj_edge<true><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, a->fbar, lamS, a->zeb, g);
-    else
-        k_adj_edge<false><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, a->fbar, lamS, a->zeb, g);
+#define ADJ_EDGE(W, F) \
+    k_adj_edge<W, F><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, a->fbar, lamS, a->zeb, g)
+    if (c->p.flux == 0) { /* the reference's Roe flux, compiled alone */
+        if (wd)
+            ADJ_EDGE(true, 0);
+        else
+            ADJ_EDGE(false, 0);
+    } else {
+        if (wd)
+            ADJ_EDGE(true, -1);
+        else
+            ADJ_EDGE(false, -1);
+    }
+#undef ADJ_EDGE
     c->launches += 4;
 }
 

@@ -744,15 +744,22 @@ static void launch_limit(dgr_ctx *c, double *S, const int *wd_in, int *wd_out, i
     }
 }
 
-static void launch_edge(dgr_ctx *c, const double *S, const int *wd, int lam_slot, int phase)
+template <bool WD, int FT>
+static void launch_edge_ft(dgr_ctx *c, const double *S, const int *wd, int lam_slot, int phase)
 {
-    const MeshDev m = mesh_dev(c);
-    if (c->p.wet_dry)
-        k_edge_flux<true><<<blocks(c->nf, 256), 256, 0, c->stream>>>(m, S, wd, c->bzeta, c->bqn, c->flux, c->clk,
-                                                                     lam_slot, phase, c->p.g);
-    else
-        k_edge_flux<false><<<blocks(c->nf, 256), 256, 0, c->stream>>>(m, S, wd, c->bzeta, c->bqn, c->flux, c->clk,
-                                                                      lam_slot, phase, c->p.g);
+    k_edge_flux<WD, FT><<<blocks(c->nf, 256), 256, 0, c->stream>>>(mesh_dev(c), S, wd, c->bzeta, c->bqn, c->flux,
+                                                                   c->clk, lam_slot, phase, c->p.g);
+}
+
+/* the edge kernel compiled for the context's wet/dry mode and numerical flux */
+void launch_edge(dgr_ctx *c, const double *S, const int *wd, int lam_slot, int phase)
+{
+    const bool w = c->p.wet_dry != 0;
+    switch (c->p.flux) {
+    case 1: w ? launch_edge_ft<true, 1>(c, S, wd, lam_slot, phase) : launch_edge_ft<false, 1>(c, S, wd, lam_slot, phase); break;
+    case 2: w ? launch_edge_ft<true, 2>(c, S, wd, lam_slot, phase) : launch_edge_ft<false, 2>(c, S, wd, lam_slot, phase); break;
+    default: w ? launch_edge_ft<true, 0>(c, S, wd, lam_slot, phase) : launch_edge_ft<false, 0>(c, S, wd, lam_slot, phase);
+    }
 }
 
 /* one RK stage of the p = 2 step: edge fluxes at the Gauss points, element update */

@@ -89,7 +89,9 @@ struct PhysParams {
 
 /* One edge (2DCode/compute2DL.c:17-331): traces, ghost state, Roe flux(es); stores Fhat.n
  * for both sides and returns the edge's max wave speed (0 for a finished scenario). */
-template <bool WD, bool COH = false>
+/* FT: the numerical flux as a compile-time constant (0 Roe, 1 LLF, 2 HLLC), or -1 to take
+ * it from the mesh at run time */
+template <bool WD, bool COH = false, int FT = -1>
 DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, const double *bzeta,
                               const double *bqn, double *flux, DevClock *clk, int phase, double g, int i)
 {
@@ -115,7 +117,8 @@ DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, 
         const int wdi = WD ? ldm<COH>(&wd[el_in]) : 1, wde = WD ? ldm<COH>(&wd[el_ex]) : 1;
         double fin[3], fex[3];
         int code;
-        lam = flux_core<double, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code, m.flux);
+        lam = flux_core<double, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code,
+                                    FT >= 0 ? FT : m.flux);
         if (code) atomicMin(&ck->err, err_key(ldm<COH>(&ck->step), phase, code, i - ck->ed_off));
         const int lf = m.ldF;
         flux[i] = fin[0];
@@ -157,7 +160,7 @@ DGR_DEV void block_max_speed(double lam, int sid, bool valid, DevClock *clk, int
     }
 }
 
-template <bool WD>
+template <bool WD, int FT>
 __global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, const double *__restrict__ S,
                                                                   const int *__restrict__ wd,
                                                                   const double *__restrict__ bzeta,
@@ -168,7 +171,7 @@ __global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, con
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < m.nf;
     const int sid = (valid && m.ed_sid) ? m.ed_sid[i] : 0;
-    const double lam = valid ? edge_flux_item<WD>(m, S, wd, bzeta, bqn, flux, clk, phase, g, i) : 0.0;
+    const double lam = valid ? edge_flux_item<WD, false, FT>(m, S, wd, bzeta, bqn, flux, clk, phase, g, i) : 0.0;
     block_max_speed(lam, sid, valid, clk, lam_slot);
 }
 

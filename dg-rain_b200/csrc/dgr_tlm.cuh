@@ -557,7 +557,7 @@ __global__ void __launch_bounds__(128, DGR_ADJ_MINB_ELEMENT) k_adj_element(MeshD
 
 /* edge reverse: Roe flux(es), ghost states; adds the trace adjoints into the slots of the
  * adjacent elements (each slot belongs to one edge side) and the mid-edge depth adjoint */
-template <bool WD>
+template <bool WD, int FT = -1>
 __global__ void __launch_bounds__(256, DGR_ADJ_MINB_EDGE) k_adj_edge(MeshDev m, const double *__restrict__ S, const int *__restrict__ wd,
                                                   const double *__restrict__ bzeta, const double *__restrict__ bqn,
                                                   const double *__restrict__ fbar, double *__restrict__ lamS,
@@ -589,7 +589,7 @@ __global__ void __launch_bounds__(256, DGR_ADJ_MINB_EDGE) k_adj_edge(MeshDev m, 
         fexb[k] = boundary ? 0.0 : fbar[(3 + k) * lf + i]; /* no element gathers a boundary edge's ex side */
     }
     EdgeBar b = {0, 0, 0, 0, 0, 0, 0};
-    flux_core_rev<WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, finb, fexb, b, m.flux);
+    flux_core_rev<WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, finb, fexb, b, FT >= 0 ? FT : m.flux);
     if (boundary) {
         ghost_state_rev(bd, nx, ny, bz, bq, b.ze, b.qxe, b.qye, b.zi, b.qxi, b.qyi);
     } else {
