@@ -683,7 +683,12 @@ def main():
             lib.dgr_host_free(C.c_void_p(host[k].ctypes.data))
         lib.dgr_host_free(C.c_void_p(wdp))
 
-    io = io_bench(m, solver, os.path.join("gpurun_out", "io_tmp")) if args.io and rank == 0 else None
+    io = None
+    if args.io and rank == 0:
+        import tempfile
+
+        with tempfile.TemporaryDirectory() as tmp:
+            io = io_bench(m, solver, tmp)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
