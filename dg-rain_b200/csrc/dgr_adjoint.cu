@@ -350,8 +350,7 @@ static void recorded_stage(dgr_ctx *c, int j, int stage, const double *S, double
     const double *U = seg_U(c, j);
     const unsigned nb = blocks(c->ne, 128);
     if (c->p.order == 2) {
-        k_p2_edge<128><<<blocks(c->nf, 128), 128, 0, s>>>(c->p2ref, m, c->p2g, S, c->bzeta, c->bqn, c->flux, c->clk,
-                                                          stage, 2 * stage, c->p.g);
+        launch_p2_edge(c, S, stage, 2 * stage);
 #define P2_EL(MD) \
     k_p2_element<MD, 128><<<nb, 128, 0, s>>>(c->p2ref, m, c->p2g, S, U, c->flux, OUT, c->clk, c->p.g)
         if (mode == MODE_STAGE1)
@@ -413,7 +412,12 @@ static void reverse_stage_p2(dgr_ctx *c, int j, int n, int stage)
     else
         P2_ADJ_EL(MODE_RK3_3);
 #undef P2_ADJ_EL
-    k_p2_adj_edge<<<blocks(c->nf, 128), 128, 0, s>>>(c->p2ref, m, c->p2g, S, c->bzeta, c->bqn, a->fbar, a->zeb, g);
+    if (c->p.flux == 0)
+        k_p2_adj_edge<0><<<blocks(c->nf, 128), 128, 0, s>>>(c->p2ref, m, c->p2g, S, c->bzeta, c->bqn, a->fbar, a->zeb,
+                                                            g);
+    else
+        k_p2_adj_edge<-1><<<blocks(c->nf, 128), 128, 0, s>>>(c->p2ref, m, c->p2g, S, c->bzeta, c->bqn, a->fbar,
+                                                             a->zeb, g);
     k_p2_adj_trace<<<nb, 128, 0, s>>>(c->p2ref, m, a->fbar, lamS);
     c->launches += 3;
 }

@@ -762,14 +762,26 @@ void launch_edge(dgr_ctx *c, const double *S, const int *wd, int lam_slot, int p
     }
 }
 
+/* p = 2 edge fluxes of state S: the Roe flux compiled alone, the other fluxes by run-time
+ * choice */
+void launch_p2_edge(dgr_ctx *c, const double *S, int lam_slot, int phase)
+{
+    const MeshDev m = mesh_dev(c);
+    if (c->p.flux == 0)
+        k_p2_edge<128, 0><<<blocks(c->nf, 128), 128, 0, c->stream>>>(c->p2ref, m, c->p2g, S, c->bzeta, c->bqn,
+                                                                     c->flux, c->clk, lam_slot, phase, c->p.g);
+    else
+        k_p2_edge<128, -1><<<blocks(c->nf, 128), 128, 0, c->stream>>>(c->p2ref, m, c->p2g, S, c->bzeta, c->bqn,
+                                                                      c->flux, c->clk, lam_slot, phase, c->p.g);
+}
+
 /* one RK stage of the p = 2 step: edge fluxes at the Gauss points, element update */
 static void launch_p2_stage(dgr_ctx *c, int stage, bool count)
 {
     const StageIO io = stage_io(c, stage);
     const MeshDev m = mesh_dev(c);
     cudaStream_t s = c->stream;
-    k_p2_edge<128><<<blocks(c->nf, 128), 128, 0, s>>>(c->p2ref, m, c->p2g, io.S, c->bzeta, c->bqn, c->flux, c->clk,
-                                                      stage, 2 * stage, c->p.g);
+    launch_p2_edge(c, io.S, stage, 2 * stage);
     const unsigned nb = blocks(c->ne, 128);
     switch (io.mode) {
     case MODE_STAGE1:
@@ -1000,8 +1012,7 @@ extern "C" int dgr_compute_L(dgr_ctx *c, double time, double *rz, double *rqx, d
     k_clock_set<<<1, 1, 0, s>>>(c->clk, 0.0, 0.0);
     if (c->p.order == 2) {
         const MeshDev m = mesh_dev(c);
-        k_p2_edge<128><<<blocks(c->nf, 128), 128, 0, s>>>(c->p2ref, m, c->p2g, c->U, c->bzeta, c->bqn, c->flux,
-                                                          c->clk, 0, 0, c->p.g);
+        launch_p2_edge(c, c->U, 0, 0);
         k_p2_element<MODE_RHS, 128><<<blocks(c->ne, 128), 128, 0, s>>>(c->p2ref, m, c->p2g, c->U, c->U, c->flux,
                                                                        c->W, c->clk, c->p.g);
     } else {
@@ -1371,8 +1382,7 @@ static int profile_p2(dgr_ctx *c, int nsteps, double *kernel_ms)
         for (int stage = 0; stage < c->p.rk_stages; ++stage) {
             const StageIO io = stage_io(c, stage);
             cudaEventRecord(ev[0], s);
-            k_p2_edge<128><<<blocks(c->nf, 128), 128, 0, s>>>(c->p2ref, m, c->p2g, io.S, c->bzeta, c->bqn, c->flux,
-                                                              c->clk, stage, 2 * stage, c->p.g);
+            launch_p2_edge(c, io.S, stage, 2 * stage);
             cudaEventRecord(ev[1], s);
             const unsigned nb = blocks(c->ne, 128);
             if (io.mode == MODE_STAGE1)

@@ -171,6 +171,7 @@ int read_clock(dgr_ctx *c);                      /* device clocks -> h_clk (sync
 int write_clock(dgr_ctx *c);                     /* h_clk -> device clocks (synchronises) */
 void launch_stage(dgr_ctx *c, int stage, bool count); /* one RK stage, four kernels */
 void launch_edge(dgr_ctx *c, const double *S, const int *wd, int lam_slot, int phase); /* p = 1 edge fluxes */
+void launch_p2_edge(dgr_ctx *c, const double *S, int lam_slot, int phase);            /* p = 2 edge fluxes */
 void launch_wd_refresh(dgr_ctx *c);              /* status for the next step when stale */
 int decode_err(unsigned long long key, int *code, int *index, int *step);
 int first_error(const dgr_ctx *c);               /* first scenario failure code in h_clk */

@@ -228,7 +228,8 @@ struct P2PlaneZ {
 
 /* --------------------------------------------------------------- kernels ---- */
 
-template <int BS>
+/* FT: the numerical flux as a compile-time constant, or -1 to take it from the mesh */
+template <int BS, int FT = -1>
 __global__ void __launch_bounds__(BS, DGR_P2_MINB_EDGE) k_p2_edge(P2Ref ref, MeshDev m, const double *__restrict__ p2g,
                                                 const double *__restrict__ S, const double *__restrict__ bzeta,
                                                 const double *__restrict__ bqn, double *__restrict__ flux,
@@ -252,7 +253,7 @@ __global__ void __launch_bounds__(BS, DGR_P2_MINB_EDGE) k_p2_edge(P2Ref ref, Mes
             double fh[P2_NGP][3];
             int code;
             lam = p2_edge_core<double>(ref, st, el_in, el_ex, info, nx, ny, za, zb, bd ? bzeta[i] : 0.0,
-                                       bd ? bqn[i] : 0.0, g, fh, code, m.flux);
+                                       bd ? bqn[i] : 0.0, g, fh, code, FT >= 0 ? FT : m.flux);
             if (code) atomicMin(&ck->err, err_key(ck->step, phase, code, i - ck->ed_off));
 #pragma unroll
             for (int gp = 0; gp < P2_NGP; ++gp)

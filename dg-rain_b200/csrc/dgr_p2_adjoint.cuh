@@ -336,7 +336,8 @@ __global__ void __launch_bounds__(128, DGR_P2_MINB_ADJ_ELEMENT) k_p2_adj_element
  * the flux adjoints in fbar, and the adjoints of the Gauss-point depths go to the edge's
  * end vertices (zeb).
  */
-static __global__ void __launch_bounds__(128, DGR_P2_MINB_ADJ_EDGE) k_p2_adj_edge(P2Ref ref, MeshDev m, const double *__restrict__ p2g,
+template <int FT = -1>
+__global__ void __launch_bounds__(128, DGR_P2_MINB_ADJ_EDGE) k_p2_adj_edge(P2Ref ref, MeshDev m, const double *__restrict__ p2g,
                                                             const double *__restrict__ S,
                                                             const double *__restrict__ bzeta,
                                                             const double *__restrict__ bqn, double *__restrict__ fbar,
@@ -382,7 +383,7 @@ static __global__ void __launch_bounds__(128, DGR_P2_MINB_ADJ_EDGE) k_p2_adj_edg
         for (int v = 0; v < 3; ++v)
             fhb[v] = fbar[(3 * gp + v) * lf + i] + (boundary ? 0.0 : fbar[(9 + 3 * gp + v) * lf + i]);
         RoeBar b = {0, 0, 0, 0, 0, 0, 0};
-        numerical_flux_rev(m.flux, fhb, ui[0], ue[0], ui[1], ue[1], ui[2], ue[2], z_g, nx, ny, g, g, b);
+        numerical_flux_rev(FT >= 0 ? FT : m.flux, fhb, ui[0], ue[0], ui[1], ue[1], ui[2], ue[2], z_g, nx, ny, g, g, b);
         if (boundary) ghost_state_rev(bd, nx, ny, bz, bq, b.zex, b.qxex, b.qyex, b.zin, b.qxin, b.qyin);
         fbar[(3 * gp) * lf + i] = b.zin;
         fbar[(3 * gp + 1) * lf + i] = b.qxin;
