@@ -258,7 +258,7 @@ DGR_HD double fma_exact(double a, double b, double c)
 #endif
 }
 
-DGR_HD double pow43(double x)
+DGR_HD double pow43_exact(double x)
 {
     if (!(x >= 1e-200 && x <= 1e200)) return pow(x, 4. / 3);
     const double c0 = cbrt(x);
@@ -273,6 +273,62 @@ DGR_HD double pow43(double x)
     const double eta = log(x) * -7.401486830834377e-17;
     const double lo = (p_l - x * d) + p_h * eta;
     return p_h + lo;
+}
+
+/*
+ * pow43 on the device: the same correctly rounded value in two phases (Ziv's strategy).
+ *   Fast phase, for 2^-120 <= x < 2^120 (every float conversion below stays normal):
+ *     1. r0 = rcbrtf(x) (float, 1 ulp), one Newton step in double for x^(-1/3):
+ *        r1 = r0 + r0 (1 - x r0^3)/3, relative error 2 e0^2 ~ 2^-44;
+ *     2. c0 = x r1^2 ~ cbrt(x) to 2^-43, corrected by c = c0 - (c0^3 - x)/(3 c0^2) with the
+ *        residual formed exactly as in pow43_exact and 1/(3 c0^2) taken as r1^2/3: the
+ *        error left is ~2^-84 relative;
+ *     3. eta = -ln(x)/(3*2^52) from the exponent and a float log2 of the mantissa
+ *        (absolute error of log2 below 2^-21.5 on [1, 2)): eta is off by < 2^-75 relative.
+ *   The result y = RN(x c e^eta) is then within 2^-74 of x^p, so when both ends of the
+ *   interval +-2^-70 |y| round to the same double, that double is the correctly rounded
+ *   x^p.  Otherwise (x^p within 2^-70 of a rounding midpoint, about 1 argument in 10^5)
+ *   pow43_exact, whose error is a few 2^-100, decides.  The host keeps pow43_exact.
+ */
+#ifdef __CUDA_ARCH__
+DGR_DEV double pow43_fast_or_exact(double x)
+{
+    if (!(x >= 0x1p-120 && x < 0x1p120)) return pow43_exact(x);
+    const double r0 = (double)rcbrtf(__double2float_rn(x));
+    const double q = r0 * r0; /* exact: 24-bit significands */
+    const double t = __fma_rn(-x, q * r0, 1.0);
+    const double r1 = __fma_rn(r0 * t, 0x1.5555555555555p-2, r0);
+    const double c0 = (x * r1) * r1;
+    const double a_h = c0 * c0;
+    const double a_l = __fma_rn(c0, c0, -a_h);
+    const double b_h = a_h * c0;
+    const double b_l = __fma_rn(a_h, c0, -b_h);
+    const double res = ((b_h - x) + b_l) + a_l * c0; /* c0^3 - x */
+    const double d = res * ((r1 * r1) * 0x1.5555555555555p-2);
+    const double p_h = x * c0;
+    const double p_l = __fma_rn(x, c0, -p_h);
+    /* x = 2^e m, m in [1, 2) */
+    const int hi = __double2hiint(x);
+    const int e = ((hi >> 20) & 0x7ff) - 1023;
+    const double m = __hiloint2double((hi & 0x000fffff) | 0x3ff00000, __double2loint(x));
+    const double lg2 = (double)e + (double)__log2f(__double2float_rn(m));
+    const double eta = lg2 * -0x1.d9303fea2f7eap-55; /* -ln(2)/(3*2^52) */
+    const double lo = (p_l - x * d) + p_h * eta;
+    const double err = p_h * 0x1p-70;
+    const double y_lo = p_h + (lo - err);
+    const double y_hi = p_h + (lo + err);
+    if (y_lo == y_hi) return y_lo;
+    return pow43_exact(x);
+}
+#endif
+
+DGR_HD double pow43(double x)
+{
+#ifdef __CUDA_ARCH__
+    return pow43_fast_or_exact(x);
+#else
+    return pow43_exact(x);
+#endif
 }
 
 /* x / d for the limiter's redistribution count d in {1, 2, 3} (as a double).  Division

@@ -222,4 +222,11 @@ int dgr_t_limit(int pdop, const double *w, const double *bmax, const double *bmi
     return 0;
 }
 
+/* the Manning power x^(4./3) as the host compiles it (pow43_exact: cbrt refined by one
+ * Newton step with exact residuals, log-based exponent correction) */
+void dgr_t_pow43(const double *x, double *y, int n)
+{
+    for (int i = 0; i < n; ++i) y[i] = pow43(x[i]);
+}
+
 }  // extern "C"

@@ -45,6 +45,7 @@ def cores():
     lib = C.CDLL(LIB)
     d = C.c_double
     lib.dgr_t_set_flux.argtypes = [C.c_int]
+    lib.dgr_t_pow43.argtypes = [dp, dp, C.c_int]
     lib.dgr_t_roe.argtypes = [dp, d, d, d, d, dp, dp, dp, dp, dp]
     lib.dgr_t_edge.argtypes = [C.c_int] * 5 + [d, d, dp, d, d, d, dp, dp, dp, dp, dp]
     lib.dgr_t_element.argtypes = ([C.c_int, dp, dp, dp, d, d, d, d, d] + [dp] * 7 + [d, dp, dp, dp, dp, dp, dp, dp,
@@ -335,3 +336,13 @@ def test_hllc_inputs_cover_every_branch():
         x, nx, ny = _roe_inputs(rng)
         seen.add(_hllc_branch(x, nx, ny))
     assert seen == {0, 1, 2, 3}, seen
+
+
+def test_host_manning_power_is_correctly_rounded(cores):
+    """pow43 as the host compiles it against the 60-digit decimal values of the golden file;
+    the device's two-phase evaluation is checked against this one (test_gpu_parity)."""
+    g = np.load(os.path.join(HERE, "golden", "pow43_cr.npz"))
+    x = np.ascontiguousarray(g["x"])
+    y = np.empty_like(x)
+    cores.dgr_t_pow43(x, y, len(x))
+    assert np.array_equal(y, g["cr"])

@@ -262,3 +262,36 @@ def test_manning_power_correctly_rounded(dgrain):
     # glibc's pow (the reference's) agrees wherever glibc is correctly rounded
     agree = (y == g["glibc"]).mean()
     assert agree > 0.998, agree
+
+
+def test_manning_power_fast_phase_equals_exact(dgrain):
+    """The device evaluates x^(4./3) in two phases (a float-seeded fast value kept only when
+    its error interval rounds to one double, else the exact path); the host compiles the
+    exact path alone.  On 4 million seeded depths, both ends of the fast domain and the
+    rare fallback arguments included, the two agree bit for bit."""
+    import ctypes as C
+
+    from test_adjoint_cores import LIB as CORES_LIB, _build as build_cores
+
+    rng = np.random.default_rng(2024)
+    n = 1 << 20
+    x = np.concatenate([
+        np.exp(rng.uniform(np.log(1e-6), np.log(1e3), n)),          # depths of the runs
+        1e-3 + rng.uniform(-2e-5, 2e-5, n),                          # around the wet/dry film H0
+        np.exp(rng.uniform(-90.0, 90.0, n)),                         # across the fast domain's ends
+        rng.uniform(0.5, 20.0, n),
+        np.array([2.0 ** -120, np.nextafter(2.0 ** -120, 0), 2.0 ** 120, np.nextafter(2.0 ** 120, 0),
+                  1e-200, 1e200, 1.0, 8.0, 27.0, 0.125]),
+    ])
+    y = np.empty_like(x)
+    lib = dgrain.load()
+    assert lib.dgr_pow43_batch(x.ctypes.data_as(dgrain._lib.dptr), y.ctypes.data_as(dgrain._lib.dptr),
+                               len(x), 0) == 0
+    build_cores()
+    host = C.CDLL(CORES_LIB)
+    dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+    host.dgr_t_pow43.argtypes = [dp, dp, C.c_int]
+    want = np.empty_like(x)
+    host.dgr_t_pow43(x, want, len(x))
+    bad = np.flatnonzero(y != want)
+    assert bad.size == 0, (bad.size, x[bad[:5]], y[bad[:5]], want[bad[:5]])
