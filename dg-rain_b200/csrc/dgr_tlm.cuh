@@ -286,6 +286,7 @@ __global__ void __launch_bounds__(128) k_tlm_element(MeshDev m, const double *__
                                                      double *__restrict__ avg, double *__restrict__ avg_x,
                                                      const DevClock *clk, double g, const double *__restrict__ dt_n)
 {
+    l2_prefetch_slice(m.geo, m.ldE, NG, blockIdx.x * blockDim.x, min((int)blockDim.x, m.ne - (int)(blockIdx.x * blockDim.x)));
     const int el = blockIdx.x * blockDim.x + threadIdx.x;
     if (el >= m.ne) return;
     const T *tag = nullptr;
@@ -497,6 +498,7 @@ __global__ void __launch_bounds__(128, DGR_ADJ_MINB_ELEMENT) k_adj_element(MeshD
                                                      double *__restrict__ nbar, const double *__restrict__ n_el,
                                                      double g, const double *__restrict__ dt_n)
 {
+    l2_prefetch_slice(m.geo, m.ldE, NG, blockIdx.x * blockDim.x, min((int)blockDim.x, m.ne - (int)(blockIdx.x * blockDim.x)));
     const int el = blockIdx.x * blockDim.x + threadIdx.x;
     if (el >= m.ne) return;
     const int ld = m.ldE, lb = m.ldN;
