@@ -983,3 +983,93 @@ int orc_run_rk(orc_ctx *c, int nsteps, double final_time, double cfl, double dt0
     *steps_done = done;
     return rc;
 }
+
+/* ------------------------------------------------------------ channel coupling ---- */
+
+/* Junction side of one coupled edge e as ChanNet/internal_BC.c:33-95 forms it: the element
+ * EdgtoEls[2e], its local edge found by vertex matching (pairs (1,2), (2,3), (3,1) in that
+ * order), the edge length and outward normal from the element's vertices, and the mid-edge
+ * depth of the edge's own vertices. */
+static int orc_cpl_edge(const double *x, const double *y, const double *z, const int *el2v, const int *ed2v,
+                        const int *ed2el, int e, int *el_out, int *k_out, double *len, double *nx, double *ny,
+                        double *zmid)
+{
+    const int el = ed2el[2 * e];
+    const int a = el2v[3 * el], b = el2v[3 * el + 1], c = el2v[3 * el + 2];
+    const int p = ed2v[2 * e], q = ed2v[2 * e + 1];
+    const double xa = x[a], xb = x[b], xc = x[c], ya = y[a], yb = y[b], yc = y[c];
+    double x0, x1, y0, y1, l;
+    int k;
+    if ((a == p && b == q) || (a == q && b == p)) {
+        k = 0;
+        x0 = xa; x1 = xb; y0 = ya; y1 = yb;
+        l = sqrt((xa - xb) * (xa - xb) + (ya - yb) * (ya - yb));
+    } else if ((b == p && c == q) || (b == q && c == p)) {
+        k = 1;
+        x0 = xb; x1 = xc; y0 = yb; y1 = yc;
+        l = sqrt((xb - xc) * (xb - xc) + (yb - yc) * (yb - yc));
+    } else if ((c == p && a == q) || (c == q && a == p)) {
+        k = 2;
+        x0 = xc; x1 = xa; y0 = yc; y1 = ya;
+        l = sqrt((xa - xc) * (xa - xc) + (ya - yc) * (ya - yc));
+    } else {
+        return -1;
+    }
+    const double jac = (xb - xa) * (yc - ya) - (xc - xa) * (yb - ya);
+    const int s = (jac < 0) ? -1 : (jac == 0 ? 0 : 1); /* sign() of ChanNet/mathfunctions.c:17-25 */
+    *el_out = el;
+    *k_out = k;
+    *len = l;
+    *nx = s * (y1 - y0) / l;
+    *ny = s * (x0 - x1) / l;
+    *zmid = 0.5 * (z[p] + z[q]);
+    return 0;
+}
+
+int orc_internal_bc(int ne, int nf, const double *x, const double *y, const double *z, const int *el2v,
+                    const int *ed2v, const int *ed2el, const double *zeta, const double *qx, const double *qy,
+                    double *bzeta, double *bqn, int nchan, const int *in_ptr, const int *in_edges,
+                    const int *out_ptr, const int *out_edges, const int *chan_nodes, const int *chan_off,
+                    double *A, double *Q)
+{
+    (void)ne;
+    for (int ch = 0; ch < nchan; ++ch) {
+        double *Ac = A + 2 * (size_t)chan_off[ch], *Qc = Q + 2 * (size_t)chan_off[ch];
+        const int nn = chan_nodes[ch];
+        for (int side = 0; side < 2; ++side) { /* inflow list (:23-114), then outflow (:116-196) */
+            const int *ptr = side ? out_ptr : in_ptr;
+            const int *edges = side ? out_edges : in_edges;
+            const int n = ptr[ch + 1] - ptr[ch];
+            const int node_val = side ? 2 * nn - 2 : 1; /* the channel's own trace at the junction */
+            double area = 0, qn_sum = 0;
+            for (int j = ptr[ch]; j < ptr[ch + 1]; ++j) {
+                const int e = edges[j];
+                if (e < 0 || e >= nf) return -1;
+                int el, k;
+                double len, nx, ny, zmid;
+                if (orc_cpl_edge(x, y, z, el2v, ed2v, ed2el, e, &el, &k, &len, &nx, &ny, &zmid)) return -1;
+                const double h = zeta[3 * el + k] + zmid;
+                const double qn = qx[3 * el + k] * nx + qy[3 * el + k] * ny;
+                if (side) {
+                    area += h * len;
+                } else {
+                    area += len * h;
+                }
+                qn_sum += qn * len;
+                const double Hc = Ac[node_val] / (n * len);
+                bzeta[e] = Hc - zmid;
+                bqn[e] = side ? -Qc[node_val] / (n * len) : Qc[node_val] / (n * len);
+            }
+            if (n != 0) {
+                if (side) {
+                    Qc[2 * nn - 1] = -qn_sum;
+                    Ac[2 * nn - 1] = area;
+                } else {
+                    Qc[0] = qn_sum;
+                    Ac[0] = area;
+                }
+            }
+        }
+    }
+    return 0;
+}

@@ -100,6 +100,18 @@ int orc_run(orc_ctx *c, int nsteps, double final_time, double cfl, double dt0, i
             double rain, int tide_on, double amp, double period, double *time_io, double *dt_io,
             double *dt_hist, int *steps_done);
 
+/* Channel <-> junction coupling of ChanNet/internal_BC.c:17-196 on one junction mesh
+ * (reference arrays: el2v [3*ne], ed2v / ed2el [2*nf], state [3*el+k]).  Channel ch has
+ * chan_nodes[ch] nodes and its A, Q traces at [2*chan_off[ch], 2*chan_off[ch] + 2*nodes);
+ * its inflow-end edges are in_edges[in_ptr[ch] .. in_ptr[ch+1]), its outflow-end edges
+ * out_edges[out_ptr[ch] ..].  Writes bzeta / bqn of those edges and the channels' ghost
+ * traces A/Q[0] (inflow) and A/Q[2*nodes-1] (outflow).  -1 on a bad edge. */
+int orc_internal_bc(int ne, int nf, const double *x, const double *y, const double *z, const int *el2v,
+                    const int *ed2v, const int *ed2el, const double *zeta, const double *qx, const double *qy,
+                    double *bzeta, double *bqn, int nchan, const int *in_ptr, const int *in_edges,
+                    const int *out_ptr, const int *out_edges, const int *chan_nodes, const int *chan_off,
+                    double *A, double *Q);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,7 +3,8 @@
 ctypes bindings of
   * oracle/_build/liboracle.so  — the C restatement (dgr_oracle.c), and
   * oracle/_ref/libref2d.so / libref2d_wd.so — the unmodified reference 2DCode built by
-    oracle/Makefile (present only where the reference tree was available at build time).
+    oracle/Makefile (present only where the reference tree was available at build time),
+  * oracle/_ref/librefchan.so — the unmodified ChanNet/internal_BC.c (channel coupling).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module.
 """
@@ -20,6 +21,7 @@ ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref2d.so")
 REF_LIB_WD = os.path.join(HERE, "_ref", "libref2d_wd.so")
 REF_LIB_WD_O3 = os.path.join(HERE, "_ref", "libref2d_wd_o3.so")  # -O3 -march=x86-64-v3, timing only
+REF_CHAN_LIB = os.path.join(HERE, "_ref", "librefchan.so")
 
 dptr = C.POINTER(C.c_double)
 iptr = C.POINTER(C.c_int)
@@ -83,8 +85,59 @@ def _oracle_lib():
         lib.orc_run.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
                                 C.c_int, C.c_double, C.c_double, dptr, dptr, dptr, iptr]
         lib.orc_run_rk.argtypes = lib.orc_run.argtypes + [C.c_int]
+        lib.orc_internal_bc.argtypes = _INTERNAL_BC_ARGS
         _olib = lib
     return _olib
+
+
+_INTERNAL_BC_ARGS = ([C.c_int, C.c_int, dptr, dptr, dptr, iptr, iptr, iptr, dptr, dptr, dptr, dptr, dptr, C.c_int]
+                     + [iptr] * 6 + [dptr, dptr])
+_clib = None
+
+
+def have_reference_coupling() -> bool:
+    return os.path.exists(REF_CHAN_LIB)
+
+
+def internal_bc(mesh, zeta, qx, qy, bzeta, bqn, channels, reference=False):
+    """ChanNet/internal_BC.c on one junction mesh, by the restatement (dgr_oracle.c) or by the
+    reference build.  zeta/qx/qy: reference layout [3*el+k]; bzeta/bqn [nf] (copied);
+    channels: list of (A, Q, inflow_edges, outflow_edges), A and Q the channel's traces
+    (2 per node, copied).  Returns (bzeta, bqn, [(A, Q)...]) after the coupling pass."""
+    global _clib
+    if reference:
+        if _clib is None:
+            _clib = C.CDLL(REF_CHAN_LIB, mode=os.RTLD_LOCAL)
+            _clib.ref_internal_bc.argtypes = _INTERNAL_BC_ARGS
+            _clib.ref_internal_bc.restype = C.c_int
+        fn = _clib.ref_internal_bc
+    else:
+        fn = _oracle_lib().orc_internal_bc
+        fn.restype = C.c_int
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)  # noqa: E731
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+    nodes = i32([len(c[0]) // 2 for c in channels])
+    off = i32(np.concatenate([[0], np.cumsum(nodes)[:-1]]) if len(channels) else [0])
+    A = f64(np.concatenate([c[0] for c in channels]) if channels else [0.0])
+    Q = f64(np.concatenate([c[1] for c in channels]) if channels else [0.0])
+    in_ptr = i32(np.concatenate([[0], np.cumsum([len(c[2]) for c in channels])]))
+    out_ptr = i32(np.concatenate([[0], np.cumsum([len(c[3]) for c in channels])]))
+    in_e = i32(np.concatenate([np.asarray(c[2], dtype=np.int32) for c in channels] + [np.zeros(1, np.int32)]))
+    out_e = i32(np.concatenate([np.asarray(c[3], dtype=np.int32) for c in channels] + [np.zeros(1, np.int32)]))
+    bz, bq = f64(bzeta).copy(), f64(bqn).copy()
+    zt, qxx, qyy = f64(zeta), f64(qx), f64(qy)
+    x, y, z = f64(mesh.x), f64(mesh.y), f64(mesh.z)
+    el2v, ed2v, ed2el = i32(mesh.el2v.ravel()), i32(mesh.ed2v.ravel()), i32(mesh.ed2el.ravel())
+    rc = fn(mesh.num_el, mesh.num_edges, _d(x), _d(y), _d(z), _i(el2v), _i(ed2v), _i(ed2el), _d(zt), _d(qxx),
+            _d(qyy), _d(bz), _d(bq), len(channels), _i(in_ptr), _i(in_e), _i(out_ptr), _i(out_e), _i(nodes),
+            _i(off), _d(A), _d(Q))
+    if rc != 0:
+        raise ValueError("internal_bc: bad coupled edge")
+    out, o = [], 0
+    for n in nodes:
+        out.append((A[2 * o:2 * (o + n)].copy(), Q[2 * o:2 * (o + n)].copy()))
+        o += n
+    return bz, bq, out
 
 
 class Oracle:
