@@ -517,6 +517,39 @@ def io_bench(m, solver, outdir: str):
             "dat_bytes": nbytes, "dat_identical": bool(same_dat)}
 
 
+def coupling_bench(m, solver, repeats: int = 200):
+    """Channel <-> junction coupling (ChanNet internal_BC) on the bench mesh: its x = 0
+    edges (prescribed, elevation-specified) as channel inflow ends of 4 consecutive edges
+    each; one coupling pass through dgr_couple_channel_ends (host arrays, copies and the
+    synchronisation included) against the unmodified reference internal_BC on the same
+    inputs (one host core), identical ghosts required."""
+    from oracle import oracle as orc
+
+    e = np.flatnonzero((m.ed2el[:, 0] == m.ed2el[:, 1]) & (m.bdry == 2))
+    e = e[np.argsort(m.y[m.ed2v[e, 0]] + m.y[m.ed2v[e, 1]], kind="stable")]
+    per = 4
+    groups = [e[i * per:(i + 1) * per].astype(np.int32) for i in range(len(e) // per)]
+    rng = np.random.default_rng(5)
+    a_end = rng.uniform(5.0, 50.0, len(groups))
+    q_end = rng.normal(0.0, 5.0, len(groups))
+    solver.set_channel_ends([(g, 0) for g in groups])
+    solver.couple_channel_ends(a_end, q_end)
+    t0 = time.perf_counter()
+    for _ in range(repeats):
+        ag, qg = solver.couple_channel_ends(a_end, q_end)
+    dev_s = (time.perf_counter() - t0) / repeats
+    z, x, y, _ = solver.download_state()
+    bz, bq = solver.get_boundary()
+    solver.set_channel_ends([])
+    chans = [(np.array([0.0, a, 0.0, 0.0]), np.array([0.0, q, 0.0, 0.0]), g, np.zeros(0, np.int32))
+             for a, q, g in zip(a_end, q_end, groups)]
+    ref = orc.have_reference_coupling()
+    _, _, outs, ref_s = orc.internal_bc(m, z, x, y, bz, bq, chans, reference=ref, repeats=repeats)
+    same = all(ag[i] == outs[i][0][0] and qg[i] == outs[i][1][0] for i in range(len(groups)))
+    return {"channel_ends": len(groups), "coupled_edges": per * len(groups), "device_pass_us": dev_s * 1e6,
+            "host_pass_us": ref_s * 1e6, "host_kind": "reference" if ref else "port", "identical": bool(same)}
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -561,6 +594,7 @@ def main():
     ap.add_argument("--calib-iterations", type=int, default=0)
     ap.add_argument("--no-calibration", action="store_true")
     ap.add_argument("--io", action="store_true", help="add the mesh-ingest and .dat-writer comparison")
+    ap.add_argument("--coupling", action="store_true", help="add the channel-junction coupling pass comparison")
     args = ap.parse_args()
     if args.e2e_steps < 0:
         args.e2e_steps = args.steps
@@ -690,6 +724,10 @@ def main():
         with tempfile.TemporaryDirectory() as tmp:
             io = io_bench(m, solver, tmp)
 
+    cpl = None
+    if args.coupling and rank == 0:
+        cpl = coupling_bench(m, solver)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_reference(m, st)
@@ -734,6 +772,7 @@ def main():
             "adjoint": adj,
             "calibration": cal,
             "io": io,
+            "coupling": cpl,
         }
         print(json.dumps(line), flush=True)
     solver.close()

@@ -83,6 +83,7 @@ static void release(dgr_ctx *c)
     for (void *q : ptrs)
         if (q) cudaFree(q);
     adjoint_release(c);
+    coupling_release(c);
     if (c->h_clk) cudaFreeHost(c->h_clk);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->ev0) cudaEventDestroy(c->ev0);

@@ -94,6 +94,11 @@ struct dgr_ctx {
     int gauge_n, gauge_cap;
     int *gauge_el, *gauge_sid;
     double *gauge_w, *gauge_series; /* weights [n][nm], series [cap][n] */
+    /* channel ends coupled to prescribed boundary edges (dgr_set_channel_ends) */
+    int cpl_nends, cpl_nedges;
+    int *cpl_ptr, *cpl_out, *cpl_edge, *cpl_slot; /* [nends + 1], [nends], [nedges], [nedges] */
+    double *cpl_geo;                              /* [4][nedges]: length, nx, ny, mid-edge depth */
+    double *cpl_io, *h_cpl_io;                    /* [4][nends] in/out, and its pinned mirror */
 };
 
 static inline dgr::MeshDev mesh_dev(const dgr_ctx *c)
@@ -178,3 +183,4 @@ int first_error(const dgr_ctx *c);               /* first scenario failure code 
 
 /* dgr_adjoint.cu */
 void adjoint_release(dgr_ctx *c);
+void coupling_release(dgr_ctx *c);

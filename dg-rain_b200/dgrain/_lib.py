@@ -138,6 +138,9 @@ SIGNATURES = [
     ("dgr_last_device_ms", C.c_double, [C.c_void_p]),
     ("dgr_profile_step", C.c_int, [C.c_void_p, C.c_int, dptr, C.c_int]),
     ("dgr_pow43_batch", C.c_int, [dptr, dptr, C.c_int, C.c_int]),
+    ("dgr_set_channel_ends", C.c_int, [C.c_void_p, C.c_int, iptr, iptr, iptr]),
+    ("dgr_couple_channel_ends", C.c_int, [C.c_void_p, dptr, dptr, dptr, dptr]),
+    ("dgr_get_boundary", C.c_int, [C.c_void_p, dptr, dptr]),
     ("dgr_ensemble_create", C.c_int, [C.c_int, C.POINTER(DgrMeshView), C.POINTER(DgrScenarioParams),
                                       C.POINTER(DgrParams), C.POINTER(C.c_void_p)]),
     ("dgr_ensemble_size", C.c_int, [C.c_void_p]),

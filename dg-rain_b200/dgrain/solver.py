@@ -136,6 +136,37 @@ class Solver:
     def boundary_conditions(self, time: float = 0.0) -> None:
         _lib.check(self.lib.dgr_boundary_conditions(self.ctx, time), "dgr_boundary_conditions")
 
+    def get_boundary(self):
+        """(bzeta, bQn) of every edge as the device holds them"""
+        bz, bq = np.empty(self.nf), np.empty(self.nf)
+        _lib.check(self.lib.dgr_get_boundary(self.ctx, _dp(bz), _dp(bq)), "dgr_get_boundary")
+        return bz, bq
+
+    # ----------------------------------------------------- channel coupling ----
+    def set_channel_ends(self, ends) -> None:
+        """ends: list of (edges, outflow) — the mesh edges a channel end is attached to, in
+        the order of the reference's junction-edge list, and whether it is the channel's
+        last node (outflow, 1) or its first (inflow, 0); see dgr_set_channel_ends"""
+        ptr = np.concatenate([[0], np.cumsum([len(e) for e, _ in ends])]).astype(np.int32)
+        edges = np.ascontiguousarray(np.concatenate([np.asarray(e, dtype=np.int32) for e, _ in ends]
+                                                    + [np.zeros(0, np.int32)]), dtype=np.int32)
+        out = np.ascontiguousarray([int(o) for _, o in ends], dtype=np.int32)
+        rc = self.lib.dgr_set_channel_ends(self.ctx, len(ends), _ip(ptr), _ip(edges if edges.size else ptr),
+                                           _ip(out if out.size else ptr))
+        _lib.check(rc, "dgr_set_channel_ends")
+        self._nends = len(ends)
+
+    def couple_channel_ends(self, a_end, q_end):
+        """one coupling pass (internal_BC): returns the ends' ghost (A, Q)"""
+        n = getattr(self, "_nends", 0)
+        a = np.ascontiguousarray(a_end, dtype=np.float64).reshape(n)
+        q = np.ascontiguousarray(q_end, dtype=np.float64).reshape(n)
+        ag, qg = np.empty(n), np.empty(n)
+        if n:
+            _lib.check(self.lib.dgr_couple_channel_ends(self.ctx, _dp(a), _dp(q), _dp(ag), _dp(qg)),
+                       "dgr_couple_channel_ends")
+        return ag, qg
+
     # ------------------------------------------------------------- operators ----
     def _status(self, rc: int, where: str) -> None:
         if rc == _lib.DGR_OK:

@@ -374,6 +374,37 @@ DGR_API int dgr_set_bathymetry(dgr_ctx *ctx, const double *z);
  *   [220..233]  reference coordinates (r, s) of the 7 area points [7][2]. */
 DGR_API int dgr_p2_reference(double *tables, int n);
 
+/* ---- channel <-> junction coupling (ChanNet/internal_BC.c:17-218) ----------------
+ * This context's mesh is a ChanNet junction; 1D channels attach to its prescribed boundary
+ * edges.  A channel END is the first node of a channel (the reference's
+ * InflowJunctionEdges list, end_outflow = 0) or its last node (OutflowJunctionEdges,
+ * end_outflow = 1); end k owns the mesh edges end_edges[end_ptr[k] .. end_ptr[k+1]) in the
+ * order of the reference's list.  Each edge must be a prescribed boundary edge
+ * (BdryPrescribed != 0) and belong to one end; each end has at least one edge.  One
+ * context (not an ensemble), order 1.  Replaces the channel lists of
+ * ChanNet/ChannelsAndJunctions.h:47-66 (struct channel) for the junction's side. */
+DGR_API int dgr_set_channel_ends(dgr_ctx *ctx, int nends, const int *end_ptr, const int *end_edges,
+                                 const int *end_outflow);
+
+/* One coupling pass, internal_BC() for this junction (host arrays of nends):
+ *   in:  a_end[k], q_end[k]: the channel's own trace A, Q at the junction node (the
+ *        reference's A[1], Q[1] for an inflow end; A[2N-2], Q[2N-2] for an outflow end);
+ *   out: the ends' edges get bzeta = a_end / (n len) - z_mid and bQn = +-q_end / (n len)
+ *        on the device (read by the next dgr_step, as the reference's junction step reads
+ *        junc->bzeta / bQn), and a_ghost[k], q_ghost[k] = the junction's sums over the
+ *        end's edges of len * (zeta + z_mid) and +-len * (Qx nx + Qy ny) from the current
+ *        state (the reference's A[0], Q[0] or A[2N-1], Q[2N-1]).
+ * The reference's loop calls it after the channels' step and again after the junction's
+ * (ChanNet/time_evolution.c:552-578).  Results are those of internal_BC bit for bit.
+ * A coupled junction is stepped with dgr_step: the device clock of dgr_run rewrites every
+ * prescribed edge's values each step from its boundary type (boundary_conditions()). */
+DGR_API int dgr_couple_channel_ends(dgr_ctx *ctx, const double *a_end, const double *q_end, double *a_ghost,
+                                    double *q_ghost);
+
+/* The device's prescribed boundary values bzeta[e], bQn[e] for every edge (reference edge
+ * numbering; only prescribed edges are meaningful). */
+DGR_API int dgr_get_boundary(dgr_ctx *ctx, double *bzeta, double *bQn);
+
 /* Diagnostic: y[i] = x[i]^(4./3) as the kernels evaluate the Manning term of
  * 2DCode/2DInnerProducts.c:318 (correctly rounded; see dgr_device.cuh). */
 DGR_API int dgr_pow43_batch(const double *x, double *y, int n, int device);

@@ -1036,7 +1036,7 @@ int orc_internal_bc(int ne, int nf, const double *x, const double *y, const doub
     for (int ch = 0; ch < nchan; ++ch) {
         double *Ac = A + 2 * (size_t)chan_off[ch], *Qc = Q + 2 * (size_t)chan_off[ch];
         const int nn = chan_nodes[ch];
-        for (int side = 0; side < 2; ++side) { /* inflow list (:23-114), then outflow (:116-196) */
+        for (int side = 0; side < 2; ++side) { /* inflow list (:23-115), then outflow (:117-216) */
             const int *ptr = side ? out_ptr : in_ptr;
             const int *edges = side ? out_edges : in_edges;
             const int n = ptr[ch + 1] - ptr[ch];

@@ -100,7 +100,7 @@ int orc_run(orc_ctx *c, int nsteps, double final_time, double cfl, double dt0, i
             double rain, int tide_on, double amp, double period, double *time_io, double *dt_io,
             double *dt_hist, int *steps_done);
 
-/* Channel <-> junction coupling of ChanNet/internal_BC.c:17-196 on one junction mesh
+/* Channel <-> junction coupling of ChanNet/internal_BC.c:17-218 on one junction mesh
  * (reference arrays: el2v [3*ne], ed2v / ed2el [2*nf], state [3*el+k]).  Channel ch has
  * chan_nodes[ch] nodes and its A, Q traces at [2*chan_off[ch], 2*chan_off[ch] + 2*nodes);
  * its inflow-end edges are in_edges[in_ptr[ch] .. in_ptr[ch+1]), its outflow-end edges

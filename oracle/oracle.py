@@ -99,11 +99,13 @@ def have_reference_coupling() -> bool:
     return os.path.exists(REF_CHAN_LIB)
 
 
-def internal_bc(mesh, zeta, qx, qy, bzeta, bqn, channels, reference=False):
+def internal_bc(mesh, zeta, qx, qy, bzeta, bqn, channels, reference=False, repeats=0):
     """ChanNet/internal_BC.c on one junction mesh, by the restatement (dgr_oracle.c) or by the
     reference build.  zeta/qx/qy: reference layout [3*el+k]; bzeta/bqn [nf] (copied);
     channels: list of (A, Q, inflow_edges, outflow_edges), A and Q the channel's traces
-    (2 per node, copied).  Returns (bzeta, bqn, [(A, Q)...]) after the coupling pass."""
+    (2 per node, copied).  Returns (bzeta, bqn, [(A, Q)...]) after the coupling pass; with
+    repeats > 0 the pass runs that many more times on the same inputs and the seconds per
+    pass of the C call alone come last."""
     global _clib
     if reference:
         if _clib is None:
@@ -128,15 +130,23 @@ def internal_bc(mesh, zeta, qx, qy, bzeta, bqn, channels, reference=False):
     zt, qxx, qyy = f64(zeta), f64(qx), f64(qy)
     x, y, z = f64(mesh.x), f64(mesh.y), f64(mesh.z)
     el2v, ed2v, ed2el = i32(mesh.el2v.ravel()), i32(mesh.ed2v.ravel()), i32(mesh.ed2el.ravel())
-    rc = fn(mesh.num_el, mesh.num_edges, _d(x), _d(y), _d(z), _i(el2v), _i(ed2v), _i(ed2el), _d(zt), _d(qxx),
+    args = (mesh.num_el, mesh.num_edges, _d(x), _d(y), _d(z), _i(el2v), _i(ed2v), _i(ed2el), _d(zt), _d(qxx),
             _d(qyy), _d(bz), _d(bq), len(channels), _i(in_ptr), _i(in_e), _i(out_ptr), _i(out_e), _i(nodes),
             _i(off), _d(A), _d(Q))
+    rc = fn(*args)
     if rc != 0:
         raise ValueError("internal_bc: bad coupled edge")
     out, o = [], 0
     for n in nodes:
         out.append((A[2 * o:2 * (o + n)].copy(), Q[2 * o:2 * (o + n)].copy()))
         o += n
+    if repeats > 0:
+        import time
+
+        t0 = time.perf_counter()
+        for _ in range(repeats):
+            fn(*args)
+        return bz, bq, out, (time.perf_counter() - t0) / repeats
     return bz, bq, out
 
 
