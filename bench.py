@@ -521,8 +521,10 @@ def coupling_bench(m, solver, repeats: int = 200):
     """Channel <-> junction coupling (ChanNet internal_BC) on the bench mesh: its x = 0
     edges (prescribed, elevation-specified) as channel inflow ends of 4 consecutive edges
     each; one coupling pass through dgr_couple_channel_ends (host arrays, copies and the
-    synchronisation included) against the unmodified reference internal_BC on the same
-    inputs (one host core), identical ghosts required."""
+    synchronisation included) and through dgr_couple_channel_ends_device (device buffers,
+    passes enqueued back to back, CUDA events on the context's stream), against the
+    unmodified reference internal_BC on the same inputs (one host core), identical ghosts
+    required."""
     from oracle import oracle as orc
 
     e = np.flatnonzero((m.ed2el[:, 0] == m.ed2el[:, 1]) & (m.bdry == 2))
@@ -538,6 +540,23 @@ def coupling_bench(m, solver, repeats: int = 200):
     for _ in range(repeats):
         ag, qg = solver.couple_channel_ends(a_end, q_end)
     dev_s = (time.perf_counter() - t0) / repeats
+    # the same pass on device buffers (channel states kept on the GPU), enqueued back to back
+    import torch
+
+    dv = torch.device("cuda", torch.cuda.current_device())
+    da, dq = torch.tensor(a_end, device=dv), torch.tensor(q_end, device=dv)
+    ga, gq = torch.empty_like(da), torch.empty_like(dq)
+    torch.cuda.synchronize()
+    st = torch.cuda.ExternalStream(solver.stream())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    solver.couple_channel_ends_device(da, dq, ga, gq)
+    ev0.record(st)
+    for _ in range(repeats):
+        solver.couple_channel_ends_device(da, dq, ga, gq)
+    ev1.record(st)
+    ev1.synchronize()
+    dev_buf_us = ev0.elapsed_time(ev1) * 1e3 / repeats
+    same_dev = bool(np.array_equal(ga.cpu().numpy(), ag) and np.array_equal(gq.cpu().numpy(), qg))
     z, x, y, _ = solver.download_state()
     bz, bq = solver.get_boundary()
     solver.set_channel_ends([])
@@ -547,7 +566,8 @@ def coupling_bench(m, solver, repeats: int = 200):
     _, _, outs, ref_s = orc.internal_bc(m, z, x, y, bz, bq, chans, reference=ref, repeats=repeats)
     same = all(ag[i] == outs[i][0][0] and qg[i] == outs[i][1][0] for i in range(len(groups)))
     return {"channel_ends": len(groups), "coupled_edges": per * len(groups), "device_pass_us": dev_s * 1e6,
-            "host_pass_us": ref_s * 1e6, "host_kind": "reference" if ref else "port", "identical": bool(same)}
+            "device_buffers_pass_us": dev_buf_us, "host_pass_us": ref_s * 1e6,
+            "host_kind": "reference" if ref else "port", "identical": bool(same and same_dev)}
 
 
 def run_reference_arm(args):

@@ -61,18 +61,19 @@ __global__ void __launch_bounds__(128) k_cpl_setup(int n, int ldE, const int *__
     geo[3 * n + j] = 0.5 * (z[p] + z[q]);
 }
 
-/* one coupling pass; io = [a_end | q_end | a_ghost | q_ghost], nends each */
+/* one coupling pass: the ends' traces in, their ghosts out (nends each) */
 __global__ void __launch_bounds__(128) k_cpl_pass(int nends, int nedges, int ldE, const int *__restrict__ ptr,
                                                   const int *__restrict__ outflow, const int *__restrict__ edges,
                                                   const int *__restrict__ slot, const double *__restrict__ geo,
                                                   const double *__restrict__ U, double *__restrict__ bzeta,
-                                                  double *__restrict__ bqn, double *__restrict__ io)
+                                                  double *__restrict__ bqn, const double *a_in, const double *q_in,
+                                                  double *a_ghost, double *q_ghost)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nends) return;
     const int out = outflow[c];
     const int j0 = ptr[c], j1 = ptr[c + 1], n = j1 - j0;
-    const double a_end = io[c], q_end = io[nends + c];
+    const double a_end = a_in[c], q_end = q_in[c];
     double area = 0, qn_sum = 0;
     for (int j = j0; j < j1; ++j) {
         const double len = geo[j], nx = geo[nedges + j], ny = geo[2 * nedges + j], zmid = geo[3 * nedges + j];
@@ -85,8 +86,8 @@ __global__ void __launch_bounds__(128) k_cpl_pass(int nends, int nedges, int ldE
         bzeta[e] = a_end / (n * len) - zmid;
         bqn[e] = out ? -q_end / (n * len) : q_end / (n * len);
     }
-    io[2 * nends + c] = area;
-    io[3 * nends + c] = out ? -qn_sum : qn_sum;
+    a_ghost[c] = area;
+    q_ghost[c] = out ? -qn_sum : qn_sum;
 }
 
 #define CPL_TRY(x)           \
@@ -170,8 +171,10 @@ extern "C" int dgr_couple_channel_ends(dgr_ctx *c, const double *a_end, const do
     std::copy(a_end, a_end + n, c->h_cpl_io);
     std::copy(q_end, q_end + n, c->h_cpl_io + n);
     CK(cudaMemcpyAsync(c->cpl_io, c->h_cpl_io, 2 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s));
+    double *io = c->cpl_io;
     k_cpl_pass<<<blocks(n, 128), 128, 0, s>>>(n, c->cpl_nedges, c->ldE, c->cpl_ptr, c->cpl_out, c->cpl_edge,
-                                              c->cpl_slot, c->cpl_geo, c->U, c->bzeta, c->bqn, c->cpl_io);
+                                              c->cpl_slot, c->cpl_geo, c->U, c->bzeta, c->bqn, io, io + n,
+                                              io + 2 * n, io + 3 * n);
     c->launches++;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->h_cpl_io + 2 * n, c->cpl_io + 2 * n, 2 * (size_t)n * sizeof(double),
@@ -179,6 +182,29 @@ extern "C" int dgr_couple_channel_ends(dgr_ctx *c, const double *a_end, const do
     CK(cudaStreamSynchronize(s));
     std::copy(c->h_cpl_io + 2 * n, c->h_cpl_io + 3 * n, a_ghost);
     std::copy(c->h_cpl_io + 3 * n, c->h_cpl_io + 4 * n, q_ghost);
+    return DGR_OK;
+}
+
+extern "C" int dgr_couple_channel_ends_device(dgr_ctx *c, const double *d_a_end, const double *d_q_end,
+                                              double *d_a_ghost, double *d_q_ghost)
+{
+    if (!c || c->nscen != 1) return DGR_ERR_INVALID;
+    const int n = c->cpl_nends;
+    if (n == 0) return DGR_OK;
+    if (!d_a_end || !d_q_end || !d_a_ghost || !d_q_ghost) return DGR_ERR_INVALID;
+    CK(cudaSetDevice(c->device));
+    k_cpl_pass<<<blocks(n, 128), 128, 0, c->stream>>>(n, c->cpl_nedges, c->ldE, c->cpl_ptr, c->cpl_out,
+                                                      c->cpl_edge, c->cpl_slot, c->cpl_geo, c->U, c->bzeta, c->bqn,
+                                                      d_a_end, d_q_end, d_a_ghost, d_q_ghost);
+    c->launches++;
+    CK(cudaGetLastError());
+    return DGR_OK;
+}
+
+extern "C" int dgr_get_stream(dgr_ctx *c, void **stream)
+{
+    if (!c || !stream) return DGR_ERR_INVALID;
+    *stream = (void *)c->stream;
     return DGR_OK;
 }
 

@@ -141,6 +141,8 @@ SIGNATURES = [
     ("dgr_set_channel_ends", C.c_int, [C.c_void_p, C.c_int, iptr, iptr, iptr]),
     ("dgr_couple_channel_ends", C.c_int, [C.c_void_p, dptr, dptr, dptr, dptr]),
     ("dgr_get_boundary", C.c_int, [C.c_void_p, dptr, dptr]),
+    ("dgr_couple_channel_ends_device", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("dgr_get_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     ("dgr_ensemble_create", C.c_int, [C.c_int, C.POINTER(DgrMeshView), C.POINTER(DgrScenarioParams),
                                       C.POINTER(DgrParams), C.POINTER(C.c_void_p)]),
     ("dgr_ensemble_size", C.c_int, [C.c_void_p]),

@@ -156,6 +156,19 @@ class Solver:
         _lib.check(rc, "dgr_set_channel_ends")
         self._nends = len(ends)
 
+    def stream(self) -> int:
+        """the context's cudaStream_t as an integer (torch.cuda.ExternalStream accepts it)"""
+        s = C.c_void_p()
+        _lib.check(self.lib.dgr_get_stream(self.ctx, C.byref(s)), "dgr_get_stream")
+        return int(s.value or 0)
+
+    def couple_channel_ends_device(self, a_end, q_end, a_ghost, q_ghost) -> None:
+        """the coupling pass on device buffers (torch CUDA float64 tensors of the ends'
+        count, or raw device addresses), enqueued on the solver's stream"""
+        ptr = [int(t.data_ptr()) if hasattr(t, "data_ptr") else int(t) for t in (a_end, q_end, a_ghost, q_ghost)]
+        _lib.check(self.lib.dgr_couple_channel_ends_device(self.ctx, *[C.c_void_p(p) for p in ptr]),
+                   "dgr_couple_channel_ends_device")
+
     def couple_channel_ends(self, a_end, q_end):
         """one coupling pass (internal_BC): returns the ends' ghost (A, Q)"""
         n = getattr(self, "_nends", 0)

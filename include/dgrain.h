@@ -401,6 +401,16 @@ DGR_API int dgr_set_channel_ends(dgr_ctx *ctx, int nends, const int *end_ptr, co
 DGR_API int dgr_couple_channel_ends(dgr_ctx *ctx, const double *a_end, const double *q_end, double *a_ghost,
                                     double *q_ghost);
 
+/* The same pass with the ends' traces and ghosts in DEVICE arrays (nends doubles each),
+ * enqueued on the context's stream without synchronising: for channel states that stay on
+ * the GPU.  The caller orders its own work on those arrays with that stream. */
+DGR_API int dgr_couple_channel_ends_device(dgr_ctx *ctx, const double *d_a_end, const double *d_q_end,
+                                           double *d_a_ghost, double *d_q_ghost);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own device
+ * work against the context's (e.g. around dgr_couple_channel_ends_device). */
+DGR_API int dgr_get_stream(dgr_ctx *ctx, void **stream);
+
 /* The device's prescribed boundary values bzeta[e], bQn[e] for every edge (reference edge
  * numbering; only prescribed edges are meaningful). */
 DGR_API int dgr_get_boundary(dgr_ctx *ctx, double *bzeta, double *bQn);

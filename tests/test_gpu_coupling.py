@@ -138,3 +138,31 @@ def test_channel_end_lists_are_checked(dgrain):
         s.set_channel_ends(ends)
         s.set_channel_ends([])      # removes the coupling
         assert s.couple_channel_ends(np.zeros(0), np.zeros(0))[0].size == 0
+
+
+def test_device_buffer_pass_equals_host_pass(dgrain):
+    """dgr_couple_channel_ends_device on torch CUDA buffers, ordered through the context's
+    stream, gives the host-array pass's ghosts and boundary values bit for bit."""
+    import torch
+
+    m0, (zeta, qx, qy), bz, bq, chans = coupling_case(dgrain, seed=5, nchan=5)
+    m = prescribed(dgrain, m0, chans)
+    ends, where = ends_of(chans)
+    a_end = np.array([chans[ch][0][i] for ch, i, _ in where])
+    q_end = np.array([chans[ch][1][i] for ch, i, _ in where])
+    with dgrain.Solver(m, wet_dry=1) as s:
+        s.upload_state(zeta, qx, qy)
+        s.set_boundary(bz, bq)
+        s.set_channel_ends(ends)
+        ag, qg = s.couple_channel_ends(a_end, q_end)
+        hb = s.get_boundary()
+        s.set_boundary(bz, bq)
+        dev = torch.device("cuda", 0)
+        da, dq = torch.tensor(a_end, device=dev), torch.tensor(q_end, device=dev)
+        dga, dgq = torch.empty_like(da), torch.empty_like(dq)
+        torch.cuda.synchronize()
+        s.couple_channel_ends_device(da, dq, dga, dgq)
+        torch.cuda.ExternalStream(s.stream()).synchronize()
+        db = s.get_boundary()
+    assert np.array_equal(dga.cpu().numpy(), ag) and np.array_equal(dgq.cpu().numpy(), qg)
+    assert np.array_equal(db[0], hb[0]) and np.array_equal(db[1], hb[1])
