@@ -291,9 +291,12 @@ DGR_HD double pow43_exact(double x)
  *   pow43_exact, whose error is a few 2^-100, decides.  The host keeps pow43_exact.
  */
 #ifdef __CUDA_ARCH__
+/* the rare slow phase stays out of line: one copy per kernel instead of one per call site */
+__device__ __noinline__ double pow43_slow(double x) { return pow43_exact(x); }
+
 DGR_DEV double pow43_fast_or_exact(double x)
 {
-    if (!(x >= 0x1p-120 && x < 0x1p120)) return pow43_exact(x);
+    if (!(x >= 0x1p-120 && x < 0x1p120)) return pow43_slow(x);
     const double r0 = (double)rcbrtf(__double2float_rn(x));
     const double q = r0 * r0; /* exact: 24-bit significands */
     const double t = __fma_rn(-x, q * r0, 1.0);
@@ -318,7 +321,7 @@ DGR_DEV double pow43_fast_or_exact(double x)
     const double y_lo = p_h + (lo - err);
     const double y_hi = p_h + (lo + err);
     if (y_lo == y_hi) return y_lo;
-    return pow43_exact(x);
+    return pow43_slow(x);
 }
 #endif
 

@@ -144,8 +144,10 @@ DGR_HD void p2_element_core(const P2Ref &ref, const T S[3][P2_NM], const T F[3][
 #pragma unroll
         for (int m = 0; m < P2_NM; ++m) acc[v][m] = 0.0;
 
-    /* area integrals */
-#pragma unroll
+    /* area integrals; the point loop stays a loop (its mode and variable indices are still
+     * compile-time): unrolled, seven copies of its body overflow the instruction cache
+     * (measured: 8 % off the p = 2 step rolled) */
+#pragma unroll 1
     for (int q = 0; q < P2_NQ; ++q) {
         T uq[3];
 #pragma unroll

@@ -154,7 +154,8 @@ DGR_HD void p2_area_rev(const P2Ref &ref, const double S[3][P2_NM], const double
                         double sx, double sy, double detJ, const double zv[3], double dzx, double dzy, double gnn,
                         double g, double Sb[3][P2_NM], double zvb[3], double dzb[2], double &gnnb)
 {
-#pragma unroll
+    /* a loop, as the forward's area loop (instruction cache) */
+#pragma unroll 1
     for (int q = 0; q < P2_NQ; ++q) {
         double uq[3];
 #pragma unroll
