@@ -90,3 +90,23 @@ def test_internal_bc_lake_at_rest(dgrain):
             assert Q2[0] == 0.0 and A2[0] > 0
         if len(e_out):
             assert Q2[-1] == 0.0 and A2[-1] > 0
+
+
+def test_internal_bc_restatement_matches_golden(dgrain):
+    """The restatement against the reference internal_BC's own outputs committed in
+    tests/golden/coupling_internal_bc.npz (tests/golden/make_coupling_golden.py), so the
+    pin holds where oracle/_ref was not built."""
+    from conftest import load_golden, mesh_from_golden
+
+    g = load_golden("coupling_internal_bc.npz")
+    m = mesh_from_golden(dgrain, g)
+    chans, off = [], 0
+    for k, n in enumerate(g["nodes"]):
+        chans.append((g["A"][2 * off:2 * (off + n)], g["Q"][2 * off:2 * (off + n)],
+                      g["in_edges"][g["in_ptr"][k]:g["in_ptr"][k + 1]],
+                      g["out_edges"][g["out_ptr"][k]:g["out_ptr"][k + 1]]))
+        off += n
+    bz, bq, out = oracle.internal_bc(m, g["zeta"], g["qx"], g["qy"], g["bz"], g["bq"], chans)
+    assert np.array_equal(bz, g["bz_out"]) and np.array_equal(bq, g["bq_out"])
+    assert np.array_equal(np.concatenate([o[0] for o in out]), g["A_out"])
+    assert np.array_equal(np.concatenate([o[1] for o in out]), g["Q_out"])
