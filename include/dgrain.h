@@ -403,7 +403,9 @@ DGR_API int dgr_couple_channel_ends(dgr_ctx *ctx, const double *a_end, const dou
 
 /* The same pass with the ends' traces and ghosts in DEVICE arrays (nends doubles each),
  * enqueued on the context's stream without synchronising: for channel states that stay on
- * the GPU.  The caller orders its own work on those arrays with that stream. */
+ * the GPU.  The caller orders its own work on those arrays with that stream.  Device,
+ * managed and pinned host memory are accepted; pageable host memory is refused
+ * (DGR_ERR_INVALID) before anything is launched. */
 DGR_API int dgr_couple_channel_ends_device(dgr_ctx *ctx, const double *d_a_end, const double *d_q_end,
                                            double *d_a_ghost, double *d_q_ghost);
 

@@ -166,3 +166,25 @@ def test_device_buffer_pass_equals_host_pass(dgrain):
         db = s.get_boundary()
     assert np.array_equal(dga.cpu().numpy(), ag) and np.array_equal(dgq.cpu().numpy(), qg)
     assert np.array_equal(db[0], hb[0]) and np.array_equal(db[1], hb[1])
+
+
+def test_device_buffer_pass_accepts_pinned_host_memory(dgrain):
+    """Pinned host buffers are addressable by the kernel (unified addressing), so the
+    device-buffer pass takes them and gives the host pass's ghosts."""
+    import torch
+
+    m0, (zeta, qx, qy), bz, bq, chans = coupling_case(dgrain, seed=6, nchan=4)
+    m = prescribed(dgrain, m0, chans)
+    ends, where = ends_of(chans)
+    a_end = np.array([chans[ch][0][i] for ch, i, _ in where])
+    q_end = np.array([chans[ch][1][i] for ch, i, _ in where])
+    with dgrain.Solver(m, wet_dry=1) as s:
+        s.upload_state(zeta, qx, qy)
+        s.set_channel_ends(ends)
+        ag, qg = s.couple_channel_ends(a_end, q_end)
+        pa = torch.tensor(a_end).pin_memory()
+        pq = torch.tensor(q_end).pin_memory()
+        ga, gq = torch.empty_like(pa).pin_memory(), torch.empty_like(pq).pin_memory()
+        s.couple_channel_ends_device(pa, pq, ga, gq)
+        torch.cuda.ExternalStream(s.stream()).synchronize()
+    assert np.array_equal(ga.numpy(), ag) and np.array_equal(gq.numpy(), qg)
