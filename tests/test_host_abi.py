@@ -90,3 +90,18 @@ def test_device_calls_fail_loudly_without_gpu(dgrain):
     assert ei.value.code == dgrain._lib.DGR_ERR_NO_DEVICE
     p = dgrain.default_params()
     assert p.g == 9.81 and p.H0 == 1e-3 and p.VELZERO == 1e-2 and p.cfl == 0.1 and p.dt0 == 1e-7
+
+
+def test_coupling_entry_points_check_their_arguments(dgrain):
+    """The coupling entry points refuse a missing context or missing arrays before any
+    device work (no GPU needed)."""
+    lib = dgrain.load()
+    inv = dgrain._lib.DGR_ERR_INVALID
+    one = (C.c_int * 2)(0, 1)
+    d = (C.c_double * 1)(0.0)
+    assert lib.dgr_set_channel_ends(None, 1, one, one, one) == inv
+    assert lib.dgr_couple_channel_ends(None, d, d, d, d) == inv
+    assert lib.dgr_couple_channel_ends_device(None, None, None, None, None) == inv
+    assert lib.dgr_get_boundary(None, d, d) == inv
+    p = C.c_void_p()
+    assert lib.dgr_get_stream(None, C.byref(p)) == inv
