@@ -346,3 +346,16 @@ def test_host_manning_power_is_correctly_rounded(cores):
     y = np.empty_like(x)
     cores.dgr_t_pow43(x, y, len(x))
     assert np.array_equal(y, g["cr"])
+
+
+def test_manning_power_fast_phase_error_analysis(tmp_path):
+    """The device's fast phase of x^(4./3), restated with host stand-ins for its float
+    intrinsics (tests/pow43_sim.c), with the seed and the log pushed to the ends of their
+    error bounds: every value its rounding test keeps equals the exact phase's."""
+    exe = str(tmp_path / "pow43_sim")
+    subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-o", exe, os.path.join(HERE, "pow43_sim.c"), "-lm"],
+                   check=True)
+    res = subprocess.run([exe, "2000000"], capture_output=True, text=True)
+    assert res.returncode == 0, res.stdout
+    lines = res.stdout.strip().splitlines()
+    assert len(lines) == 3 and all(" 0 differ" in ln for ln in lines), lines
