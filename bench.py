@@ -613,8 +613,12 @@ def main():
     ap.add_argument("--calib-ckpt", type=int, default=50)
     ap.add_argument("--calib-iterations", type=int, default=0)
     ap.add_argument("--no-calibration", action="store_true")
-    ap.add_argument("--io", action="store_true", help="add the mesh-ingest and .dat-writer comparison")
-    ap.add_argument("--coupling", action="store_true", help="add the channel-junction coupling pass comparison")
+    ap.add_argument("--io", action="store_true",
+                    help="the mesh-ingest and .dat-writer comparison also at N > 1 (on by default at N = 1)")
+    ap.add_argument("--no-io", action="store_true")
+    ap.add_argument("--coupling", action="store_true",
+                    help="the channel-junction coupling comparison also at N > 1 (on by default at N = 1)")
+    ap.add_argument("--no-coupling", action="store_true")
     args = ap.parse_args()
     if args.e2e_steps < 0:
         args.e2e_steps = args.steps
@@ -737,16 +741,24 @@ def main():
             lib.dgr_host_free(C.c_void_p(host[k].ctypes.data))
         lib.dgr_host_free(C.c_void_p(wdp))
 
+    # the legs beside the step: rank 0, at N = 1 unless asked for; a failure there is
+    # reported in its own key and leaves the rest of the line intact
     io = None
-    if args.io and rank == 0:
+    if rank == 0 and (args.io or (world == 1 and not args.no_io)):
         import tempfile
 
-        with tempfile.TemporaryDirectory() as tmp:
-            io = io_bench(m, solver, tmp)
+        try:
+            with tempfile.TemporaryDirectory() as tmp:
+                io = io_bench(m, solver, tmp)
+        except Exception as e:  # noqa: BLE001
+            io = {"error": f"{type(e).__name__}: {e}"}
 
     cpl = None
-    if args.coupling and rank == 0:
-        cpl = coupling_bench(m, solver)
+    if rank == 0 and (args.coupling or (world == 1 and not args.no_coupling)):
+        try:
+            cpl = coupling_bench(m, solver)
+        except Exception as e:  # noqa: BLE001
+            cpl = {"error": f"{type(e).__name__}: {e}"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
