@@ -30,7 +30,7 @@ CC_FLAGS = ["-std=c99", "-O2", "-ffp-contract=off", "-fPIC", "-Wall", "-Wextra",
 CU_SOURCES = ["dgr_capi.cu", "dgr_noalloc.cu", "dgr_adjoint.cu", "dgr_output.cu", "dgr_ingest.cu", "dgr_coupling.cu"]
 C_SOURCES = ["dgr_host.c"]
 DEPS = ["dgr_kernels.cuh", "dgr_device.cuh", "dgr_forcing.h", "dgr_internal.cuh", "dgr_scheme.cuh",
-        "dgr_dual.cuh", "dgr_reverse.cuh", "dgr_tlm.cuh", "dgr_p2.cuh", "dgr_p2_adjoint.cuh", "dgr_format.cuh", os.path.join("..", "..", "include", "dgrain.h")]
+        "dgr_dual.cuh", "dgr_reverse.cuh", "dgr_tlm.cuh", "dgr_p2.cuh", "dgr_p2_adjoint.cuh", "dgr_format.cuh", "dgr_ptr.h", os.path.join("..", "..", "include", "dgrain.h")]
 
 
 def _nvcc() -> str:

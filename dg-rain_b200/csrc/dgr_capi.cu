@@ -1261,16 +1261,13 @@ extern "C" int dgr_get_schedule(const dgr_ctx *c, int *block_size, int *fusion)
  * receives the ms per step of each trial at index 3*b + f (b: 64, 128, 256; f: fusion),
  * -1 where the schedule could not run.
  */
-extern "C" int dgr_autotune(dgr_ctx *c, int trial_steps, int *block_size, int *fusion, double *ms_out)
+/* The trials of dgr_autotune, with the state saved in saveU/saveWD (owned by the caller,
+ * which frees them on every return path). */
+static int autotune_trials(dgr_ctx *c, int trial_steps, double *saveU, int *saveWD, int *best_bs_out,
+                           int *best_f_out, double *ms_out)
 {
-    if (!c || trial_steps <= 0) return DGR_ERR_INVALID;
-    CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     const size_t nU = 3 * (size_t)c->nm * c->ldE;
-    double *saveU = nullptr;
-    int *saveWD = nullptr;
-    CK(cudaMallocAsync((void **)&saveU, nU * 8, s));
-    CK(cudaMallocAsync((void **)&saveWD, 3 * (size_t)c->ne * 4, s));
     CK(cudaMemcpyAsync(saveU, c->U, nU * 8, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(saveWD, c->wdA, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(saveWD + c->ne, c->wdB, (size_t)c->ne * 4, cudaMemcpyDeviceToDevice, s));
@@ -1318,15 +1315,38 @@ extern "C" int dgr_autotune(dgr_ctx *c, int trial_steps, int *block_size, int *f
             c->wd_fresh = fresh0;
             c->wd_stepped = curB0;
         }
-    CK(cudaFreeAsync(saveU, s));
-    CK(cudaFreeAsync(saveWD, s));
-    CK(cudaStreamSynchronize(s));
+    *best_bs_out = best_bs;
+    *best_f_out = best_f;
+    return best < 1e300 ? DGR_OK : DGR_ERR_CUDA;
+}
+
+extern "C" int dgr_autotune(dgr_ctx *c, int trial_steps, int *block_size, int *fusion, double *ms_out)
+{
+    if (!c || trial_steps <= 0) return DGR_ERR_INVALID;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    const size_t nU = 3 * (size_t)c->nm * c->ldE;
+    double *saveU = nullptr;
+    int *saveWD = nullptr;
+    CK(cudaMallocAsync((void **)&saveU, nU * 8, s));
+    if (cudaMallocAsync((void **)&saveWD, 3 * (size_t)c->ne * 4, s) != cudaSuccess) {
+        cudaFreeAsync(saveU, s);
+        return DGR_ERR_CUDA;
+    }
+    int best_bs = c->bs, best_f = c->fusion;
+    const int rc = autotune_trials(c, trial_steps, saveU, saveWD, &best_bs, &best_f, ms_out);
+    const cudaError_t e1 = cudaFreeAsync(saveU, s), e2 = cudaFreeAsync(saveWD, s);
+    const cudaError_t e3 = cudaStreamSynchronize(s);
     c->bs = best_bs;
     c->fusion = best_f;
     drop_graph(c);
+    if (rc) return rc;
+    CK(e1);
+    CK(e2);
+    CK(e3);
     if (block_size) *block_size = best_bs;
     if (fusion) *fusion = best_f;
-    return best < 1e300 ? DGR_OK : DGR_ERR_CUDA;
+    return DGR_OK;
 }
 
 extern "C" int dgr_get_decisions(dgr_ctx *c, int stage, int *limit, int *pdop)

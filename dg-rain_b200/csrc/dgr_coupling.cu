@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "dgr_internal.cuh"
+#include "dgr_ptr.h"
 
 using namespace dgr;
 
@@ -114,18 +115,6 @@ void free_coupling(dgr_ctx *c)
 
 void coupling_release(dgr_ctx *c) { free_coupling(c); }
 
-/* memory the kernel may address: device, managed, or pinned host memory (mapped into the
- * unified address space); pageable host memory is refused before any launch */
-static bool device_addressable(const void *p)
-{
-    cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        (void)cudaGetLastError();
-        return false;
-    }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged || a.type == cudaMemoryTypeHost;
-}
-
 extern "C" int dgr_set_channel_ends(dgr_ctx *c, int nends, const int *end_ptr, const int *end_edges,
                                     const int *end_outflow)
 {
@@ -207,7 +196,7 @@ extern "C" int dgr_couple_channel_ends_device(dgr_ctx *c, const double *d_a_end,
     CK(cudaSetDevice(c->device));
     for (const void *p : {(const void *)d_a_end, (const void *)d_q_end, (const void *)d_a_ghost,
                           (const void *)d_q_ghost})
-        if (!device_addressable(p)) return DGR_ERR_INVALID;
+        if (!dgr_device_addressable(p, c->device)) return DGR_ERR_INVALID; /* before any launch */
     k_cpl_pass<<<blocks(n, 128), 128, 0, c->stream>>>(n, c->cpl_nedges, c->ldE, c->cpl_ptr, c->cpl_out,
                                                       c->cpl_edge, c->cpl_slot, c->cpl_geo, c->U, c->bzeta, c->bqn,
                                                       d_a_end, d_q_end, d_a_ghost, d_q_ghost);

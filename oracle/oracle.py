@@ -35,9 +35,18 @@ def _i(a):
     return a.ctypes.data_as(iptr)
 
 
+# Where the reference tree is mounted in the build container (DGR_REFERENCE overrides it);
+# hosts without it build the restatement only and use the prebuilt reference files.
+REFERENCE_TREE = os.environ.get("DGR_REFERENCE", "/root/reference")
+
+
 def build() -> None:
     """make -C oracle (restatement always; the reference only where its tree exists)."""
-    res = subprocess.run(["make", "-s", "-C", HERE], capture_output=True, text=True)
+    cmd = ["make", "-s", "-C", HERE]
+    ref2d = os.path.join(REFERENCE_TREE, "2DCode")
+    if os.path.exists(os.path.join(ref2d, "compute2DL.c")):
+        cmd.append(f"REF={ref2d}")
+    res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + res.stdout + res.stderr)
 

@@ -105,3 +105,31 @@ def test_coupling_entry_points_check_their_arguments(dgrain):
     assert lib.dgr_get_boundary(None, d, d) == inv
     p = C.c_void_p()
     assert lib.dgr_get_stream(None, C.byref(p)) == inv
+
+
+def test_pointer_rule_of_the_device_buffer_entry_points(tmp_path):
+    """The rule dgr_couple_channel_ends_device and dgr_slope_limiter_noalloc apply to a
+    caller's pointer before launching (dg-rain_b200/csrc/dgr_ptr.h), on attribute values a
+    one-GPU machine cannot produce: another GPU's buffer is refused even though it is
+    device memory, and so are unmapped or pageable host memory."""
+    import subprocess
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    lib_path = str(tmp_path / "libptr_host.so")
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", cuda_inc, "-o", lib_path,
+                    os.path.join(here, "ptr_host.cpp")], check=True)
+    lib = C.CDLL(lib_path)
+    lib.dgr_t_may_access.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+    types = (C.c_int * 4)()
+    lib.dgr_t_memory_types(types)
+    unregistered, host, device, managed = list(types)
+    p = 0x7f0000001000
+    ok = lambda t, owner, dptr, dev: bool(lib.dgr_t_may_access(t, owner, dptr, p, dev))  # noqa: E731
+    assert ok(device, 0, p, 0) and ok(device, 3, p, 3)
+    assert not ok(device, 1, p, 0)          # another GPU's memory
+    assert not ok(device, 0, p + 256, 0)    # not addressable at this address
+    assert ok(managed, 0, p, 2)             # managed memory, mapped where the kernel runs
+    assert ok(host, 0, p, 0)                # pinned and mapped (unified addressing)
+    assert not ok(host, 0, None, 0)         # pinned but not mapped
+    assert not ok(unregistered, 0, None, 0) and not ok(unregistered, 0, p, 0)  # pageable memory
