@@ -48,6 +48,18 @@ DGR_HD double val(double x) { return x; }
  * tie the values agree and a is taken. */
 DGR_HD bool fmax_takes_b(double a, double b) { return (b > a) || isnan(a); }
 
+/* fmax as the reference build evaluates it.  glibc's x86-64 fmax(x, y) returns
+ * x > y ? x : y, a NaN operand giving the other one, so a tie returns y (which decides
+ * the sign of a zero result); and gcc passes a call's operands in whichever order it
+ * chooses, fmax being commutative up to that sign.  The reference step as compiled
+ * (gcc -O2 -ffp-contract=off, x86-64) keeps the written order at the limiter's clamp
+ * (2DCode/SlopeLimiter2D.c:244-246) and swaps it in RoeFlux's entropy fix
+ * (2DCode/numericalFlux2D.c:74-84).  fmax_b(a, b) is the call as written (a tie returns
+ * b), fmax_a(a, b) the swapped call (a tie returns a).  CUDA's fmax is not used there: its
+ * result for zeros of opposite sign is not the reference's. */
+DGR_HD double fmax_b(double a, double b) { return (a > b || isnan(b)) ? a : b; }
+DGR_HD double fmax_a(double a, double b) { return (b > a || isnan(a)) ? b : a; }
+
 /* Dense 3x3 times vector, summed from +0 in column order (2DCode/mathfunctions.c:24-35). */
 template <class T>
 DGR_HD void matvec3(const T m[3][3], const T v[3], T out[3])
@@ -103,15 +115,15 @@ DGR_HD T roe_flux(T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy
     const T un_hat = u_hat * nx + v_hat * ny;
     T lh1 = un_hat - c, lh2 = un_hat, lh3 = un_hat + c;
 
-    T e1 = fmax(0.0, (lh1 - l1_in));
-    e1 = fmax(e1, (l1_ex - lh1));
-    lh1 = fmax(e1, fabs(lh1));
-    T e2 = fmax(0.0, (lh2 - l2_in));
-    e2 = fmax(e2, (l2_ex - lh2));
-    lh2 = fmax(e2, fabs(lh2));
-    T e3 = fmax(0.0, (lh3 - l3_in));
-    e3 = fmax(e3, (l3_ex - lh3));
-    lh3 = fmax(e3, fabs(lh3));
+    T e1 = fmax_a(0.0, (lh1 - l1_in));
+    e1 = fmax_a(e1, (l1_ex - lh1));
+    lh1 = fmax_a(e1, fabs(lh1));
+    T e2 = fmax_a(0.0, (lh2 - l2_in));
+    e2 = fmax_a(e2, (l2_ex - lh2));
+    lh2 = fmax_a(e2, fabs(lh2));
+    T e3 = fmax_a(0.0, (lh3 - l3_in));
+    e3 = fmax_a(e3, (l3_ex - lh3));
+    lh3 = fmax_a(e3, fabs(lh3));
 
     const T lam[3][3] = {{lh1, 0, 0}, {0, lh2, 0}, {0, 0, lh3}};
     T p1[3], p2[3], p3[3];

@@ -8,7 +8,9 @@
  * flags, limiter clamps, entropy-fix selections, PDop branches) frozen at the primal's.
  *
  * Conventions at the kinks, shared with the hand-written reverse in dgr_reverse.cuh:
- *   fmax(a, b)  takes b when b > a (or a is NaN), else a
+ *   fmax(a, b)  takes b when b > a (or a is NaN), else a; so do fmax_a and fmax_b (the
+ *               reference build's two operand orders), whose values differ from fmax's
+ *               only in the sign of a zero
  *   fabs(a)     derivative -d for a < 0, +d otherwise
  *   sqrt(a)     derivative 0 at a == 0 (the only zero argument on the path is the speed
  *               |u| of the Manning term, whose product with the discharge has derivative 0)
@@ -86,6 +88,17 @@ DGR_HD Dual fmax(const Dual &a, const Dual &b)
 }
 DGR_HD Dual fmax(double a, const Dual &b) { return fmax(Dual(a), b); }
 DGR_HD Dual fmax(const Dual &a, double b) { return fmax(a, Dual(b)); }
+/* the reference build's two orders of fmax (dgr_device.cuh): values as the double
+ * functions, derivatives by the same convention as fmax */
+DGR_HD Dual fmax_a(const Dual &a, const Dual &b) { return ((b.v > a.v) || ::isnan(a.v)) ? b : a; }
+DGR_HD Dual fmax_a(double a, const Dual &b) { return fmax_a(Dual(a), b); }
+DGR_HD Dual fmax_a(const Dual &a, double b) { return fmax_a(a, Dual(b)); }
+DGR_HD Dual fmax_b(const Dual &a, const Dual &b)
+{
+    return Dual(dgr::fmax_b(a.v, b.v), ((b.v > a.v) || ::isnan(a.v)) ? b.d : a.d);
+}
+DGR_HD Dual fmax_b(double a, const Dual &b) { return fmax_b(Dual(a), b); }
+DGR_HD Dual fmax_b(const Dual &a, double b) { return fmax_b(a, Dual(b)); }
 
 /* x^(4/3) with the correctly rounded value of the double path; d/dx = (4/3) x^(1/3) */
 DGR_HD Dual pow43(const Dual &a)
@@ -149,6 +162,15 @@ DGR_HD Pert fmax(const Pert &a, const Pert &b)
 }
 DGR_HD Pert fmax(double a, const Pert &b) { return fmax(Pert(a), b); }
 DGR_HD Pert fmax(const Pert &a, double b) { return fmax(a, Pert(b)); }
+DGR_HD Pert fmax_a(const Pert &a, const Pert &b) { return ((b.v > a.v) || ::isnan(a.v)) ? b : a; }
+DGR_HD Pert fmax_a(double a, const Pert &b) { return fmax_a(Pert(a), b); }
+DGR_HD Pert fmax_a(const Pert &a, double b) { return fmax_a(a, Pert(b)); }
+DGR_HD Pert fmax_b(const Pert &a, const Pert &b)
+{
+    return Pert(dgr::fmax_b(a.v, b.v), ((b.v > a.v) || ::isnan(a.v)) ? b.p : a.p);
+}
+DGR_HD Pert fmax_b(double a, const Pert &b) { return fmax_b(Pert(a), b); }
+DGR_HD Pert fmax_b(const Pert &a, double b) { return fmax_b(a, Pert(b)); }
 DGR_HD Pert pow43(const Pert &a) { return Pert(dgr::pow43(a.v), dgr::pow43(a.p)); }
 DGR_HD double val(const Pert &x) { return x.v; }
 

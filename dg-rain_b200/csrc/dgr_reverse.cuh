@@ -79,13 +79,13 @@ DGR_HD void roe_flux_rev(const double fhb[3], double zeta_in, double zeta_ex, do
     for (int i = 0; i < 3; ++i) {
         const double ea = raw[i] - lin[i];
         int s = fmax_takes_b(0.0, ea) ? 1 : 0;
-        double e = fmax(0.0, ea);
+        double e = fmax_a(0.0, ea);
         const double eb = lex[i] - raw[i];
         if (fmax_takes_b(e, eb)) s = 2;
-        e = fmax(e, eb);
+        e = fmax_a(e, eb);
         const double al = fabs(raw[i]);
         if (fmax_takes_b(e, al)) s = 3;
-        lh[i] = fmax(e, al);
+        lh[i] = fmax_a(e, al);
         sel[i] = s;
     }
     /* p1 = R^-1 jump in closed form (the forward's matrix entries simplified):

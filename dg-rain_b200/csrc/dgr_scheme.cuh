@@ -437,7 +437,7 @@ DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, doub
                     if (fmax_takes_b(val(r1), val(vmin[k]))) c = 2;
                     tb |= c << (2 * k);
                 }
-                vx[k] = fmax(rmin(vx[k], vmax[k]), vmin[k]);
+                vx[k] = fmax_b(rmin(vx[k], vmax[k]), vmin[k]);
             }
             /* the three passes stay a loop: unrolled, the 27 copies of the pass body overflow
              * the instruction cache (measured: 8 % off the limiter kernel rolled) */

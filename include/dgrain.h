@@ -295,18 +295,22 @@ DGR_API double dgr_last_device_ms(const dgr_ctx *ctx);
  * bounds, limiter + PDop. */
 DGR_API int dgr_profile_step(dgr_ctx *ctx, int nsteps, double *kernel_ms, int n);
 
-/* Slope limiter without any device allocation — no counterpart in the reference, whose
- * SlopeLimiter (2DCode/SlopeLimiter2D.c:10) mallocs its node lists on every call.  For
- * callers that may not allocate device memory (buffers handed over by a host framework
- * or pool, or code running where cudaMalloc/cudaFree are not allowed): they pass their
- * own device arrays in the reference layout — EltoVert[3*num_el], node depth z[num_nodes],
- * zeta/Qx/Qy[3*num_el] limited in place — and a cudaStream_t (NULL = default stream).
- * The result equals dgr_slope_limiter's.  Scratch is a static device array for at most
- * DGR_NOALLOC_MAX_NODES nodes (6 MiB, held on every GPU that loads this library until
- * the process exits); larger meshes get DGR_ERR_TOO_LARGE.  All calls share that array,
- * so calls that overlap on the GPU race.  The first call on a device looks up the
- * array's address and should come before any stream capture.  The call only enqueues
- * work on the stream. */
+/* Slope limiter without any device allocation.  This entry point has no counterpart in
+ * the reference.  It is for callers that may not allocate device memory: code handed its
+ * buffers by a host framework or memory pool, or code running where cudaMalloc/cudaFree
+ * are not allowed (cudaFree synchronises the device; allocating inside a stream capture
+ * is an error).  They pass their own device arrays in the reference layout —
+ * EltoVert[3*num_el], node depth z[num_nodes], zeta/Qx/Qy[3*num_el] limited in place —
+ * and a cudaStream_t (NULL = default stream).  Every array must be memory a kernel on the
+ * current device may use (that device's own memory, managed, or mapped pinned host
+ * memory); anything else is refused with DGR_ERR_INVALID before any launch.  The result
+ * equals dgr_slope_limiter's bit for bit, signed zeros included.  Scratch is a static
+ * device array for at most DGR_NOALLOC_MAX_NODES nodes (7.5 MiB, held on every GPU that
+ * loads this library until the process exits); larger meshes get DGR_ERR_TOO_LARGE.
+ * All calls share that array, so calls that overlap on the GPU race.  The first call on
+ * a device looks up the array's address and should come before any stream capture; the
+ * address is kept for the life of the process, so the entry point must not be used on a
+ * device after a cudaDeviceReset.  The call only enqueues work on the stream. */
 #define DGR_NOALLOC_MAX_NODES 131072
 DGR_API int dgr_slope_limiter_noalloc(int num_el, int num_nodes, const int *d_EltoVert, const double *d_z,
                                       double *d_zeta, double *d_Qx, double *d_Qy, double H0, void *stream);

@@ -53,6 +53,17 @@ static int orc_sign(double a)
 static double orc_max(double a, double b) { return (a > b) ? a : b; }
 static double orc_min(double a, double b) { return (a < b) ? a : b; }
 
+/* fmax as the reference build evaluates it.  glibc's x86-64 fmax(x, y) returns
+ * x > y ? x : y, a NaN operand giving the other one; so when x and y compare equal it
+ * returns y, which matters for zeros of opposite sign.  gcc treats fmax as commutative
+ * and passes a call's operands in either order.  The build of the reference step made by
+ * oracle/Makefile (gcc -O2 -ffp-contract=off, read from its x86-64 code) keeps the
+ * written order at the limiter's clamp (2DCode/SlopeLimiter2D.c:244-246) and swaps it at
+ * RoeFlux's entropy fix (2DCode/numericalFlux2D.c:74-84).  These two helpers are those
+ * two orders of fmax(a, b): fmax_b returns b on a tie, fmax_a returns a. */
+static double fmax_b(double a, double b) { return (a > b || b != b) ? a : b; }
+static double fmax_a(double a, double b) { return (b > a || a != a) ? b : a; }
+
 orc_ctx *orc_create(int ne, int nn, int nf, const double *x, const double *y, const double *z,
                     const double *nfric, const int *el2v, const int *ed2el, const int *ed2v,
                     const int *bdry, double min_edge)
@@ -284,15 +295,15 @@ double orc_roe_flux(double *fh, double zeta_in, double zeta_ex, double qx_in, do
     double lh2 = u_hat * nx + v_hat * ny;
     double lh3 = u_hat * nx + v_hat * ny + c;
 
-    double e1 = fmax(0, (lh1 - l1_in));
-    e1 = fmax(e1, (l1_ex - lh1));
-    lh1 = fmax(e1, fabs(lh1));
-    double e2 = fmax(0, (lh2 - l2_in));
-    e2 = fmax(e2, (l2_ex - lh2));
-    lh2 = fmax(e2, fabs(lh2));
-    double e3 = fmax(0, (lh3 - l3_in));
-    e3 = fmax(e3, (l3_ex - lh3));
-    lh3 = fmax(e3, fabs(lh3));
+    double e1 = fmax_a(0, (lh1 - l1_in));
+    e1 = fmax_a(e1, (l1_ex - lh1));
+    lh1 = fmax_a(e1, fabs(lh1));
+    double e2 = fmax_a(0, (lh2 - l2_in));
+    e2 = fmax_a(e2, (l2_ex - lh2));
+    lh2 = fmax_a(e2, fabs(lh2));
+    double e3 = fmax_a(0, (lh3 - l3_in));
+    e3 = fmax_a(e3, (l3_ex - lh3));
+    lh3 = fmax_a(e3, fabs(lh3));
 
     /* R |Lambda| R^-1 jump as three dense 3x3 products (mathfunctions.c:24-35) */
     double lam[3][3] = {{lh1, 0, 0}, {0, lh2, 0}, {0, 0, lh3}};
@@ -678,7 +689,7 @@ int orc_slope_limiter(orc_ctx *c)
                 double m0 = vmin[0] + zz[0], m1 = vmin[1] + zz[1], m2 = vmin[2] + zz[2];
                 if (h1 > h0 && h2 > h0 && h3 > h0 && m0 > h0 && m1 > h0 && m2 > h0) modify = 1;
             }
-            for (int k = 0; k < 3; ++k) vx[k] = fmax(orc_min(vx[k], vmax[k]), vmin[k]);
+            for (int k = 0; k < 3; ++k) vx[k] = fmax_b(orc_min(vx[k], vmax[k]), vmin[k]);
             /* three passes of mass-conserving redistribution (:249-299) */
             for (int ll = 0; ll < 3; ++ll) {
                 double sumloc = (vx[0] + vx[1] + vx[2]) / 3;

@@ -10,7 +10,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import land_film_state
+from conftest import bits_equal, land_film_state
 
 pytestmark = pytest.mark.gpu
 
@@ -50,7 +50,7 @@ def test_ensemble_equals_scenarios_alone(dgrain):
         for k in range(len(meshes)):
             assert (t[k], dt[k], n[k]) == ref[k][0]
             for a, b in zip(e.download_state(k), ref[k][1]):
-                assert np.array_equal(a, b), k
+                assert bits_equal(a, b), k
 
 
 @pytest.mark.parametrize("block_size", [64, 128, 256])
@@ -69,10 +69,10 @@ def test_schedules_give_identical_bits(dgrain, block_size, fusion):
             base = (clock, out)
             continue
         for a, b in zip(clock, base[0]):
-            assert np.array_equal(a, b)
+            assert bits_equal(a, b)
         for k in range(len(meshes)):
             for a, b in zip(out[k], base[1][k]):
-                assert np.array_equal(a, b), (sched, k)
+                assert bits_equal(a, b), (sched, k)
 
 
 def test_single_mesh_schedules_match_oracle(dgrain, oracle_mod, mesh_c1):
@@ -92,7 +92,7 @@ def test_single_mesh_schedules_match_oracle(dgrain, oracle_mod, mesh_c1):
             s.upload_state(*st)
             assert s.time_evolution(1e9, 60) == (t_o, dt_o, n_o)
             for a, b in zip(s.download_state(), want):
-                assert np.array_equal(a, b), sched
+                assert bits_equal(a, b), sched
 
 
 def test_autotune_keeps_state_and_picks_a_schedule(dgrain):
@@ -108,7 +108,7 @@ def test_autotune_keeps_state_and_picks_a_schedule(dgrain):
         assert e.get_schedule() == (bs, fu)
         for k in range(2):
             for a, b in zip(e.download_state(k), before[k]):
-                assert np.array_equal(a, b)
+                assert bits_equal(a, b)
         t2, dt2, n2 = e.run(5, time=t, dt=dt)
         assert (n2 == 5).all()
 

@@ -16,7 +16,8 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import land_film_state, load_golden, mesh_from_golden, moving_state
+from conftest import (bits_equal, land_film_state, load_golden, mesh_from_golden, moving_state, negative_zeros,
+                      signed_zero_state)
 
 pytestmark = pytest.mark.gpu
 
@@ -30,7 +31,7 @@ def rel_err(a, b):
 
 
 def same(a, b):
-    return np.array_equal(np.asarray(a), np.asarray(b))
+    return bits_equal(a, b)
 
 
 def no_friction(dgrain, m):
@@ -258,7 +259,7 @@ def test_manning_power_correctly_rounded(dgrain):
     lib = dgrain.load()
     assert lib.dgr_pow43_batch(x.ctypes.data_as(dgrain._lib.dptr), y.ctypes.data_as(dgrain._lib.dptr),
                                len(x), 0) == 0
-    assert np.array_equal(y, g["cr"])
+    assert bits_equal(y, g["cr"])
     # glibc's pow (the reference's) agrees wherever glibc is correctly rounded
     agree = (y == g["glibc"]).mean()
     assert agree > 0.998, agree
@@ -295,3 +296,20 @@ def test_manning_power_fast_phase_equals_exact(dgrain):
     host.dgr_t_pow43(x, want, len(x))
     bad = np.flatnonzero(y != want)
     assert bad.size == 0, (bad.size, x[bad[:5]], y[bad[:5]], want[bad[:5]])
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_limiter_signed_zero_bounds(dgrain, oracle_mod, seed):
+    """Node bounds that are zeros of either sign: the device limiter keeps the sign of the
+    first zero mean in element order and clamps as the reference build does (its fmax
+    returns the second operand on a tie), bit for bit with the oracle."""
+    m = dgrain.rectangle(60, 30, jitter=0.1, seed=13)
+    st = signed_zero_state(dgrain, m, seed, nx=60)
+    s, o = make_pair(dgrain, oracle_mod, m, st)
+    s.SlopeLimiter()
+    o.slope_limiter()
+    got, want = s.download_state(), o.get_state()
+    for a, b in zip(got, want):
+        assert same(a, b)
+    assert negative_zeros(want[1]) > 0
+    s.close()

@@ -7,7 +7,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import land_film_state
+from conftest import bits_equal, land_film_state
 
 pytestmark = pytest.mark.gpu
 
@@ -30,7 +30,7 @@ def test_rk3_run_matches_oracle(dgrain, oracle_mod, schedule):
         s.upload_state(*st)
         assert s.time_evolution(1e9, 40) == (t_o, dt_o, n_o)
         for a, b in zip(s.download_state(), o.get_state()):
-            assert np.array_equal(a, b), schedule
+            assert bits_equal(a, b), schedule
 
 
 def test_rk3_host_step_matches_device_loop(dgrain):
@@ -49,7 +49,7 @@ def test_rk3_host_step_matches_device_loop(dgrain):
             d = 0.3 * m.min_edge / lam
         assert (tt, d) == (t, dt)
         for a, b in zip(s.download_state(), want):
-            assert np.array_equal(a, b)
+            assert bits_equal(a, b)
 
 
 def test_rk3_ensemble_equals_alone(dgrain):
@@ -69,7 +69,7 @@ def test_rk3_ensemble_equals_alone(dgrain):
         for k in range(2):
             assert (t[k], dt[k], n[k]) == alone[k][0]
             for a, b in zip(e.download_state(k), alone[k][1]):
-                assert np.array_equal(a, b)
+                assert bits_equal(a, b)
 
 
 def test_rk3_adjoint(dgrain):

@@ -10,7 +10,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import land_film_state, moving_state
+from conftest import bits_equal, land_film_state, moving_state, negative_zeros, signed_zero_state
 
 pytestmark = pytest.mark.skipif(
     not __import__("oracle.oracle", fromlist=["x"]).have_reference(),
@@ -18,7 +18,7 @@ pytestmark = pytest.mark.skipif(
 
 
 def _same(a, b):
-    return np.array_equal(np.asarray(a), np.asarray(b))
+    return bits_equal(a, b)
 
 
 @pytest.mark.parametrize("jitter,seed,nx,ny", [(0.0, 1, 40, 20), (0.1, 3, 30, 17), (0.1, 9, 13, 29)])
@@ -200,3 +200,24 @@ def test_time_loop_matches_reference_time_evolution(dgrain, oracle_mod, mesh_j, 
     s = orc.get_state()
     for a, b in zip(got, s[:3]):
         np.testing.assert_allclose(a, b, rtol=0, atol=1e-15 * (1 + np.abs(b).max()) + 1e-15)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_limiter_signed_zero_bounds_bitexact(dgrain, oracle_mod, seed):
+    """Node bounds that are zeros of either sign, and the limiter's clamp on them: the
+    restatement gives the reference build's bits, signs of zeros included (the reference
+    binary's fmax returns its second operand on a tie)."""
+    m = dgrain.rectangle(60, 30, jitter=0.1, seed=13)
+    st = signed_zero_state(dgrain, m, seed, nx=60)
+    o = oracle_mod.Oracle(m)
+    o.set_state(*st)
+    o.slope_limiter()
+    r = oracle_mod.Reference(wet_dry=True)
+    r.set_mesh(m)
+    r.initialize()
+    r.set_state(*st)
+    r.slope_limiter()
+    got, want = o.get_state(), r.get_state()
+    for a, b in zip(got[:3], want[:3]):
+        assert _same(a, b)
+    assert negative_zeros(want[1]) > 0  # the case reaches the sign of a zero

@@ -16,19 +16,16 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from conftest import land_film_state
+from conftest import negative_zeros, signed_zero_state
 
 pytestmark = pytest.mark.gpu
 
 
-def rough_state(dgrain, m, seed):
-    rng = np.random.default_rng(seed)
-    z, qx, qy, wd = land_film_state(dgrain, m)
-    return (z + 0.002 * rng.standard_normal(z.shape), 0.01 * rng.standard_normal(qx.shape),
-            0.01 * rng.standard_normal(qy.shape), wd)
+def bits(a):
+    return np.ascontiguousarray(a, dtype=np.float64).view(np.int64)
 
 
-def test_noalloc_limiter_matches_context_limiter(dgrain):
+def test_noalloc_limiter_matches_context_limiter(dgrain, oracle_mod):
     import torch
 
     lib = dgrain.load()
@@ -39,11 +36,16 @@ def test_noalloc_limiter_matches_context_limiter(dgrain):
     stream = torch.cuda.current_stream(dev)
     fired = 0
     for seed in (1, 2):  # two calls in a row
-        st = rough_state(dgrain, m, seed)
+        st = signed_zero_state(dgrain, m, seed, nx=60)
         with dgrain.Solver(m) as s:  # the existing entry point
             s.upload_state(*st)
             s.SlopeLimiter()
             want = s.download_state()[:3]
+        o = oracle_mod.Oracle(m)  # the reference's limiter, restated on the CPU
+        o.set_state(*st)
+        o.slope_limiter()
+        for a, b in zip(want, o.get_state()[:3]):
+            assert np.array_equal(bits(a), bits(b))
         d = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in st[:3]]
         rc = lib.dgr_slope_limiter_noalloc(m.num_el, m.num_nodes, C.c_void_p(el2v.data_ptr()),
                                            C.c_void_p(z.data_ptr()), C.c_void_p(d[0].data_ptr()),
@@ -53,8 +55,10 @@ def test_noalloc_limiter_matches_context_limiter(dgrain):
         torch.cuda.synchronize(dev)
         got = [t.cpu().numpy() for t in d]
         for a, b in zip(got, want):
-            assert np.array_equal(a, b)
+            assert np.array_equal(bits(a), bits(b))  # bit patterns: the signs of zeros count
         fired += int((got[0] != st[0]).any())
+        # the zero patch reached the output: the limited Qx holds zeros of both signs
+        assert 0 < negative_zeros(got[1]) < int((got[1] == 0.0).sum())
     assert fired == 2  # the limiter changed both states
 
 
