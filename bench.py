@@ -39,6 +39,7 @@ for _p in (ROOT, PKG):
 NX, NY, JITTER, CFL, AMP, PERIOD = 2000, 1000, 0.1, 0.3, 0.5, 44712.0
 LAND_FILM = 0.5e-3      # dry land holds H0/2: with exactly H0 the reference wet/dry step stops on a NaN flux
 ALG_BYTES = 216         # algorithmic bytes per element-stage (state in, step input, state out)
+RTOL_PARITY = 1e-11     # device vs reference state, relative to each field's largest magnitude
 METRIC = "element-stage updates/s"
 ADJ_CFL = 0.1           # the reference's own CFL (2DCode/time_evolution.c:399) for the 4,000-step adjoint run:
                         # at 0.3 the rising tide takes the reference wet/dry scheme to a NaN flux at step 2,610
@@ -48,15 +49,50 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def make_workload(seed: int, nx=NX, ny=NY):
+def make_workload(seed: int, nx=NX, ny=NY, native=True):
+    """The bench mesh and its initial state.  native=False builds the connectivity and the
+    state with the oracle's numpy restatement of the reference's set-up instead of this
+    repository's library, so that the reference arm loads no code of ours (same arrays:
+    tests/test_golden.py)."""
     import dgrain
 
     t0 = time.perf_counter()
-    m = dgrain.rectangle(nx, ny, jitter=JITTER, seed=seed)
-    st = dgrain.initial_state(m, np.maximum(0.0, LAND_FILM - m.z))
+    zn = lambda m: np.maximum(0.0, LAND_FILM - m.z)  # noqa: E731
+    if native:
+        m = dgrain.rectangle(nx, ny, jitter=JITTER, seed=seed)
+        st = dgrain.initial_state(m, zn(m))
+    else:
+        from oracle import mesh_setup
+
+        m = dgrain.rectangle(nx, ny, jitter=JITTER, seed=seed, connect=False)
+        m.ed2v, m.ed2el, m.bdry, m.min_edge = mesh_setup.connectivity(m.el2v, m.x, m.y, m.inflow1, m.inflow2,
+                                                                      m.outflow)
+        st = mesh_setup.initial_state(m.el2v, zn(m))
     log(f"[bench] mesh {m.num_el} triangles, {m.num_nodes} nodes, {m.num_edges} edges "
         f"built in {time.perf_counter() - t0:.1f} s")
     return m, st
+
+
+def workload_config(nx: int, ny: int, num_el: int, num_edges: int, n_gpus: int) -> dict:
+    """The `config` of both arms' JSON lines (one dict, so that they compare equal)."""
+    return {"workload": f"coastal rectangle {nx}x{ny} cells (10 km x 5 km), {num_el:,} triangles, "
+                        "jitter 0.1, p=1 CR/RT0, SSP-RK2, Roe, vertex limiter, wet/dry on, "
+                        "tide 0.5 m / 12.42 h, Manning 0.03, CFL 0.3, FP64",
+            "num_el": num_el, "num_edges": num_edges, "parallelism": f"replicas x{n_gpus}",
+            "l2": f"inputs larger than L2 (state {72 * num_el / 1e6:.0f} MB, geometry {504 * num_el / 1e9:.1f} GB "
+                  "per replica); no flush"}
+
+
+def bits_equal(a, b) -> bool:
+    """bit for bit (signs of zeros count; NaNs match whatever their payload)"""
+    a, b = np.asarray(a), np.asarray(b)
+    if a.shape != b.shape:
+        return False
+    if a.dtype.kind != "f":
+        return bool(np.array_equal(a, b))
+    a, b = np.ascontiguousarray(a, dtype=np.float64), np.ascontiguousarray(b, dtype=np.float64)
+    na, nb = np.isnan(a), np.isnan(b)
+    return bool(np.array_equal(na, nb) and np.array_equal(a.view(np.int64)[~na], b.view(np.int64)[~nb]))
 
 
 def measured_peak():
@@ -142,10 +178,12 @@ class ClockSampler:
 
 
 def cpu_baseline_reference(m, st, steps: int = 2, warmup: int = 1, max_seconds: float = 60.0,
-                           optimised: bool = False):
+                           optimised: bool = False, final: dict | None = None, o3_steps: int = 2):
     """The reference C step (oracle/_ref, unmodified 2DCode compiled with gcc -O2) on this
     host, one core, on the same mesh and state; falls back to the oracle restatement.
-    optimised: the -O3 -march=x86-64-v3 build of the same sources (timing only)."""
+    optimised: the -O3 -march=x86-64-v3 build of the same sources (timing only; o3_steps of it
+    are timed beside the -O2 figure).  final: receives the reference's state, clock and step counts after the sample (the
+    parity check runs the device loop over the same steps)."""
     from oracle import oracle as O
 
     if O.have_reference():
@@ -168,14 +206,39 @@ def cpu_baseline_reference(m, st, steps: int = 2, warmup: int = 1, max_seconds: 
             break
         done += 1
     el = time.perf_counter() - t0
+    if final is not None:
+        final.update(state=r.get_state(), time=t, dt=dt, warmup=warmup, steps=done, rc=rc, kind=kind)
     value = m.num_el * 2 * done / el if done else 0.0
-    out = {"value": value, "unit": METRIC, "cores": 1, "kind": kind,
+    out = {"value": value, "unit": METRIC, "cores": 1, "kind": kind, "steps": done, "seconds": el,
            "sample": f"{done} time steps of the {m.num_el}-triangle workload after {warmup} warm-up step(s), "
                      f"{el:.1f} s, gcc {'-O3 -march=x86-64-v3' if optimised else '-O2'} build, one host core"}
-    if kind == "reference" and not optimised and os.path.exists(O.REF_LIB_WD_O3):
-        o3 = cpu_baseline_reference(m, st, steps=steps, warmup=warmup, max_seconds=max_seconds, optimised=True)
+    if kind == "reference" and not optimised and os.path.exists(O.REF_LIB_WD_O3) and o3_steps > 0:
+        o3 = cpu_baseline_reference(m, st, steps=o3_steps, warmup=warmup, max_seconds=max_seconds, optimised=True)
         out["o3_x86_64_v3"] = {"value": o3["value"], "sample": o3["sample"]}
     return out
+
+
+def parity_vs_reference(m, st, solver, ref: dict) -> dict:
+    """The device loop over the steps the reference sample ran (its warm-up, then its timed
+    steps, in the same calls), from the same initial state: wet/dry flags must be identical
+    and the state within RTOL_PARITY of each field's largest magnitude (Manning friction:
+    the device's H^(4/3) is correctly rounded, glibc's pow is not for ~0.1 % of arguments)."""
+    if ref.get("rc", 0) != 0:
+        return {"kind": ref.get("kind"), "error": f"reference stopped with status {ref['rc']}"}
+    solver.upload_state(*st)
+    t, dt = -1.0, 0.0
+    if ref["warmup"]:
+        t, dt, _ = solver.time_evolution(1e9, ref["warmup"])
+    t, dt, n = solver.time_evolution(1e9, ref["steps"], t, dt)
+    got, want = solver.download_state(), ref["state"]
+    rel = {k: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+           for k, a, b in zip(("zeta", "qx", "qy"), got[:3], want[:3])}
+    mism = int((got[3] != want[3]).sum())
+    return {"kind": ref["kind"], "steps": ref["warmup"] + n, "triangles": m.num_el, "wd_mismatches": mism,
+            "max_rel": rel, "bit_identical": {k: bits_equal(a, b) for k, a, b in zip(("zeta", "qx", "qy"), got[:3],
+                                                                                     want[:3])},
+            "time_equal": t == ref["time"], "dt_rel": abs(dt - ref["dt"]) / abs(ref["dt"]),
+            "tolerance": RTOL_PARITY, "ok": bool(mism == 0 and max(rel.values()) <= RTOL_PARITY)}
 
 
 def ensemble_workload(nscen: int, seed: int = 7, lo: int = 5000, hi: int = 80000, subset=None):
@@ -301,7 +364,7 @@ def ensemble_bench(nscen: int, steps: int, warmup: int, device: int = 0, dist=No
         tk, dk, nk = s.time_evolution(1e300, steps, clocks[k][0], clocks[k][1])
         looped_dev += s.last_device_ms()
     looped_wall = (time.perf_counter() - w0) * 1e3
-    same = all(all(np.array_equal(a, b) for a, b in zip(s.download_state(), batched[k]))
+    same = all(all(bits_equal(a, b) for a, b in zip(s.download_state(), batched[k]))
                for k, s in enumerate(solvers))
     for s in solvers:
         s.close()
@@ -556,7 +619,7 @@ def coupling_bench(m, solver, repeats: int = 200):
     ev1.record(st)
     ev1.synchronize()
     dev_buf_us = ev0.elapsed_time(ev1) * 1e3 / repeats
-    same_dev = bool(np.array_equal(ga.cpu().numpy(), ag) and np.array_equal(gq.cpu().numpy(), qg))
+    same_dev = bits_equal(ga.cpu().numpy(), ag) and bits_equal(gq.cpu().numpy(), qg)
     z, x, y, _ = solver.download_state()
     bz, bq = solver.get_boundary()
     solver.set_channel_ends([])
@@ -564,25 +627,47 @@ def coupling_bench(m, solver, repeats: int = 200):
              for a, q, g in zip(a_end, q_end, groups)]
     ref = orc.have_reference_coupling()
     _, _, outs, ref_s = orc.internal_bc(m, z, x, y, bz, bq, chans, reference=ref, repeats=repeats)
-    same = all(ag[i] == outs[i][0][0] and qg[i] == outs[i][1][0] for i in range(len(groups)))
+    same = bits_equal(ag, [o[0][0] for o in outs]) and bits_equal(qg, [o[1][0] for o in outs])
     return {"channel_ends": len(groups), "coupled_edges": per * len(groups), "device_pass_us": dev_s * 1e6,
             "device_buffers_pass_us": dev_buf_us, "host_pass_us": ref_s * 1e6,
             "host_kind": "reference" if ref else "port", "identical": bool(same and same_dev)}
 
 
+def headline(ens, adj, cal) -> dict:
+    """The task's three targets in one short object, printed last on the line: batched
+    ensemble vs the plain step looped (bit-identical), adjoint cost over the forward run,
+    and the adjoint checks; the calibration leg's adjoint cost as well."""
+    ok = lambda d: isinstance(d, dict) and "error" not in d  # noqa: E731
+    h = {}
+    if ok(ens):
+        h["ensemble_speedup"] = round(ens["speedup"], 3)
+        h["ensemble_bit_identical"] = ens["bit_identical"]
+        h["ensemble_schedule"] = f'{ens["schedule"]["block_size"]}/{ens["schedule"]["fusion"]}'
+    if ok(adj):
+        h["adjoint_over_forward"] = round(adj["adjoint_over_forward"], 3)
+        h["fd_max_rel"] = adj["fd_max_rel"]
+        h["tlm_vs_adjoint_max_rel"] = adj["tlm_vs_adjoint_max_rel"]
+    if ok(cal):
+        h["calibration_adjoint_over_forward"] = round(cal["adjoint_over_forward"], 3)
+    return h
+
+
 def run_reference_arm(args):
+    """The reference's own C step (oracle/_ref, the unmodified 2DCode sources, gcc -O2) on this
+    host's cores over the same workload; it is serial, so one core.  Mesh set-up and initial
+    state come from the oracle's numpy restatement of the reference's set-up: no code of this
+    repository's library runs in this arm."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    m, st = make_workload(2)
-    cb = cpu_baseline_reference(m, st, steps=max(1, args.steps), warmup=max(0, min(args.warmup, 1)),
-                                max_seconds=args.ref_seconds)
-    line = {"metric": METRIC, "value": cb["value"], "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "impl": "reference", "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "coastal rectangle 2000x1000 cells, 4,000,000 triangles, jitter 0.1, "
-                                   "p=1 SSP-RK2 Roe limiter wet/dry on, tide 0.5 m, CFL 0.3",
-                       "num_el": m.num_el},
+    m, st = make_workload(2, args.nx, args.ny, native=False)
+    warm = max(0, min(args.warmup, 1))
+    cb = cpu_baseline_reference(m, st, steps=max(1, args.steps), warmup=warm, max_seconds=args.ref_seconds,
+                                o3_steps=args.ref_o3_steps)
+    line = {"metric": METRIC, "value": cb["value"], "unit": METRIC, "n_gpus": args.gpus, "steps": cb["steps"],
+            "warmup": warm, "ms_per_step": cb["seconds"] * 1e3 / max(cb["steps"], 1), "impl": "reference",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args.nx, args.ny, m.num_el, m.num_edges, args.gpus),
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -600,9 +685,14 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=-1,
                     help="steps of the end-to-end run (default: --steps, the workload's length; 0: none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-seconds", type=float, default=90.0)
+    ap.add_argument("--ref-seconds", type=float, default=400.0,
+                    help="cap on the reference arm's timed steps (about 5 s per step at 4M triangles)")
+    ap.add_argument("--ref-o3-steps", type=int, default=3,
+                    help="steps of the -O3 -march=x86-64-v3 reference build timed beside the -O2 figure")
+    ap.add_argument("--cpu-steps", type=int, default=4,
+                    help="timed steps of the reference sample beside the device run (and of its parity check)")
     ap.add_argument("--ensemble-scenarios", type=int, default=256)
-    ap.add_argument("--ensemble-steps", type=int, default=100)
+    ap.add_argument("--ensemble-steps", type=int, default=1000)
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=4000)
     ap.add_argument("--adjoint-ckpt", type=int, default=100)
@@ -760,9 +850,14 @@ def main():
         except Exception as e:  # noqa: BLE001
             cpl = {"error": f"{type(e).__name__}: {e}"}
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_reference(m, st)
+        ref_final: dict = {}
+        cpu = cpu_baseline_reference(m, st, steps=args.cpu_steps, final=ref_final)
+        try:
+            parity = parity_vs_reference(m, st, solver, ref_final)
+        except Exception as e:  # noqa: BLE001
+            parity = {"error": f"{type(e).__name__}: {e}"}
 
     ens = None
     if not args.no_ensemble and args.ensemble_scenarios > 0:
@@ -786,12 +881,7 @@ def main():
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"coastal rectangle {args.nx}x{args.ny} cells (10 km x 5 km), "
-                                   f"{m.num_el:,} triangles, "
-                                   "jitter 0.1, p=1 CR/RT0, SSP-RK2, Roe, vertex limiter, wet/dry on, "
-                                   "tide 0.5 m / 12.42 h, Manning 0.03, CFL 0.3, FP64",
-                       "num_el": m.num_el, "num_edges": m.num_edges, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (state 288 MB, geometry 2 GB per replica); no flush"},
+            "config": workload_config(args.nx, args.ny, m.num_el, m.num_edges, world),
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": names[top], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
@@ -805,6 +895,8 @@ def main():
             "calibration": cal,
             "io": io,
             "coupling": cpl,
+            "parity": parity,
+            "headline": headline(ens, adj, cal),
         }
         print(json.dumps(line), flush=True)
     solver.close()

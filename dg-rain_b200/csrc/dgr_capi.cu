@@ -245,6 +245,8 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     if (c->p.order == 2) c->p2ref = make_p2_ref();
     c->bs = 128;
     c->fusion = 0;
+    c->bar_polls = kBarrierSpins;
+    c->bar_phantom = 0;
     if (c->device < 0 || c->device >= ndev) {
         release(c);
         return DGR_ERR_INVALID;
@@ -866,6 +868,8 @@ static FusedArgs fused_args(dgr_ctx *c)
     a.p = phys(c);
     a.dec = c->p.record_decisions ? c->dec : nullptr;
     a.bar = c->bar;
+    a.bar_polls = c->bar_polls;
+    a.bar_phantom = c->bar_phantom;
     return a;
 }
 
@@ -889,7 +893,9 @@ static cudaError_t launch_fused_bs(dgr_ctx *c, int stage_begin, int stage_end, i
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaMemsetAsync(c->bar, 0, 16, c->stream);
+    /* arrivals and generation start at zero; the time-out flag (bar[2]) is left alone, so a
+     * time-out of any launch of a run is still seen when the run ends */
+    e = cudaMemsetAsync(c->bar, 0, 8, c->stream);
     if (e != cudaSuccess) return e;
     return cudaLaunchKernelEx(&cfg, fn, a, stage_begin, stage_end, with_clock);
 }
@@ -1172,6 +1178,7 @@ static int run_impl(dgr_ctx *c, int nsteps, const double *final_time, double *ti
         r = build_graph(c);
         if (r) return r;
     }
+    if (c->fusion) CK(cudaMemsetAsync(c->bar + 2, 0, 4, s)); /* no barrier time-out yet */
     CK(cudaEventRecord(c->ev0, s));
     launch_wd_refresh(c);
     for (int i = 0; i < nsteps; ++i) {
@@ -1232,6 +1239,15 @@ extern "C" int dgr_ensemble_last_error(dgr_ctx *c, int scenario, int *code, int 
 extern "C" int dgr_last_error(dgr_ctx *c, int *code, int *index, int *step)
 {
     return dgr_ensemble_last_error(c, 0, code, index, step);
+}
+
+extern "C" int dgr_set_barrier_wait(dgr_ctx *c, unsigned max_polls, unsigned phantom_blocks)
+{
+    if (!c || max_polls == 0 || phantom_blocks > 1) return DGR_ERR_INVALID;
+    c->bar_polls = max_polls;
+    c->bar_phantom = phantom_blocks;
+    drop_graph(c); /* the captured launches hold the old values */
+    return DGR_OK;
 }
 
 extern "C" int dgr_set_schedule(dgr_ctx *c, int block_size, int fusion)

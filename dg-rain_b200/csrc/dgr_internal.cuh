@@ -76,6 +76,8 @@ struct dgr_ctx {
     int *wdA, *wdB, *wdC; /* wet/dry flags: stage s reads buffer s, writes buffer (s+1) mod stages */
     int *dec; /* [6][ne]: limit and pdop decisions of stage 0, 1, 2 */
     unsigned *bar;
+    unsigned bar_polls;   /* bound of a grid-barrier wait (dgr_set_barrier_wait) */
+    unsigned bar_phantom; /* phantom arrivals a barrier waits for (0 except in tests) */
     dgr::DevClock *clk;
     dgr::DevClock *h_clk; /* pinned mirror [nscen] */
     double *h_stage;

@@ -522,16 +522,20 @@ struct FusedArgs {
     PhysParams p;
     int *dec;         /* [4][ne] decisions, or nullptr */
     unsigned *bar;    /* [0] arrivals, [1] generation, [2] time-out flag */
+    unsigned bar_polls;   /* polls of a barrier wait before it gives up */
+    unsigned bar_phantom; /* blocks a barrier also waits for that never arrive (0; tests of the time-out) */
 };
 
 /* Polls of a grid-barrier wait before it gives up (about a second with the 64 ns sleeps). */
 constexpr unsigned kBarrierSpins = 1u << 24;
 
 /* Grid-wide barrier of a cooperative launch (every block resident).  The wait is bounded:
- * a block that polls kBarrierSpins times records a time-out, and every block leaves the
- * kernel at its next barrier check, so a broken invariant ends the launch with an error
- * flag instead of hanging the GPU.  Returns false once a time-out is recorded. */
-DGR_DEV bool grid_barrier(unsigned *bar)
+ * a block that polls `polls` times records a time-out, and every block leaves the kernel
+ * at its next barrier check, so a broken invariant ends the launch with an error flag
+ * instead of hanging the GPU.  `phantom` extra arrivals are expected on top of the grid's
+ * blocks: nonzero only to make the wait run out on purpose (a test of that path).
+ * Returns false once a time-out is recorded. */
+DGR_DEV bool grid_barrier(unsigned *bar, unsigned polls, unsigned phantom)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -539,14 +543,14 @@ DGR_DEV bool grid_barrier(unsigned *bar)
         const unsigned gen = *vgen;
         __threadfence();
         const unsigned arrived = atomicAdd(bar, 1u);
-        if (arrived == gridDim.x - 1) {
+        if (arrived == gridDim.x - 1 + phantom) {
             atomicExch(bar, 0u);
             __threadfence();
             atomicAdd(bar + 1, 1u);
         } else {
             unsigned spins = 0;
             while (*vgen == gen) {
-                if (++spins > kBarrierSpins) {
+                if (++spins > polls) {
                     atomicExch(bar + 2, 1u);
                     break;
                 }
@@ -573,7 +577,7 @@ __global__ void __launch_bounds__(BS, 512 / BS) k_step_fused(FusedArgs a, int st
     if (with_clock) {
         if (blockIdx.x == 0)
             clock_begin_body(a.clk, a.nscen, a.p, a.bnd_edges, a.bnd_type, a.bnd_sid, a.nbnd, a.bzeta, a.bqn);
-        if (!grid_barrier(a.bar)) return;
+        if (!grid_barrier(a.bar, a.bar_polls, a.bar_phantom)) return;
     }
     const int stride = gridDim.x * BS;
     const int ne = a.m.ne;
@@ -597,7 +601,7 @@ __global__ void __launch_bounds__(BS, 512 / BS) k_step_fused(FusedArgs a, int st
                       : 0.0;
             block_max_speed(lam, sid, valid, a.clk, stage);
         }
-        if (!grid_barrier(a.bar)) return;
+        if (!grid_barrier(a.bar, a.bar_polls, a.bar_phantom)) return;
         for (int el = blockIdx.x * BS + threadIdx.x; el < ne; el += stride) {
             if (mode == MODE_STAGE1)
                 element_item<MODE_STAGE1, true>(a.m, S, a.U, wd_in, a.flux, OUT, a.avg, a.clk, a.p.g, el);
@@ -608,14 +612,14 @@ __global__ void __launch_bounds__(BS, 512 / BS) k_step_fused(FusedArgs a, int st
             else
                 element_item<MODE_RK3_3, true>(a.m, S, a.U, wd_in, a.flux, OUT, a.avg, a.clk, a.p.g, el);
         }
-        if (!grid_barrier(a.bar)) return;
+        if (!grid_barrier(a.bar, a.bar_polls, a.bar_phantom)) return;
         for (int n = blockIdx.x * BS + threadIdx.x; n < a.m.nn; n += stride) node_item<true>(a.m, a.avg, a.bounds, n);
-        if (!grid_barrier(a.bar)) return;
+        if (!grid_barrier(a.bar, a.bar_polls, a.bar_phantom)) return;
         for (int el = blockIdx.x * BS + threadIdx.x; el < ne; el += stride)
             limit_item<true, WD, WD, true>(a.m, OUT, a.bounds, wd_in, wd_out, a.clk, a.p.h0, a.p.velzero,
                                            2 * stage + 1, dl, dp, el);
         if (stage + 1 < stage_end || with_clock)
-            if (!grid_barrier(a.bar)) return;
+            if (!grid_barrier(a.bar, a.bar_polls, a.bar_phantom)) return;
     }
     if (with_clock && blockIdx.x == 0)
         for (int sc = threadIdx.x; sc < a.nscen; sc += BS) clock_end_item<true>(a.clk, sc);

@@ -152,6 +152,7 @@ SIGNATURES = [
     ("dgr_ensemble_last_error", C.c_int, [C.c_void_p, C.c_int, iptr, iptr, iptr]),
     ("dgr_set_schedule", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     ("dgr_get_schedule", C.c_int, [C.c_void_p, iptr, iptr]),
+    ("dgr_set_barrier_wait", C.c_int, [C.c_void_p, C.c_uint, C.c_uint]),
     ("dgr_autotune", C.c_int, [C.c_void_p, C.c_int, iptr, iptr, dptr]),
     ("dgr_slope_limiter_noalloc", C.c_int,
      [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),

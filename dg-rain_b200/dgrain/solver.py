@@ -272,9 +272,15 @@ def _schedule_methods(cls):
         table = {(bs, fu): ms[3 * i + fu] for i, bs in enumerate((64, 128, 256)) for fu in range(3)}
         return b.value, f.value, table
 
+    def set_barrier_wait(self, max_polls: int = 1 << 24, phantom_blocks: int = 0) -> None:
+        """Bound of the persistent kernels' grid-barrier wait; phantom_blocks = 1 makes the
+        wait run out on purpose (DGR_ERR_TIMEOUT), a test of that path."""
+        _lib.check(self.lib.dgr_set_barrier_wait(self.ctx, max_polls, phantom_blocks), "dgr_set_barrier_wait")
+
     cls.set_schedule = set_schedule
     cls.get_schedule = get_schedule
     cls.autotune = autotune
+    cls.set_barrier_wait = set_barrier_wait
     return cls
 
 

@@ -271,6 +271,14 @@ DGR_API int dgr_ensemble_last_error(dgr_ctx *ctx, int scenario, int *code, int *
  * 3*b + f, b = 0,1,2 for 64,128,256.  Results do not depend on the schedule. */
 DGR_API int dgr_set_schedule(dgr_ctx *ctx, int block_size, int fusion);
 DGR_API int dgr_get_schedule(const dgr_ctx *ctx, int *block_size, int *fusion);
+/* Bound of the persistent kernels' grid-barrier wait (fusion 1 and 2): a block that polls
+ * max_polls times (default 2^24, about a second) gives up, every block leaves the launch
+ * and the call returns DGR_ERR_TIMEOUT; the context stays usable.  No counterpart in the
+ * reference, which has no device waits; it replaces the hang such a wait could cause by a
+ * status, as the reference's failures (2DCode/compute2DL.c:245-302) become statuses here.
+ * phantom_blocks = 1 makes every barrier also wait for a block that never arrives, so the
+ * wait runs out on purpose: a test of the time-out path that faults nothing (0: normal). */
+DGR_API int dgr_set_barrier_wait(dgr_ctx *ctx, unsigned max_polls, unsigned phantom_blocks);
 DGR_API int dgr_autotune(dgr_ctx *ctx, int trial_steps, int *block_size, int *fusion, double *ms_out);
 
 /* First failure since the last upload: status code, edge or element index, step. */

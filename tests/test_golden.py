@@ -53,3 +53,35 @@ def test_oracle_failure_golden(dgrain, oracle_mod):
     code, idx = orc.last_error()
     assert rc == code == 1
     assert idx == int(g["fail_edge"]) and n == int(g["steps_done"])
+
+
+def test_numpy_mesh_setup_golden(dgrain):
+    """The oracle's numpy mesh set-up (oracle/mesh_setup.py, used where the reference step
+    runs on meshes too large for its own set-up) gives the arrays the reference wrote."""
+    from oracle import mesh_setup
+
+    for name in ("compute2DL_jittered576.npz", "run120_wd_tide_rect1600.npz"):
+        g = load_golden(name)
+        ed2v, ed2el, bdry, min_edge = mesh_setup.connectivity(g["el2v"], g["x"], g["y"], g["inflow1"],
+                                                              g["inflow2"], g["outflow"])
+        assert bits_equal(ed2v, g["ed2v"]) and bits_equal(ed2el, g["ed2el"]) and bits_equal(bdry, g["bdry"]), name
+        assert min_edge == float(g["min_edge"]), name
+
+
+@pytest.mark.parametrize("nx,ny,jitter,seed", [(40, 20, 0.0, 1), (57, 31, 0.1, 4), (200, 100, 0.1, 2)])
+def test_numpy_mesh_setup_equals_native_builder(dgrain, nx, ny, jitter, seed):
+    """The numpy set-up against the library's hashed builder and initial state, with every
+    boundary type present."""
+    from oracle import mesh_setup
+
+    m = dgrain.rectangle(nx, ny, jitter=jitter, seed=seed, connect=False)
+    bottom = np.stack([np.arange(nx), np.arange(1, nx + 1)], 1).astype(np.int32)
+    m.inflow1 = np.ascontiguousarray(bottom[: nx // 2])
+    m.inflow2 = np.ascontiguousarray(np.concatenate([bottom[nx // 2:], bottom[:2]]))
+    dgrain.build_connectivity(m)
+    ed2v, ed2el, bdry, min_edge = mesh_setup.connectivity(m.el2v, m.x, m.y, m.inflow1, m.inflow2, m.outflow)
+    assert bits_equal(ed2v, m.ed2v) and bits_equal(ed2el, m.ed2el) and bits_equal(bdry, m.bdry)
+    assert min_edge == m.min_edge
+    zn = np.maximum(0.0, 0.5e-3 - m.z)
+    for a, b in zip(mesh_setup.initial_state(m.el2v, zn), dgrain.initial_state(m, zn)):
+        assert bits_equal(a, b)

@@ -249,6 +249,35 @@ def test_large_mesh_one_step(dgrain, oracle_mod):
         assert rel_err(a, b) <= RTOL_RUN
 
 
+@pytest.mark.parametrize("friction", [False, True])
+def test_million_triangle_wet_dry_run(dgrain, oracle_mod, friction):
+    """Six wet/dry steps with the tide on the benchmark's generator at 1,000,000 triangles
+    (1,000 x 500 cells, jitter 0.1, land film H0/2, CFL 0.3), device loop against the
+    oracle: the same clock and wet/dry flags; without friction the state bit for bit, with
+    Manning n = 0.03 within RTOL_RUN of each field's largest magnitude."""
+    m = dgrain.rectangle(1000, 500, jitter=0.1, seed=2)
+    if not friction:
+        m = no_friction(dgrain, m)
+    st = land_film_state(dgrain, m)
+    s, o = make_pair(dgrain, oracle_mod, m, st, 1, cfl=0.3, tide_on=1, tide_amp=0.5)
+    rc, t_o, dt_o, n_o, _ = o.run(6, 1e9, 0.3, wet_dry=1, tide_on=1, amp=0.5)
+    assert rc == 0 and n_o == 6
+    t, dt, n = s.time_evolution(1e9, 6)
+    assert n == 6
+    # the clock follows the max wave speed, which friction's last-bit differences can move
+    assert t == t_o if not friction else abs(t - t_o) <= RTOL_RUN * abs(t_o)
+    gs, os_ = s.download_state(), o.get_state()
+    assert same(gs[3], os_[3])
+    for a, b in zip(gs[:3], os_[:3]):
+        if friction:
+            assert rel_err(a, b) <= RTOL_RUN
+        else:
+            assert same(a, b)
+    if not friction:
+        assert dt == dt_o
+    s.close()
+
+
 def test_manning_power_correctly_rounded(dgrain):
     """The device x^(4./3) against 60-digit decimal values rounded once to double."""
     import ctypes as C

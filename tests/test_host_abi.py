@@ -105,6 +105,7 @@ def test_coupling_entry_points_check_their_arguments(dgrain):
     assert lib.dgr_get_boundary(None, d, d) == inv
     p = C.c_void_p()
     assert lib.dgr_get_stream(None, C.byref(p)) == inv
+    assert lib.dgr_set_barrier_wait(None, 1000, 0) == inv
 
 
 def test_pointer_rule_of_the_device_buffer_entry_points(tmp_path):

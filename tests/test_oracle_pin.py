@@ -44,6 +44,13 @@ def test_connectivity_matches_reference(dgrain, oracle_mod, tmp_path, jitter, se
         assert _same(getattr(m2, k), rm[k]), k
     assert m.min_edge == rm["min_edge"] == m2.min_edge
     assert set(np.unique(m.bdry)) == {0, 1, 2, 3}
+    # the numpy restatement that lets the reference step run on meshes too large for its
+    # own set-up (bench.py's reference arm)
+    from oracle import mesh_setup
+
+    ed2v, ed2el, bdry, min_edge = mesh_setup.connectivity(m.el2v, m.x, m.y, m.inflow1, m.inflow2, m.outflow)
+    assert _same(ed2v, rm["ed2v"]) and _same(ed2el, rm["ed2el"]) and _same(bdry, rm["bdry"])
+    assert min_edge == rm["min_edge"]
 
 
 def _pair(dgrain, oracle_mod, mesh, wet_dry, state):
