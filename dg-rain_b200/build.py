@@ -1,8 +1,10 @@
 """Build recipe of the native library libdgrain.so (C host code + sm_100a CUDA kernels).
 
     python dg-rain_b200/build.py            # builds dg-rain_b200/dgrain/libdgrain.so
+    python dg-rain_b200/build.py --checked  # ... libdgrain_checked.so (-DDGR_CHECKED)
 
 The library is built in-tree so that it travels with the repository to the GPU host.
+
 Flags: sm_100a only; --fmad=false keeps every multiply and add a separately rounded IEEE
 operation so that the kernels reproduce the reference C step's arithmetic.
 """
@@ -59,10 +61,10 @@ def _run(cmd: list[str], verbose: bool) -> None:
 
 
 def build(verbose: bool = False, ptxas_verbose: bool = False, force: bool = False, out: str | None = None,
-          defines: list[str] | None = None) -> str:
+          defines: list[str] | None = None, build_dir: str | None = None) -> str:
     """Build libdgrain.so (or `out`, with extra -D `defines`, for tuning sweeps)."""
     lib = out or LIB
-    build_dir = BUILD if out is None else out + ".build"
+    build_dir = build_dir or (BUILD if out is None else out + ".build")
     os.makedirs(build_dir, exist_ok=True)
     dflags = [f"-D{d}" for d in (defines or [])]
     nvcc = _nvcc()
@@ -85,6 +87,20 @@ def build(verbose: bool = False, ptxas_verbose: bool = False, force: bool = Fals
     return lib
 
 
+CHECKED_LIB = os.path.join(OUT_DIR, "libdgrain_checked.so")
+
+
+def build_checked(verbose: bool = False, force: bool = False) -> str:
+    """The checked build: the same sources with -DDGR_CHECKED (every index a kernel gathers
+    from the connectivity is tested; see dgr_kernels.cuh), loaded by the package when
+    DGRAIN_LIBRARY=checked."""
+    return build(verbose=verbose, force=force, out=CHECKED_LIB, defines=["DGR_CHECKED"],
+                 build_dir=os.path.join(HERE, "_build_checked"))
+
+
 if __name__ == "__main__":
-    path = build(verbose=True, ptxas_verbose="-v" in sys.argv, force="-f" in sys.argv)
-    print(path)
+    if "--checked" in sys.argv:
+        print(build_checked(verbose=True, force="-f" in sys.argv))
+    else:
+        path = build(verbose=True, ptxas_verbose="-v" in sys.argv, force="-f" in sys.argv)
+        print(path)

@@ -264,6 +264,7 @@ static int start_clock(dgr_ctx *c, double time, double dt)
 extern "C" int dgr_adjoint_forward(dgr_ctx *c, const double *zeta, const double *Qx, const double *Qy, const int *WD,
                                    double time, double dt, int replay_dt, double *J, double *gauge_values)
 {
+    NvtxRange nv("dgr_adjoint_forward");
     if (!c || !c->adj || !zeta || !Qx || !Qy || !WD) return DGR_ERR_INVALID;
     AdjointState *a = c->adj;
     if (replay_dt && !a->have_forward) return DGR_ERR_INVALID;
@@ -505,6 +506,7 @@ static int to_reference_layout(dgr_ctx *c, const double *planar, double *zeta, d
 extern "C" int dgr_adjoint_backward(dgr_ctx *c, double *grad_n_el, double *grad_z, double *grad_zeta0,
                                     double *grad_Qx0, double *grad_Qy0)
 {
+    NvtxRange nv("dgr_adjoint_backward");
     if (!c || !c->adj || !c->adj->have_forward) return DGR_ERR_INVALID;
     AdjointState *a = c->adj;
     CK(cudaSetDevice(c->device));
@@ -743,6 +745,7 @@ extern "C" int dgr_tlm(dgr_ctx *c, const double *zeta, const double *Qx, const d
                        const double *dzeta0, const double *dQx0, const double *dQy0, const double *dn_el,
                        const double *dz, double *J, double *dJ)
 {
+    NvtxRange nv("dgr_tlm");
     if (!c || !c->adj || !c->adj->have_forward || !zeta || !Qx || !Qy || !WD) return DGR_ERR_INVALID;
     AdjointState *a = c->adj;
     CK(cudaSetDevice(c->device));
@@ -772,6 +775,7 @@ extern "C" int dgr_fd_frozen(dgr_ctx *c, const double *zeta, const double *Qx, c
                              const double *zeta_p, const double *Qx_p, const double *Qy_p, const double *n_el_p,
                              const double *z_p, double *J, double *J_p)
 {
+    NvtxRange nv("dgr_fd_frozen");
     if (!c || !c->adj || !c->adj->have_forward || !zeta || !Qx || !Qy || !WD) return DGR_ERR_INVALID;
     AdjointState *a = c->adj;
     CK(cudaSetDevice(c->device));

@@ -305,7 +305,7 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     TRY(dalloc(&c->wdB, ne));
     TRY(dalloc(&c->wdC, ne));
     TRY(dalloc(&c->dec, 6 * ne));
-    TRY(dalloc(&c->bar, 4));
+    TRY(dalloc(&c->bar, 6)); /* barrier words [0..2]; [4..5] the checked build's bad-index word */
     TRY(dalloc(&c->clk, nscen));
     TRYC(cudaHostAlloc((void **)&c->h_clk, sizeof(DevClock) * nscen, cudaHostAllocDefault));
 
@@ -335,6 +335,7 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     TRYC(cudaMemsetAsync(c->W, 0, nst * lE * 8, s));
     TRYC(cudaMemsetAsync(c->dec, 0, 6 * ne * 4, s));
     TRYC(cudaMemsetAsync(c->bar, 0, 16, s));
+    TRYC(cudaMemsetAsync(c->bar + 4, 0xff, 8, s));
 
     /* per-element Manning n of the scenarios that give one (negative: node average) */
     bool any_nel = false;
@@ -609,6 +610,7 @@ int upload_scenarios(dgr_ctx *c, int s0, int s1, const double *zeta, const doubl
     }
     r = write_clock(c);
     if (r) return r;
+    CK(cudaMemsetAsync(c->bar + 4, 0xff, 8, c->stream)); /* no bad index recorded */
     c->wd_fresh = 0;
     c->wd_stepped = 0;
     return DGR_OK;
@@ -650,6 +652,30 @@ extern "C" int dgr_download_state(dgr_ctx *c, double *zeta, double *Qx, double *
 {
     if (!c || c->nscen != 1) return DGR_ERR_INVALID;
     return download_slice(c, 0, zeta, Qx, Qy, WD);
+}
+
+extern "C" int dgr_save_restart(dgr_ctx *c, const char *path, double time, double dt)
+{
+    NvtxRange nv("dgr_save_restart");
+    if (!c || c->nscen != 1 || !path) return DGR_ERR_INVALID;
+    const size_t n = (size_t)c->nm * c->ne;
+    std::vector<double> st(3 * n);
+    std::vector<int> wd(c->ne);
+    int r = download_slice(c, 0, st.data(), st.data() + n, st.data() + 2 * n, wd.data());
+    if (r) return r;
+    return dgr_write_restart(path, c->ne, c->nm, st.data(), st.data() + n, st.data() + 2 * n, wd.data(), time, dt);
+}
+
+extern "C" int dgr_load_restart(dgr_ctx *c, const char *path, double *time, double *dt)
+{
+    NvtxRange nv("dgr_load_restart");
+    if (!c || c->nscen != 1 || !path || !time || !dt) return DGR_ERR_INVALID;
+    const size_t n = (size_t)c->nm * c->ne;
+    std::vector<double> st(3 * n);
+    std::vector<int> wd(c->ne);
+    int r = dgr_read_restart(path, c->ne, c->nm, st.data(), st.data() + n, st.data() + 2 * n, wd.data(), time, dt);
+    if (r) return r;
+    return upload_slice(c, 0, st.data(), st.data() + n, st.data() + 2 * n, wd.data());
 }
 
 extern "C" int dgr_ensemble_upload_state(dgr_ctx *c, int scenario, const double *zeta, const double *Qx,
@@ -817,18 +843,30 @@ void launch_stage(dgr_ctx *c, int stage, bool count)
     const StageIO io = stage_io(c, stage);
     int *dl = c->p.record_decisions ? c->dec + (size_t)(2 * stage) * c->ne : nullptr;
     int *dp = c->p.record_decisions ? c->dec + (size_t)(2 * stage + 1) * c->ne : nullptr;
-    launch_edge(c, io.S, io.wd_in, stage, 2 * stage);
-    switch (io.mode) {
-    case MODE_STAGE1: launch_element<MODE_STAGE1>(c, io.S, io.wd_in, io.OUT); break;
-    case MODE_STAGE2: launch_element<MODE_STAGE2>(c, io.S, io.wd_in, io.OUT); break;
-    case MODE_RK3_2: launch_element<MODE_RK3_2>(c, io.S, io.wd_in, io.OUT); break;
-    default: launch_element<MODE_RK3_3>(c, io.S, io.wd_in, io.OUT);
+    {
+        NvtxRange r("k_edge_flux");
+        launch_edge(c, io.S, io.wd_in, stage, 2 * stage);
     }
-    k_node_bounds<<<blocks(c->nn, 256), 256, 0, c->stream>>>(mesh_dev(c), c->avg, c->bounds);
-    if (wd)
-        launch_limit<true, true, true>(c, io.OUT, io.wd_in, io.wd_out, 2 * stage + 1, dl, dp);
-    else
-        launch_limit<true, false, false>(c, io.OUT, io.wd_in, io.wd_out, 2 * stage + 1, dl, dp);
+    {
+        NvtxRange r("k_element");
+        switch (io.mode) {
+        case MODE_STAGE1: launch_element<MODE_STAGE1>(c, io.S, io.wd_in, io.OUT); break;
+        case MODE_STAGE2: launch_element<MODE_STAGE2>(c, io.S, io.wd_in, io.OUT); break;
+        case MODE_RK3_2: launch_element<MODE_RK3_2>(c, io.S, io.wd_in, io.OUT); break;
+        default: launch_element<MODE_RK3_3>(c, io.S, io.wd_in, io.OUT);
+        }
+    }
+    {
+        NvtxRange r("k_node_bounds");
+        k_node_bounds<<<blocks(c->nn, 256), 256, 0, c->stream>>>(mesh_dev(c), c->avg, c->bounds);
+    }
+    {
+        NvtxRange r("k_limit");
+        if (wd)
+            launch_limit<true, true, true>(c, io.OUT, io.wd_in, io.wd_out, 2 * stage + 1, dl, dp);
+        else
+            launch_limit<true, false, false>(c, io.OUT, io.wd_in, io.wd_out, 2 * stage + 1, dl, dp);
+    }
     if (count) c->launches += 4;
 }
 
@@ -968,8 +1006,22 @@ int decode_err(unsigned long long key, int *code, int *index, int *step)
     return cd;
 }
 
+/* Checked build: the first out-of-range gather recorded by the kernels, as
+ * (kernel << 32 | item), or ~0. */
+static unsigned long long bad_index(const dgr_ctx *c)
+{
+    unsigned long long bad = ~0ull;
+#ifdef DGR_CHECKED
+    if (cudaMemcpy(&bad, c->bar + 4, 8, cudaMemcpyDeviceToHost) != cudaSuccess) bad = ~0ull;
+#else
+    (void)c;
+#endif
+    return bad;
+}
+
 int first_error(const dgr_ctx *c)
 {
+    if (bad_index(c) != ~0ull) return DGR_ERR_BAD_INDEX;
     for (int k = 0; k < c->nscen; ++k) {
         const int cd = decode_err(c->h_clk[k].err, nullptr, nullptr, nullptr);
         if (cd) return cd;
@@ -987,6 +1039,7 @@ static int check_barrier(dgr_ctx *c)
 
 extern "C" int dgr_step(dgr_ctx *c, double time, double dt, double *max_lambda)
 {
+    NvtxRange nv("dgr_step");
     if (!c || c->nscen != 1) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
@@ -1153,6 +1206,7 @@ static int build_graph(dgr_ctx *c)
 static int run_impl(dgr_ctx *c, int nsteps, const double *final_time, double *time_io, double *dt_io,
                     int *steps_done)
 {
+    NvtxRange nv("dgr_run");
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     int r = read_clock(c);
@@ -1233,6 +1287,12 @@ extern "C" int dgr_ensemble_last_error(dgr_ctx *c, int scenario, int *code, int 
     int r = read_clock(c);
     if (r) return r;
     decode_err(c->h_clk[scenario].err, code, index, step);
+    const unsigned long long bad = bad_index(c);
+    if (bad != ~0ull) { /* checked build: the item and, in place of the step, the kernel */
+        if (code) *code = DGR_ERR_BAD_INDEX;
+        if (index) *index = (int)(bad & 0xffffffffu);
+        if (step) *step = (int)(bad >> 32);
+    }
     return DGR_OK;
 }
 
@@ -1338,6 +1398,7 @@ static int autotune_trials(dgr_ctx *c, int trial_steps, double *saveU, int *save
 
 extern "C" int dgr_autotune(dgr_ctx *c, int trial_steps, int *block_size, int *fusion, double *ms_out)
 {
+    NvtxRange nv("dgr_autotune");
     if (!c || trial_steps <= 0) return DGR_ERR_INVALID;
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;

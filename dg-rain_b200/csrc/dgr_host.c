@@ -417,6 +417,95 @@ int dgr_write_dat(const char *path, int ne, const double *v)
     return fclose(f) == 0 ? DGR_OK : DGR_ERR_IO;
 }
 
+/* ---------------------------------------------------------------- restart ---- */
+
+/* Restart file: the .dat row layout of the state (one element per line, tab-separated,
+ * 2DCode/time_evolution.c:284-306) with every value printed with 17 significant digits,
+ * which strtod reads back to the same double (signed zeros included), followed by the
+ * element's wet/dry flag; a three-line header gives the format, the sizes and the clock.
+ *
+ *   DG-RAIN restart 1
+ *   <num_el> <nm>
+ *   time <t> dt <dt>
+ *   z_0 .. z_{nm-1}  Qx_0 .. Qx_{nm-1}  Qy_0 .. Qy_{nm-1}  WD      (num_el lines)
+ */
+static const char RESTART_MAGIC[] = "DG-RAIN restart 1";
+
+int dgr_write_restart(const char *path, int ne, int nm, const double *zeta, const double *qx, const double *qy,
+                      const int *wd, double time, double dt)
+{
+    if (!path || ne <= 0 || nm <= 0 || !zeta || !qx || !qy || !wd) return DGR_ERR_INVALID;
+    FILE *f = fopen(path, "w");
+    if (!f) return DGR_ERR_IO;
+    fprintf(f, "%s\n%d %d\ntime %.17g dt %.17g\n", RESTART_MAGIC, ne, nm, time, dt);
+    const double *vars[3] = {zeta, qx, qy};
+    for (int j = 0; j < ne; ++j) {
+        for (int v = 0; v < 3; ++v)
+            for (int k = 0; k < nm; ++k) fprintf(f, "%.17g\t\t", vars[v][(size_t)nm * j + k]);
+        fprintf(f, "%d\n", wd[j]);
+    }
+    return fclose(f) == 0 ? DGR_OK : DGR_ERR_IO;
+}
+
+/* reads one whitespace-separated number; 0 on success */
+static int next_double(char **p, double *out)
+{
+    char *q;
+    *out = strtod(*p, &q);
+    if (q == *p) return 1;
+    *p = q;
+    return 0;
+}
+
+int dgr_read_restart(const char *path, int ne, int nm, double *zeta, double *qx, double *qy, int *wd,
+                     double *time, double *dt)
+{
+    if (!path || ne <= 0 || nm <= 0 || !zeta || !qx || !qy || !wd || !time || !dt) return DGR_ERR_INVALID;
+    FILE *f = fopen(path, "r");
+    if (!f) return DGR_ERR_IO;
+    int rc = DGR_ERR_IO;
+    size_t cap = 64 + 3 * (size_t)nm * 32;
+    char *line = (char *)malloc(cap);
+    if (!line) {
+        fclose(f);
+        return DGR_ERR_TOO_LARGE;
+    }
+    int fne = 0, fnm = 0;
+    if (!fgets(line, (int)cap, f) || strncmp(line, RESTART_MAGIC, sizeof RESTART_MAGIC - 1) != 0) goto done;
+    if (!fgets(line, (int)cap, f) || sscanf(line, "%d %d", &fne, &fnm) != 2) goto done;
+    if (fne != ne || fnm != nm) {
+        rc = DGR_ERR_MESH; /* written for another mesh or order */
+        goto done;
+    }
+    {
+        char *p = line;
+        if (!fgets(line, (int)cap, f) || strncmp(p, "time", 4) != 0) goto done;
+        p += 4;
+        if (next_double(&p, time)) goto done;
+        while (*p == ' ' || *p == '\t') ++p;
+        if (strncmp(p, "dt", 2) != 0) goto done;
+        p += 2;
+        if (next_double(&p, dt)) goto done;
+    }
+    double *vars[3] = {zeta, qx, qy};
+    for (int j = 0; j < ne; ++j) {
+        if (!fgets(line, (int)cap, f)) goto done;
+        char *p = line;
+        for (int v = 0; v < 3; ++v)
+            for (int k = 0; k < nm; ++k)
+                if (next_double(&p, &vars[v][(size_t)nm * j + k])) goto done;
+        char *q;
+        const long w = strtol(p, &q, 10);
+        if (q == p || w < -1 || w > 1) goto done;
+        wd[j] = (int)w;
+    }
+    rc = DGR_OK;
+done:
+    free(line);
+    fclose(f);
+    return rc;
+}
+
 const char *dgr_status_string(int code)
 {
     switch (code) {
@@ -427,6 +516,7 @@ const char *dgr_status_string(int code)
     case DGR_ERR_NEG_DEPTH: return "water height negative during wetting and drying treatment";
     case DGR_ERR_NAN_VELOCITY: return "WD-modified velocity NaN";
     case DGR_ERR_EDGE_MATCH: return "local edge number not found";
+    case DGR_ERR_BAD_INDEX: return "connectivity index out of range (checked build)";
     case DGR_ERR_INVALID: return "invalid argument";
     case DGR_ERR_MESH: return "inconsistent mesh";
     case DGR_ERR_IO: return "file i/o error";

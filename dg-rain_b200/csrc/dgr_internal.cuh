@@ -11,6 +11,8 @@
 #include <cstring>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/dgrain.h"
 #include "dgr_kernels.cuh"
 #include "dgr_p2.cuh"
@@ -103,6 +105,16 @@ struct dgr_ctx {
     double *cpl_io, *h_cpl_io;                    /* [4][nends] in/out, and its pinned mirror */
 };
 
+/* NVTX range over a host-side phase or launch (a timeline tool shows it by name; with no
+ * tool attached the calls return at once).  Kernels replayed from a CUDA graph are
+ * covered by the range of the call that replays the graph. */
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
 static inline dgr::MeshDev mesh_dev(const dgr_ctx *c)
 {
     dgr::MeshDev m;
@@ -125,6 +137,7 @@ static inline dgr::MeshDev mesh_dev(const dgr_ctx *c)
     m.el_sid = c->el_sid;
     m.ed_sid = c->ed_sid;
     m.flux = c->p.flux;
+    m.bad_index = reinterpret_cast<unsigned long long *>(c->bar + 4);
     return m;
 }
 

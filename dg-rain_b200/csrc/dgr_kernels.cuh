@@ -78,7 +78,25 @@ struct MeshDev {
     const int *el_sid;    /* scenario of each element, NULL for a single mesh */
     const int *ed_sid;    /* scenario of each edge, NULL for a single mesh */
     int flux;             /* numerical flux: 0 Roe (2DCode), 1 local Lax-Friedrichs, 2 HLLC (DG-SWEM) */
+    unsigned long long *bad_index; /* checked build: first out-of-range gather, (kernel << 32 | item) */
 };
+
+/* Checked build (compiled with -DDGR_CHECKED): every index a kernel gathers from the
+ * connectivity arrays is tested against its range before it is used; one out of range is
+ * recorded in the context's bad-index word (the least (kernel << 32 | item) wins) and the
+ * item skips its work, so a broken array becomes DGR_ERR_BAD_INDEX instead of a read or
+ * write outside an array.  Without DGR_CHECKED the test compiles to nothing. */
+enum { KID_EDGE = 1, KID_ELEMENT = 2, KID_NODE = 3, KID_LIMIT = 4 };
+#ifdef DGR_CHECKED
+DGR_DEV bool index_ok(const MeshDev &m, int idx, int n, int kernel, int item)
+{
+    if ((unsigned)idx < (unsigned)n) return true;
+    atomicMin(m.bad_index, ((unsigned long long)kernel << 32) | (unsigned)item);
+    return false;
+}
+#else
+DGR_DEV constexpr bool index_ok(const MeshDev &, int, int, int, int) { return true; }
+#endif
 
 struct PhysParams {
     double g, h0, velzero, cfl, dt0;
@@ -115,6 +133,9 @@ DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, 
     if (!ldm<COH>(&ck->done)) {
         const int el_in = m.e_in[i], el_ex = m.e_ex[i], info = m.e_info[i];
         const int k_in = info & 3, k_ex = (info >> 2) & 3, bd = (info >> 4) & 7;
+        if (!(index_ok(m, el_in, m.ne, KID_EDGE, i) && index_ok(m, el_ex, m.ne, KID_EDGE, i) &&
+              index_ok(m, k_in, 3, KID_EDGE, i) && index_ok(m, k_ex, 3, KID_EDGE, i)))
+            return 0.0;
         const double nx = m.e_geo[i], ny = m.e_geo[m.ldF + i], z_edge = m.e_geo[2 * m.ldF + i];
         const int ld = m.ldE;
         const double zi = ldm<COH>(&S[k_in * ld + el_in]), qxi = ldm<COH>(&S[(3 + k_in) * ld + el_in]),
@@ -195,19 +216,21 @@ __global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, con
 /* Gathered numerical fluxes of one element's three edges, sign flipped on the "ex" side
  * (2DCode/2DInnerProducts.c:319-329).  F[variable][local edge]. */
 template <bool COH>
-DGR_DEV void gather_flux(const MeshDev &m, const double *flux, int el, double F[3][3])
+DGR_DEV bool gather_flux(const MeshDev &m, const double *flux, int el, double F[3][3])
 {
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const int ee = m.elem_edge[k * m.ldE + el];
         const int e = ee >> 1;
         const int side = ee & 1;
+        if (!index_ok(m, e, m.nf, KID_ELEMENT, el)) return false;
 #pragma unroll
         for (int v = 0; v < 3; ++v) {
             const double f = ldm<COH>(&flux[(3 * side + v) * m.ldF + e]);
             F[v][k] = side ? -f : f;
         }
     }
+    return true;
 }
 
 /* One element of the RHS / RK stage (element_core); S is the stage input, U the step
@@ -222,7 +245,7 @@ DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, co
     const int ld = m.ldE;
     const double *G = m.geo + el;
     double F[3][3];
-    gather_flux<COH>(m, flux, el, F);
+    if (!gather_flux<COH>(m, flux, el, F)) return;
     double zr[3], qxr[3], qyr[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -267,8 +290,12 @@ DGR_DEV void node_item(const MeshDev &m, const double *avg, double *bounds, int 
 {
     double mx0 = -99999, mx1 = -99999, mx2 = -99999, mn0 = 99999, mn1 = 99999, mn2 = 99999;
     const int b = m.n2e_ptr[n], e = m.n2e_ptr[n + 1];
+    if (!(index_ok(m, b, 3 * m.ne + 1, KID_NODE, n) && index_ok(m, e, 3 * m.ne + 1, KID_NODE, n) &&
+          index_ok(m, e - b, 3 * m.ne + 1, KID_NODE, n)))
+        return;
     for (int j = b; j < e; ++j) {
         const int el = m.n2e[j];
+        if (!index_ok(m, el, m.ne, KID_NODE, n)) return;
         const double a0 = ldm<COH>(&avg[el]), a1 = ldm<COH>(&avg[m.ldE + el]), a2 = ldm<COH>(&avg[2 * m.ldE + el]);
         if (a0 < mn0) mn0 = a0;
         if (a0 > mx0) mx0 = a0;
@@ -333,6 +360,9 @@ DGR_DEV void limit_item(const MeshDev &m, double *S, const double *bounds, const
     if (ldm<COH>(&ck->done)) return;
     const int ld = m.ldE;
     const int nd[3] = {m.el2v[el], m.el2v[ld + el], m.el2v[2 * ld + el]};
+    if (!(index_ok(m, nd[0], m.nn, KID_LIMIT, el) && index_ok(m, nd[1], m.nn, KID_LIMIT, el) &&
+          index_ok(m, nd[2], m.nn, KID_LIMIT, el)))
+        return;
     const double zn[3] = {m.zn[nd[0]], m.zn[nd[1]], m.zn[nd[2]]};
     double w[3][3];
 #pragma unroll

@@ -9,7 +9,10 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libdgrain.so")
+# DGRAIN_LIBRARY=checked selects the build whose kernels test every gathered index
+# (libdgrain_checked.so, compiled with -DDGR_CHECKED by build.py --checked)
+LIB_PATH = os.path.join(_HERE, "libdgrain_checked.so" if os.environ.get("DGRAIN_LIBRARY") == "checked"
+                        else "libdgrain.so")
 
 DGR_OK = 0
 DGR_ERR_NAN_FLUX = 1
@@ -18,6 +21,7 @@ DGR_ERR_NAN_FLUX_EX = 3
 DGR_ERR_NEG_DEPTH = 4
 DGR_ERR_NAN_VELOCITY = 5
 DGR_ERR_EDGE_MATCH = 6
+DGR_ERR_BAD_INDEX = 7
 DGR_ERR_INVALID = 10
 DGR_ERR_MESH = 11
 DGR_ERR_IO = 12
@@ -152,6 +156,10 @@ SIGNATURES = [
     ("dgr_ensemble_last_error", C.c_int, [C.c_void_p, C.c_int, iptr, iptr, iptr]),
     ("dgr_set_schedule", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     ("dgr_get_schedule", C.c_int, [C.c_void_p, iptr, iptr]),
+    ("dgr_write_restart", C.c_int, [C.c_char_p, C.c_int, C.c_int, dptr, dptr, dptr, iptr, C.c_double, C.c_double]),
+    ("dgr_read_restart", C.c_int, [C.c_char_p, C.c_int, C.c_int, dptr, dptr, dptr, iptr, dptr, dptr]),
+    ("dgr_save_restart", C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_double]),
+    ("dgr_load_restart", C.c_int, [C.c_void_p, C.c_char_p, dptr, dptr]),
     ("dgr_set_barrier_wait", C.c_int, [C.c_void_p, C.c_uint, C.c_uint]),
     ("dgr_autotune", C.c_int, [C.c_void_p, C.c_int, iptr, iptr, dptr]),
     ("dgr_slope_limiter_noalloc", C.c_int,

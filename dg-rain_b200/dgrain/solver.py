@@ -122,6 +122,17 @@ class Solver:
         _lib.check(self.lib.dgr_get_gauge_series(self.ctx, _dp(out)), "dgr_get_gauge_series")
         return out
 
+    def save_restart(self, path, time: float, dt: float) -> None:
+        """state, wet/dry flags and clock (time, next dt) to a restart file (dgr_save_restart)"""
+        _lib.check(self.lib.dgr_save_restart(self.ctx, str(path).encode(), time, dt), "dgr_save_restart")
+
+    def load_restart(self, path):
+        """a restart file into this context; returns (time, dt) to continue with"""
+        t, d = C.c_double(), C.c_double()
+        _lib.check(self.lib.dgr_load_restart(self.ctx, str(path).encode(), C.byref(t), C.byref(d)),
+                   "dgr_load_restart")
+        return t.value, d.value
+
     def write_state_dat(self, zeta_path=None, qx_path=None, qy_path=None) -> None:
         """the current state as the reference's .dat snapshot files, formatted on the device"""
         enc = lambda p: None if p is None else str(p).encode()  # noqa: E731
@@ -184,7 +195,7 @@ class Solver:
     def _status(self, rc: int, where: str) -> None:
         if rc == _lib.DGR_OK:
             return
-        if 1 <= rc <= 6:
+        if 1 <= rc <= 7:
             code, index, step = C.c_int(), C.c_int(), C.c_int()
             self.lib.dgr_last_error(self.ctx, C.byref(code), C.byref(index), C.byref(step))
             raise StepError(code.value, index.value, step.value, where)
@@ -364,8 +375,8 @@ class Ensemble:
         d = np.zeros(self.n) if dt is None else np.ascontiguousarray(dt, dtype=np.float64).copy()
         steps = np.zeros(self.n, dtype=np.int32)
         rc = self.lib.dgr_ensemble_run(self.ctx, nsteps, _dp(fin), _dp(t), _dp(d), _ip(steps))
-        if rc != _lib.DGR_OK and (check or not 1 <= rc <= 6):
-            if 1 <= rc <= 6:
+        if rc != _lib.DGR_OK and (check or not 1 <= rc <= 7):
+            if 1 <= rc <= 7:
                 for s in range(self.n):
                     code, index, step = self.last_error(s)
                     if code:
@@ -419,7 +430,7 @@ class Ensemble:
     def _status(self, rc: int, where: str) -> None:
         if rc == _lib.DGR_OK:
             return
-        if 1 <= rc <= 6:
+        if 1 <= rc <= 7:
             for s in range(self.n):
                 code, index, step = self.last_error(s)
                 if code:

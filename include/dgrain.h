@@ -60,6 +60,8 @@ enum dgr_status {
     DGR_ERR_NEG_DEPTH = 4,    /* 2DCode/wetDry2D.c:142-146 */
     DGR_ERR_NAN_VELOCITY = 5, /* 2DCode/wetDry2D.c:233-237 */
     DGR_ERR_EDGE_MATCH = 6,   /* 2DCode/compute2DL.c:51-67 */
+    DGR_ERR_BAD_INDEX = 7,    /* library built with DGR_CHECKED: a kernel met an out-of-range index in the
+                                 connectivity (dgr_last_error: the item, and the kernel in place of the step) */
     DGR_ERR_INVALID = 10,     /* bad argument */
     DGR_ERR_MESH = 11,        /* inconsistent mesh (edge count, uncovered element edge) */
     DGR_ERR_IO = 12,          /* file cannot be read or written */
@@ -173,6 +175,24 @@ DGR_API int dgr_initial_state(int num_el, const int *EltoVert, const double *zet
 /* Writes one .dat file in the reference format (time_evolution.c:284-306,363-386):
  * one element per line, its three values as "%1.15f\t\t". */
 DGR_API int dgr_write_dat(const char *path, int num_el, const double *values);
+
+/* Restart files (resume a run where it stopped; the reference has none: 2DCode writes .dat
+ * snapshots at FinalTime only, time_evolution.c:324-390).  Text in the .dat row layout —
+ * one element per line, tab-separated — with each value printed with 17 significant
+ * digits, so that reading it back gives the same bits (signed zeros included), the
+ * element's wet/dry flag last on its line, and a header with the sizes and the clock
+ * (time, and the dt of the next step).  nm = values per variable and element (3 at p = 1,
+ * 6 at p = 2).  dgr_read_restart returns DGR_ERR_MESH for a file of another mesh size or
+ * order and DGR_ERR_IO for a malformed one. */
+DGR_API int dgr_write_restart(const char *path, int num_el, int nm, const double *zeta, const double *Qx,
+                              const double *Qy, const int *WD, double time, double dt);
+DGR_API int dgr_read_restart(const char *path, int num_el, int nm, double *zeta, double *Qx, double *Qy, int *WD,
+                             double *time, double *dt);
+/* The context's state, wet/dry flags and the given clock written to a restart file, and
+ * read back into a context of the same mesh: a run continued from a loaded file (dgr_run
+ * with the returned time and dt) is bit-identical to the run that never stopped. */
+DGR_API int dgr_save_restart(dgr_ctx *ctx, const char *path, double time, double dt);
+DGR_API int dgr_load_restart(dgr_ctx *ctx, const char *path, double *time, double *dt);
 
 /* The context's current state as .dat files in the same format, formatted on the device
  * (the reference's snapshot writer, time_evolution.c:324-390, runs printf on the host):

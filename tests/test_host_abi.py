@@ -134,3 +134,39 @@ def test_pointer_rule_of_the_device_buffer_entry_points(tmp_path):
     assert ok(host, 0, p, 0)                # pinned and mapped (unified addressing)
     assert not ok(host, 0, None, 0)         # pinned but not mapped
     assert not ok(unregistered, 0, None, 0) and not ok(unregistered, 0, p, 0)  # pageable memory
+
+
+def test_restart_file_round_trip_and_errors(dgrain, tmp_path):
+    """dgr_write_restart / dgr_read_restart: every value comes back with the same bits
+    (signed zeros, subnormals, the extremes), the flags and the clock too; a file of another
+    mesh size or order, or a damaged one, is refused."""
+    lib = dgrain.load()
+    from dgrain.mesh import _dp, _ip
+
+    rng = np.random.default_rng(4)
+    for ne, nm in ((7, 3), (5, 6)):
+        n = ne * nm
+        vals = [rng.standard_normal(n) * 10.0 ** rng.integers(-300, 300, n) for _ in range(3)]
+        vals[0][:4] = [-0.0, 0.0, 5e-324, -1.7976931348623157e308]
+        vals[1][:2] = [1 / 3, -2.2250738585072014e-308]
+        wd = rng.integers(-1, 2, ne).astype(np.int32)
+        path = str(tmp_path / f"r{nm}.rst").encode()
+        assert lib.dgr_write_restart(path, ne, nm, *[_dp(v) for v in vals], _ip(wd), 1234.5678, 0.1 / 3) == 0
+        got = [np.empty(n) for _ in range(3)]
+        gwd = np.empty(ne, dtype=np.int32)
+        t, d = C.c_double(), C.c_double()
+        assert lib.dgr_read_restart(path, ne, nm, *[_dp(g) for g in got], _ip(gwd), C.byref(t), C.byref(d)) == 0
+        for a, b in zip(got, vals):
+            assert np.array_equal(a.view(np.int64), b.view(np.int64))
+        assert np.array_equal(gwd, wd) and t.value == 1234.5678 and d.value == 0.1 / 3
+        # another mesh size or order
+        assert lib.dgr_read_restart(path, ne + 1, nm, *[_dp(g) for g in got], _ip(gwd), C.byref(t),
+                                    C.byref(d)) == dgrain._lib.DGR_ERR_MESH
+        # a file cut short
+        text = open(path, "rb").read()
+        bad = str(tmp_path / "cut.rst").encode()
+        open(bad, "wb").write(text[: len(text) // 2])
+        assert lib.dgr_read_restart(bad, ne, nm, *[_dp(g) for g in got], _ip(gwd), C.byref(t),
+                                    C.byref(d)) == dgrain._lib.DGR_ERR_IO
+    assert lib.dgr_read_restart(str(tmp_path / "none.rst").encode(), 7, 3, *[_dp(g) for g in got[:3]], _ip(gwd),
+                                C.byref(t), C.byref(d)) in (dgrain._lib.DGR_ERR_IO, dgrain._lib.DGR_ERR_INVALID)
