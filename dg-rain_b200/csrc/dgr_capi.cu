@@ -1629,6 +1629,39 @@ extern "C" int dgr_pow43_batch(const double *x, double *y, int n, int device)
     return DGR_OK;
 }
 
+static __global__ void k_div_rcp(int n, const double *__restrict__ a, const double *__restrict__ b, double *q,
+                                 int *valid)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    bool ok = rcp_divisor_ok(b[i]);
+    q[i] = div_rcp(a[i], b[i], 1.0 / b[i], ok);
+    valid[i] = ok ? 1 : 0;
+}
+
+extern "C" int dgr_div_rcp_batch(const double *a, const double *b, double *q, int *valid, int n, int device)
+{
+    if (!a || !b || !q || !valid || n < 0) return DGR_ERR_INVALID;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return DGR_ERR_NO_DEVICE;
+    CK(cudaSetDevice(device));
+    const size_t m = n ? (size_t)n : 1;
+    double *d = nullptr;
+    CK(cudaMalloc((void **)&d, 3 * m * sizeof(double) + m * sizeof(int)));
+    int *dv = (int *)(d + 3 * m);
+    cudaError_t e = cudaMemcpy(d, a, (size_t)n * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + m, b, (size_t)n * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n) k_div_rcp<<<blocks(n, 256), 256>>>(n, d, d + m, d + 2 * m, dv);
+    if (e == cudaSuccess) e = cudaMemcpy(q, d + 2 * m, (size_t)n * 8, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(valid, dv, (size_t)n * 4, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        snprintf(dgr_cuda_err_buffer(), 256, "div_rcp: %s", cudaGetErrorString(e));
+        return DGR_ERR_CUDA;
+    }
+    return DGR_OK;
+}
+
 /* --------------------------------------------------------------- gauges ---- */
 
 extern "C" int dgr_set_gauges(dgr_ctx *c, int ngauges, const int *gauge_el, const double *gauge_w, int capacity)

@@ -12,6 +12,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 
 #ifndef __CUDACC__
 /* plain C++ compilers (the host test harness of the derivative cores): the library's
@@ -73,16 +74,100 @@ DGR_HD void matvec3(const T m[3][3], const T v[3], T out[3])
     }
 }
 
+/* biased exponent field of a double */
+DGR_HD unsigned exponent_bits(double a)
+{
+#ifdef __CUDA_ARCH__
+    return ((unsigned)__double2hiint(a) >> 20) & 0x7ffu;
+#else
+    uint64_t u;
+    memcpy(&u, &a, 8);
+    return (unsigned)(u >> 52) & 0x7ffu;
+#endif
+}
+
+/*
+ * a / b rounded to nearest exactly as the IEEE division, from y = 1/b (itself an IEEE
+ * division, shared by every quotient with the same divisor): Markstein's correction
+ * (P. Markstein, "Computation of elementary functions on the IBM RISC System/6000
+ * processor", IBM J. Res. Develop. 34(1), 1990), taken twice.  q0 = a y is within two
+ * ulps of a/b; q1 = q0 + (a - b q0) y is within one ulp; with the residual a - b q1 then
+ * exact (a fused multiply-add), q2 = q1 + (a - b q1) y is a/b rounded to nearest.  That
+ * needs every quantity clear of underflow and overflow: the caller keeps b within
+ * [2^-100, 2^100], and `ok` is cleared when a is outside [2^-900, 2^900] (zero aside:
+ * a zero a gives a y, the IEEE signed zero), so that the caller can redo the work with
+ * plain divisions.  The library's tests compare it with the IEEE division bit for bit.
+ */
+DGR_HD double div_rcp(double a, double b, double y, bool &ok)
+{
+    const double q0 = a * y;
+    const double r0 = fma(-b, q0, a);
+    const double q1 = fma(r0, y, q0);
+    const double r1 = fma(-b, q1, a);
+    const double q2 = fma(r1, y, q1);
+    const unsigned e = exponent_bits(a);
+    ok = ok && ((e >= 1023u - 900u && e <= 1023u + 900u) || a == 0.0);
+    return a == 0.0 ? q0 : q2;
+}
+
+/* whether b may serve as div_rcp's divisor: |b| within [2^-100, 2^100] */
+DGR_HD bool rcp_divisor_ok(double b)
+{
+    const unsigned e = exponent_bits(b);
+    return e >= 1023u - 100u && e <= 1023u + 100u;
+}
+
+/* rt0_fit below with its three divisions by dM taken through div_rcp (y = 1/dM) */
+DGR_HD void rt0_fit_rcp(double R1, double R2, double R3, double M11, double M12, double M13, double M21,
+                         double M22, double M23, double M31, double M32, double M33, double dM, double y, double &a,
+                         double &b, double &c, bool &ok)
+{
+    a = div_rcp(R3 * M13 * M22 - R3 * M12 * M23 - R2 * M13 * M32 + R1 * M23 * M32 + R2 * M12 * M33 - R1 * M22 * M33,
+                dM, y, ok);
+    b = -div_rcp(R3 * M13 * M21 - R3 * M11 * M23 - R2 * M13 * M31 + R1 * M23 * M31 + R2 * M11 * M33 - R1 * M21 * M33,
+                 dM, y, ok);
+    c = div_rcp(R3 * M12 * M21 - R3 * M11 * M22 - R2 * M12 * M31 + R1 * M22 * M31 + R2 * M11 * M32 - R1 * M21 * M32,
+                dM, y, ok);
+}
+
+/* Division policies of the flux arithmetic.  PlainDiv: every quotient an IEEE division.
+ * RcpDiv (doubles): one reciprocal per divisor, shared by that divisor's quotients
+ * (div_rcp: the same bits); ok records whether every divisor and dividend was in the
+ * range where that holds, and the caller redoes the work with PlainDiv where not. */
+struct PlainDiv {
+    template <class B>
+    struct By {
+        B b;
+    };
+    template <class B>
+    DGR_HD By<B> by(const B &b) const { return {b}; }
+    template <class A, class B>
+    DGR_HD auto div(const A &a, const By<B> &d) const { return a / d.b; }
+};
+struct RcpDiv {
+    bool ok = true;
+    struct By {
+        double b, y;
+    };
+    DGR_HD By by(double b)
+    {
+        ok = ok && rcp_divisor_ok(b);
+        return {b, 1.0 / b};
+    }
+    DGR_HD double div(double a, const By &d) { return div_rcp(a, d.b, d.y, ok); }
+};
+
 /* Roe flux with entropy fix, 2DCode/numericalFlux2D.c:6-108.  Returns max |lambda| of the
  * two traces.  local_g scales the pressure term only; g sets the eigen-structure. */
-template <class T>
-DGR_HD T roe_flux(T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy_ex, T z_edge, double nx,
-                  double ny, double local_g, double g)
+template <class T, class Div>
+DGR_HD T roe_flux_div(Div &dv, T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy_ex, T z_edge,
+                      double nx, double ny, double local_g, double g)
 {
     const T h_in = zeta_in + z_edge;
     const T h_ex = zeta_ex + z_edge;
-    const T u_in = qx_in / h_in, u_ex = qx_ex / h_ex;
-    const T v_in = qy_in / h_in, v_ex = qy_ex / h_ex;
+    const auto by_h_in = dv.by(h_in), by_h_ex = dv.by(h_ex);
+    const T u_in = dv.div(qx_in, by_h_in), u_ex = dv.div(qx_ex, by_h_ex);
+    const T v_in = dv.div(qy_in, by_h_in), v_ex = dv.div(qy_ex, by_h_ex);
     const T jump[3] = {zeta_in - zeta_ex, qx_in - qx_ex, qy_in - qy_ex};
 
     const T p_in = 0.5 * local_g * (h_in * h_in - z_edge * z_edge);
@@ -95,18 +180,21 @@ DGR_HD T roe_flux(T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy
 
     const T s_in = sqrt(h_in), s_ex = sqrt(h_ex);
     const T h_hat = 0.5 * (h_in + h_ex);
-    const T u_hat = (u_in * s_in + u_ex * s_ex) / (s_in + s_ex);
-    const T v_hat = (v_in * s_in + v_ex * s_ex) / (s_in + s_ex);
+    const auto by_s = dv.by(s_in + s_ex);
+    const T u_hat = dv.div(u_in * s_in + u_ex * s_ex, by_s);
+    const T v_hat = dv.div(v_in * s_in + v_ex * s_ex, by_s);
     const T c = sqrt(g * h_hat);
 
     const T r[3][3] = {{1, 0, 1}, {u_hat - c * nx, -ny, u_hat + c * nx}, {v_hat - c * ny, nx, v_hat + c * ny}};
     const T den = -2 * c;
+    const auto by_den = dv.by(den);
     /* (-nx)/den is exactly -(nx/den): IEEE division is symmetric in sign, so the third
      * row reuses the first row's quotients. */
-    const T nx_den = nx / den, ny_den = ny / den;
-    const T ri[3][3] = {{(-c - nx * u_hat - ny * v_hat) / den, nx_den, ny_den},
-                        {(-2 * c * ny * u_hat + 2 * c * nx * v_hat) / den, 2 * c * ny / den, -2 * c * nx / den},
-                        {(-c + nx * u_hat + ny * v_hat) / den, -nx_den, -ny_den}};
+    const T nx_den = dv.div(nx, by_den), ny_den = dv.div(ny, by_den);
+    const T ri[3][3] = {{dv.div(-c - nx * u_hat - ny * v_hat, by_den), nx_den, ny_den},
+                        {dv.div(-2 * c * ny * u_hat + 2 * c * nx * v_hat, by_den), dv.div(2 * c * ny, by_den),
+                         dv.div(-2 * c * nx, by_den)},
+                        {dv.div(-c + nx * u_hat + ny * v_hat, by_den), -nx_den, -ny_den}};
 
     const T un_in = u_in * nx + v_in * ny, un_ex = u_ex * nx + v_ex * ny;
     const T c_in = sqrt(g * h_in), c_ex = sqrt(g * h_ex);
@@ -139,6 +227,14 @@ DGR_HD T roe_flux(T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy
     m = rmax(m, fabs(l3_in));
     m = rmax(m, fabs(l3_ex));
     return m;
+}
+
+template <class T>
+DGR_HD T roe_flux(T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy_ex, T z_edge, double nx,
+                  double ny, double local_g, double g)
+{
+    PlainDiv dv;
+    return roe_flux_div<T>(dv, fh, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g);
 }
 
 /* Local Lax-Friedrichs flux (DG-SWEM src/numerical_flux.F:887-1141, LLF_FLUX, in its
@@ -233,12 +329,13 @@ DGR_HD T hllc_flux(T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T q
 }
 
 /* numerical flux of kind `type` (0: Roe, 2DCode; 1: local Lax-Friedrichs, 2: HLLC, DG-SWEM) */
-template <class T>
+template <class T, class Div = PlainDiv>
 DGR_HD T numerical_flux(int type, T fh[3], T zeta_in, T zeta_ex, T qx_in, T qx_ex, T qy_in, T qy_ex, T z_edge,
-                        double nx, double ny, double local_g, double g)
+                        double nx, double ny, double local_g, double g, Div *dv = nullptr)
 {
     if (type == 1) return llf_flux<T>(fh, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g);
     if (type == 2) return hllc_flux<T>(fh, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g);
+    if (dv) return roe_flux_div<T>(*dv, fh, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g);
     return roe_flux<T>(fh, zeta_in, zeta_ex, qx_in, qx_ex, qy_in, qy_ex, z_edge, nx, ny, local_g, g);
 }
 

@@ -123,8 +123,22 @@ DGR_DEV void l2_prefetch_slice(const T *p0, int ld, int planes, int base, int n)
 /* One edge (2DCode/compute2DL.c:17-331): traces, ghost state, Roe flux(es); stores Fhat.n
  * for both sides and returns the edge's max wave speed (0 for a finished scenario). */
 /* FT: the numerical flux as a compile-time constant (0 Roe, 1 LLF, 2 HLLC), or -1 to take
- * it from the mesh at run time */
-template <bool WD, bool COH = false, int FT = -1>
+ * it from the mesh at run time.  RCP: the Roe flux's divisions share one reciprocal per
+ * divisor (RcpDiv, the same bits); an edge where that is not valid is redone by
+ * edge_flux_item_plain (plain divisions, kept out of line). */
+template <bool WD, bool COH = false, int FT = -1, bool RCP = false>
+DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, const double *bzeta,
+                              const double *bqn, double *flux, DevClock *clk, int phase, double g, int i);
+
+template <bool WD, bool COH, int FT>
+__device__ __noinline__ double edge_flux_item_plain(const MeshDev &m, const double *S, const int *wd,
+                                                    const double *bzeta, const double *bqn, double *flux,
+                                                    DevClock *clk, int phase, double g, int i)
+{
+    return edge_flux_item<WD, COH, FT, false>(m, S, wd, bzeta, bqn, flux, clk, phase, g, i);
+}
+
+template <bool WD, bool COH, int FT, bool RCP>
 DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, const double *bzeta,
                               const double *bqn, double *flux, DevClock *clk, int phase, double g, int i)
 {
@@ -153,8 +167,15 @@ DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, 
         const int wdi = WD ? ldm<COH>(&wd[el_in]) : 1, wde = WD ? ldm<COH>(&wd[el_ex]) : 1;
         double fin[3], fex[3];
         int code;
-        lam = flux_core<double, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code,
-                                    FT >= 0 ? FT : m.flux);
+        if constexpr (RCP) {
+            RcpDiv dv;
+            lam = flux_core<double, WD, RcpDiv>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex,
+                                                code, FT >= 0 ? FT : m.flux, &dv);
+            if (!dv.ok) return edge_flux_item_plain<WD, COH, FT>(m, S, wd, bzeta, bqn, flux, clk, phase, g, i);
+        } else {
+            lam = flux_core<double, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code,
+                                        FT >= 0 ? FT : m.flux);
+        }
         if (code) atomicMin(&ck->err, err_key(ldm<COH>(&ck->step), phase, code, i - ck->ed_off));
         const int lf = m.ldF;
         flux[i] = fin[0];
@@ -234,8 +255,22 @@ DGR_DEV bool gather_flux(const MeshDev &m, const double *flux, int el, double F[
 }
 
 /* One element of the RHS / RK stage (element_core); S is the stage input, U the step
- * input (stage 2 only).  MODE_RHS writes the RHS. */
-template <int MODE, bool COH = false>
+ * input (stage 2 only).  MODE_RHS writes the RHS.  RCP: the fits' divisions by their
+ * determinant share one reciprocal (div_rcp, the same bits); an element where that is not
+ * valid is redone by element_item_plain (plain divisions, kept out of line). */
+template <int MODE, bool COH = false, bool RCP = true>
+DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, const int *wd, const double *flux,
+                          double *out, double *avg, const DevClock *clk, double g, int el);
+
+template <int MODE, bool COH>
+__device__ __noinline__ void element_item_plain(const MeshDev &m, const double *S, const double *U, const int *wd,
+                                                const double *flux, double *out, double *avg, const DevClock *clk,
+                                                double g, int el)
+{
+    element_item<MODE, COH, false>(m, S, U, wd, flux, out, avg, clk, g, el);
+}
+
+template <int MODE, bool COH, bool RCP>
 DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, const int *wd, const double *flux,
                           double *out, double *avg, const DevClock *clk, double g, int el)
 {
@@ -259,7 +294,13 @@ DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, co
     const auto uin = [U, ld, el](int v, int k) { return ldm<COH>(&U[(3 * v + k) * ld + el]); };
     const double dt = (MODE == MODE_RHS) ? 0.0 : ldm<COH>(&ck->dt);
     double w[3][3], a[3];
-    element_core<MODE, double>(F, zr, qxr, qyr, geo, zg, uin, local_g, rain, dt, w, a);
+    bool rcp_ok = true;
+    element_core<MODE, double, decltype(geo), PlaneZGeo, decltype(uin), RCP>(F, zr, qxr, qyr, geo, zg, uin, local_g,
+                                                                          rain, dt, w, a, &rcp_ok);
+    if (RCP && !rcp_ok) {
+        element_item_plain<MODE, COH>(m, S, U, wd, flux, out, avg, clk, g, el);
+        return;
+    }
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
 #pragma unroll

@@ -182,10 +182,10 @@ DGR_HD void ghost_state(int bd, double nx, double ny, const T &zi, const T &qxi,
  * With WD: both dry -> two reflective g = 0 fluxes; one side dry -> that side gets the
  * g = 0 flux.
  */
-template <class T, bool WD>
+template <class T, bool WD, class Div = PlainDiv>
 DGR_HD T flux_core(const T &zi, const T &qxi, const T &qyi, const T &ze, const T &qxe, const T &qye,
                    const T &z_edge, double nx, double ny, int wdi, int wde, double g, T fin[3], T fex[3],
-                   int &code, int ftype = 0)
+                   int &code, int ftype = 0, Div *dv = nullptr)
 {
     const double tx = -ny, ty = nx;
     T lam = 0.0;
@@ -197,25 +197,28 @@ DGR_HD T flux_core(const T &zi, const T &qxi, const T &qyi, const T &ze, const T
         const double d = 1. / (nx * ty - ny * tx);
         const T qxe_ref = (ty * qn_ex - ny * qt_ex) * d;
         const T qye_ref = (-tx * qn_ex + nx * qt_ex) * d;
-        const T lam_in = numerical_flux<T>(ftype, fin, zi, zi, qxi, qxe_ref, qyi, qye_ref, z_edge, nx, ny, 0.0, g);
+        const T lam_in = numerical_flux<T, Div>(ftype, fin, zi, zi, qxi, qxe_ref, qyi, qye_ref,
+                                                  z_edge, nx, ny, 0.0, g, dv);
         qn_ex = qxe * nx + qye * ny;
         qt_ex = qxe * tx + qye * ty;
         qn_in = -qn_ex;
         qt_in = qt_ex;
         const T qxi_ref = (ty * qn_in - ny * qt_in) * d;
         const T qyi_ref = (-tx * qn_in + nx * qt_ex) * d;
-        const T lam_ex = numerical_flux<T>(ftype, fex, ze, ze, qxi_ref, qxe, qyi_ref, qye, z_edge, nx, ny, 0.0, g);
+        const T lam_ex = numerical_flux<T, Div>(ftype, fex, ze, ze, qxi_ref, qxe, qyi_ref, qye,
+                                                  z_edge, nx, ny, 0.0, g, dv);
         lam = rmax(lam_in, lam_ex);
     } else {
         T fh[3];
-        lam = numerical_flux<T>(ftype, fh, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, g, g);
+        lam = numerical_flux<T, Div>(ftype, fh, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, g, g, dv);
         if (isnan(fh[0]) || isnan(fh[1]) || isnan(fh[2])) code = 1;
         if (!WD || wdi == 1) {
             fin[0] = fh[0];
             fin[1] = fh[1];
             fin[2] = fh[2];
         } else {
-            const T l2 = numerical_flux<T>(ftype, fin, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g);
+            const T l2 =
+                numerical_flux<T, Div>(ftype, fin, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g, dv);
             if (!code && (isnan(fin[0]) || isnan(fin[1]) || isnan(fin[2]))) code = 2;
             lam = rmax(lam, l2);
         }
@@ -224,7 +227,8 @@ DGR_HD T flux_core(const T &zi, const T &qxi, const T &qyi, const T &ze, const T
             fex[1] = fh[1];
             fex[2] = fh[2];
         } else {
-            const T l2 = numerical_flux<T>(ftype, fex, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g);
+            const T l2 =
+                numerical_flux<T, Div>(ftype, fex, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g, dv);
             if (!code && (isnan(fex[0]) || isnan(fex[1]) || isnan(fex[2]))) code = 3;
             lam = rmax(lam, l2);
         }
@@ -261,15 +265,30 @@ DGR_HD void stage_coefficients(int mode, double &cu, double &cs, double &cr)
  *   uin(v, k)   step input u^n (stage 2 only)
  * Returns w[3][3] and the element means avg[3].
  */
-template <int MODE, class T, class Geo, class ZGeo, class UIn>
+template <int MODE, class T, class Geo, class ZGeo, class UIn, bool RCP = false>
 DGR_HD void element_core(const T F[3][3], const T zr[3], const T qxr[3], const T qyr[3], const Geo &geo,
                          const ZGeo &zg, const UIn &uin, double local_g, double rain, double dt, T w[3][3],
-                         T avg[3])
+                         T avg[3], bool *rcp_ok = nullptr)
 {
     const double nx[3] = {geo(G_NX), geo(G_NX + 1), geo(G_NX + 2)};
     const double ny[3] = {geo(G_NY), geo(G_NY + 1), geo(G_NY + 2)};
     const double M12 = geo(G_M12), M22 = geo(G_M12 + 1), M32 = geo(G_M12 + 2), dM = geo(G_DM);
     const double M11 = nx[0], M13 = ny[0], M21 = nx[1], M23 = ny[1], M31 = nx[2], M33 = ny[2];
+    /* RCP (T = double): the eighteen divisions by dM of the six fits share one reciprocal
+     * (div_rcp, the same bits); *rcp_ok is cleared where that is not valid, and the caller
+     * then redoes the element with plain divisions */
+    double y_dm = 0.0;
+    bool ok = true;
+    if constexpr (RCP) {
+        y_dm = 1.0 / dM;
+        ok = rcp_divisor_ok(dM);
+    }
+    const auto fit = [&](const T &R1, const T &R2, const T &R3, T &a, T &b, T &c) {
+        if constexpr (RCP)
+            rt0_fit_rcp(R1, R2, R3, M11, M12, M13, M21, M22, M23, M31, M32, M33, dM, y_dm, a, b, c, ok);
+        else
+            rt0_fit(R1, R2, R3, M11, M12, M13, M21, M22, M23, M31, M32, M33, dM, a, b, c);
+    };
 
     /* surface integrals SI[9] (:95-239) */
     T si[9];
@@ -278,7 +297,7 @@ DGR_HD void element_core(const T F[3][3], const T zr[3], const T qxr[3], const T
 #pragma unroll
         for (int v = 0; v < 3; ++v) {
             T a, b, c;
-            rt0_fit(F[v][0], F[v][1], F[v][2], M11, M12, M13, M21, M22, M23, M31, M32, M33, dM, a, b, c);
+            fit(F[v][0], F[v][1], F[v][2], a, b, c);
             T fd[3][2];
 #pragma unroll
             for (int e = 0; e < 3; ++e)
@@ -301,14 +320,26 @@ DGR_HD void element_core(const T F[3][3], const T zr[3], const T qxr[3], const T
     for (int e = 0; e < 3; ++e) {
         const T midz = zg.midz(e);
         H[e] = zr[e] + midz;
-        const T u = qxr[e] / H[e];
-        const T v = qyr[e] / H[e];
+        /* the five divisions by H: plain, or (RCP) through one reciprocal of H */
+        T yH = 0.0;
+        if constexpr (RCP) {
+            yH = 1.0 / H[e];
+            ok = ok && rcp_divisor_ok(H[e]);
+        }
+        const auto byH = [&](const T &x) -> T {
+            if constexpr (RCP)
+                return div_rcp(x, H[e], yH, ok);
+            else
+                return x / H[e];
+        };
+        const T u = byH(qxr[e]);
+        const T v = byH(qyr[e]);
         tau[e] = zg.gnn(e) * sqrt(u * u + v * v) / pow43(H[e]);
         const T pr = 0.5 * local_g * (H[e] * H[e] - midz * midz);
-        const T qxy = qxr[e] * qyr[e] / H[e];
+        const T qxy = byH(qxr[e] * qyr[e]);
         R[0][e] = qxr[e] * nx[e] + qyr[e] * ny[e];
-        R[1][e] = (qxr[e] * qxr[e] / H[e] + pr) * nx[e] + qxy * ny[e];
-        R[2][e] = qxy * nx[e] + (qyr[e] * qyr[e] / H[e] + pr) * ny[e];
+        R[1][e] = (byH(qxr[e] * qxr[e]) + pr) * nx[e] + qxy * ny[e];
+        R[2][e] = qxy * nx[e] + (byH(qyr[e] * qyr[e]) + pr) * ny[e];
     }
     const double aj = geo(G_AJ), ajw = geo(G_AJW);
     const double weight = 1.0 / 6;
@@ -316,7 +347,7 @@ DGR_HD void element_core(const T F[3][3], const T zr[3], const T qxr[3], const T
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
         T a, b, c;
-        rt0_fit(R[v][0], R[v][1], R[v][2], M11, M12, M13, M21, M22, M23, M31, M32, M33, dM, a, b, c);
+        fit(R[v][0], R[v][1], R[v][2], a, b, c);
 #pragma unroll
         for (int bf = 0; bf < 3; ++bf)
             dv[v][bf] = aj * (0.5 * a * geo(G_GP + 2 * bf) + 0.5 * c * geo(G_GP + 2 * bf + 1) +
@@ -347,6 +378,7 @@ DGR_HD void element_core(const T F[3][3], const T zr[3], const T qxr[3], const T
         rhs[0][2] += rain;
     }
 
+    if constexpr (RCP) *rcp_ok = ok;
     if (MODE == MODE_RHS) {
 #pragma unroll
         for (int v = 0; v < 3; ++v)
@@ -374,8 +406,15 @@ DGR_HD void element_core(const T F[3][3], const T zr[3], const T qxr[3], const T
 #pragma unroll
             for (int k = 0; k < 3; ++k) w[v][k] = a * uin(v, k) + b * (s[v][k] + rhs[v][k] * dt);
     }
+    if constexpr (RCP) { /* the means' divisions by 3 through the reciprocal RN(1/3) */
+        bool ok_avg = true;
 #pragma unroll
-    for (int v = 0; v < 3; ++v) avg[v] = (w[v][0] + w[v][1] + w[v][2]) / 3;
+        for (int v = 0; v < 3; ++v) avg[v] = div_rcp(w[v][0] + w[v][1] + w[v][2], 3.0, 1.0 / 3, ok_avg);
+        *rcp_ok = ok && ok_avg;
+    } else {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) avg[v] = (w[v][0] + w[v][1] + w[v][2]) / 3;
+    }
 }
 
 /* Decisions of one element's limiter and PDop pass (recorded for the adjoint tests). */

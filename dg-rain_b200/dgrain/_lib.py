@@ -142,6 +142,7 @@ SIGNATURES = [
     ("dgr_last_device_ms", C.c_double, [C.c_void_p]),
     ("dgr_profile_step", C.c_int, [C.c_void_p, C.c_int, dptr, C.c_int]),
     ("dgr_pow43_batch", C.c_int, [dptr, dptr, C.c_int, C.c_int]),
+    ("dgr_div_rcp_batch", C.c_int, [dptr, dptr, dptr, iptr, C.c_int, C.c_int]),
     ("dgr_set_channel_ends", C.c_int, [C.c_void_p, C.c_int, iptr, iptr, iptr]),
     ("dgr_couple_channel_ends", C.c_int, [C.c_void_p, dptr, dptr, dptr, dptr]),
     ("dgr_get_boundary", C.c_int, [C.c_void_p, dptr, dptr]),

@@ -452,6 +452,11 @@ DGR_API int dgr_get_boundary(dgr_ctx *ctx, double *bzeta, double *bQn);
 /* Diagnostic: y[i] = x[i]^(4./3) as the kernels evaluate the Manning term of
  * 2DCode/2DInnerProducts.c:318 (correctly rounded; see dgr_device.cuh). */
 DGR_API int dgr_pow43_batch(const double *x, double *y, int n, int device);
+/* Diagnostic: q[i] = a[i] / b[i] as the element kernel takes its divisions by the fit
+ * determinant (one reciprocal per divisor and Markstein's correction, dgr_device.cuh:
+ * div_rcp), valid[i] = 1 where that path applies (elsewhere the kernel uses the plain
+ * division).  Where valid, q equals the IEEE quotient bit for bit. */
+DGR_API int dgr_div_rcp_batch(const double *a, const double *b, double *q, int *valid, int n, int device);
 
 #ifdef __cplusplus
 }

@@ -342,3 +342,47 @@ def test_limiter_signed_zero_bounds(dgrain, oracle_mod, seed):
         assert same(a, b)
     assert negative_zeros(want[1]) > 0
     s.close()
+
+
+def _division_cases(n, seed):
+    """operand pairs for the shared-reciprocal division: random within its valid range,
+    exact and near-exact quotients, all-ones divisors, quotients near powers of two,
+    zeros of both signs, and the sizes of the RT0 fits"""
+    rng = np.random.default_rng(seed)
+
+    def rand(k, lo, hi):
+        m = rng.integers(0, 1 << 52, k, dtype=np.uint64)
+        e = rng.integers(lo, hi + 1, k).astype(np.uint64) + np.uint64(1023)
+        s = rng.integers(0, 2, k).astype(np.uint64) << np.uint64(63)
+        return (s | (e << np.uint64(52)) | m).view(np.float64)
+
+    k = n // 6
+    b = rand(6 * k, -100, 100)
+    a = np.empty(6 * k)
+    a[:k] = rand(k, -900, 900)
+    a[k:2 * k] = b[k:2 * k] * rng.integers(-2048, 2048, k)
+    near = (rand(k, -20, 20) * b[2 * k:3 * k]).view(np.int64) + rng.integers(-2, 3, k)
+    a[2 * k:3 * k] = near.view(np.float64)
+    b[3 * k:4 * k] = np.where(rng.random(k) < 0.5, 1.0, -1.0) * np.ldexp(
+        np.nextafter(2.0, 0.0), rng.integers(-100, 100, k))
+    a[3 * k:4 * k] = rand(k, -100, 100)
+    a[4 * k:5 * k] = np.where(rng.random(k) < 0.5, -0.0, 0.0)
+    a[5 * k:] = rand(k, -40, 15)
+    b[5 * k:] = rand(k, -10, 10)
+    return np.ascontiguousarray(a), np.ascontiguousarray(b)
+
+
+def test_shared_reciprocal_division_on_device(dgrain):
+    """The element kernel's divisions by the fit determinant (one reciprocal per element and
+    Markstein's correction) equal the IEEE division bit for bit, on 6 million pairs."""
+    a, b = _division_cases(6_000_000, 11)
+    q = np.empty_like(a)
+    valid = np.empty(len(a), dtype=np.int32)
+    lib = dgrain.load()
+    dp, ip = dgrain._lib.dptr, dgrain._lib.iptr
+    assert lib.dgr_div_rcp_batch(a.ctypes.data_as(dp), b.ctypes.data_as(dp), q.ctypes.data_as(dp),
+                                 valid.ctypes.data_as(ip), len(a), 0) == 0
+    v = valid == 1
+    assert v.mean() > 0.99
+    with np.errstate(all="ignore"):
+        assert bits_equal(q[v], (a / b)[v])
