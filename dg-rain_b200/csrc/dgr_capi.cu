@@ -75,7 +75,7 @@ static void release(dgr_ctx *c)
 {
     if (!c) return;
     drop_graph(c);
-    void *ptrs[] = {c->x, c->y, c->zn, c->nfric, c->n_el, c->el2v_aos, c->el2v, c->elem_edge, c->e_in,
+    void *ptrs[] = {c->x, c->y, c->zn, c->nfric, c->n_el, c->el2v_aos, c->el2v, c->elem_edge, c->e_in, c->redo,
                     c->e_ex, c->e_info, c->n2e_ptr, c->n2e, c->bnd_edges, c->bnd_type, c->bnd_sid, c->bdry,
                     c->el_sid, c->ed_sid, c->e_geo, c->geo, c->U, c->W, c->flux, c->avg, c->bounds, c->bzeta,
                     c->bqn, c->bstage, c->wdA, c->wdB, c->wdC, c->dec, c->bar, c->clk, c->p2g,
@@ -306,6 +306,7 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     TRY(dalloc(&c->wdC, ne));
     TRY(dalloc(&c->dec, 6 * ne));
     TRY(dalloc(&c->bar, 6)); /* barrier words [0..2]; [4..5] the checked build's bad-index word */
+    TRY(dalloc(&c->redo, 2 + (size_t)nf));
     TRY(dalloc(&c->clk, nscen));
     TRYC(cudaHostAlloc((void **)&c->h_clk, sizeof(DevClock) * nscen, cudaHostAllocDefault));
 
@@ -336,6 +337,7 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     TRYC(cudaMemsetAsync(c->dec, 0, 6 * ne * 4, s));
     TRYC(cudaMemsetAsync(c->bar, 0, 16, s));
     TRYC(cudaMemsetAsync(c->bar + 4, 0xff, 8, s));
+    TRYC(cudaMemsetAsync(c->redo, 0, 8, s));
 
     /* per-element Manning n of the scenarios that give one (negative: node average) */
     bool any_nel = false;
@@ -752,6 +754,17 @@ static void launch_element(dgr_ctx *c, const double *S, const int *wd, double *O
     }
 }
 
+/* the plain-division redo of the items k_limit queued (nothing queued: the blocks return
+ * at once); no launch when the limiter takes plain divisions itself */
+template <bool L, bool P, bool ST>
+static void launch_limit_redo(dgr_ctx *c, double *S, const int *wd_in, int *wd_out, int phase, int *dl, int *dp)
+{
+    if (!DGR_LIMIT_RCP) return;
+    k_limit_redo<L, P, ST><<<c->num_sms, 128, 0, c->stream>>>(mesh_dev(c), S, c->bounds, wd_in, wd_out, c->clk,
+                                                              c->p.H0, c->p.VELZERO, phase, dl, dp);
+    c->launches++;
+}
+
 template <bool L, bool P, bool ST>
 static void launch_limit(dgr_ctx *c, double *S, const int *wd_in, int *wd_out, int phase, int *dl, int *dp)
 {
@@ -771,13 +784,20 @@ static void launch_limit(dgr_ctx *c, double *S, const int *wd_in, int *wd_out, i
         k_limit<L, P, ST, 128><<<blocks(c->ne, 128), 128, 0, s>>>(m, S, c->bounds, wd_in, wd_out, c->clk, h0, vz,
                                                                   phase, dl, dp);
     }
+    launch_limit_redo<L, P, ST>(c, S, wd_in, wd_out, phase, dl, dp);
 }
 
 template <bool WD, int FT>
 static void launch_edge_ft(dgr_ctx *c, const double *S, const int *wd, int lam_slot, int phase)
 {
-    k_edge_flux<WD, FT><<<blocks(c->nf, 256), 256, 0, c->stream>>>(mesh_dev(c), S, wd, c->bzeta, c->bqn, c->flux,
-                                                                   c->clk, lam_slot, phase, c->p.g);
+    const MeshDev m = mesh_dev(c);
+    k_edge_flux<WD, FT><<<blocks(c->nf, 256), 256, 0, c->stream>>>(m, S, wd, c->bzeta, c->bqn, c->flux, c->clk,
+                                                                   lam_slot, phase, c->p.g);
+    if (DGR_EDGE_RCP) {
+        k_edge_redo<WD, FT><<<c->num_sms, 256, 0, c->stream>>>(m, S, wd, c->bzeta, c->bqn, c->flux, c->clk,
+                                                               lam_slot, phase, c->p.g);
+        c->launches++;
+    }
 }
 
 /* the edge kernel compiled for the context's wet/dry mode and numerical flux */
@@ -867,7 +887,7 @@ void launch_stage(dgr_ctx *c, int stage, bool count)
         else
             launch_limit<true, false, false>(c, io.OUT, io.wd_in, io.wd_out, 2 * stage + 1, dl, dp);
     }
-    if (count) c->launches += 4;
+    if (count) c->launches += 4; /* edge flux, element, node bounds, limiter (redo launches count themselves) */
 }
 
 void launch_wd_refresh(dgr_ctx *c)
@@ -988,7 +1008,7 @@ static int kernels_per_step(const dgr_ctx *c)
     const int ns = c->p.rk_stages;
     const int rec = c->gauge_n ? 1 : 0;
     if (c->p.order == 2) return 2 + 2 * ns + rec;
-    return rec + (c->fusion == 2 ? 1 : (c->fusion == 1 ? 2 + ns : 2 + 4 * ns));
+    return rec + (c->fusion == 2 ? 1 : (c->fusion == 1 ? 2 + ns : 2 + (4 + DGR_EDGE_RCP + DGR_LIMIT_RCP) * ns));
 }
 
 int decode_err(unsigned long long key, int *code, int *index, int *step)
@@ -1132,6 +1152,7 @@ extern "C" int dgr_slope_limiter(dgr_ctx *c)
     int *dl = c->p.record_decisions ? c->dec : nullptr;
     k_limit<true, false, false, 128><<<blocks(c->ne, 128), 128, 0, s>>>(m, c->U, c->bounds, c->wdA, c->wdA, c->clk,
                                                                          c->p.H0, c->p.VELZERO, 0, dl, nullptr);
+    launch_limit_redo<true, false, false>(c, c->U, c->wdA, c->wdA, 0, dl, nullptr);
     c->launches += 4;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
@@ -1150,6 +1171,7 @@ extern "C" int dgr_pdop(dgr_ctx *c)
     k_limit<false, true, false, 128><<<blocks(c->ne, 128), 128, 0, s>>>(mesh_dev(c), c->U, c->bounds, c->wdA,
                                                                          c->wdA, c->clk, c->p.H0, c->p.VELZERO, 1,
                                                                          nullptr, dp);
+    launch_limit_redo<false, true, false>(c, c->U, c->wdA, c->wdA, 1, nullptr, dp);
     c->launches += 2;
     CK(cudaGetLastError());
     int r = read_clock(c);

@@ -78,6 +78,7 @@ struct dgr_ctx {
     int *wdA, *wdB, *wdC; /* wet/dry flags: stage s reads buffer s, writes buffer (s+1) mod stages */
     int *dec; /* [6][ne]: limit and pdop decisions of stage 0, 1, 2 */
     unsigned *bar;
+    int *redo; /* edge queue of k_edge_flux -> k_edge_redo, [2 + nf] */
     unsigned bar_polls;   /* bound of a grid-barrier wait (dgr_set_barrier_wait) */
     unsigned bar_phantom; /* phantom arrivals a barrier waits for (0 except in tests) */
     dgr::DevClock *clk;
@@ -138,6 +139,7 @@ static inline dgr::MeshDev mesh_dev(const dgr_ctx *c)
     m.ed_sid = c->ed_sid;
     m.flux = c->p.flux;
     m.bad_index = reinterpret_cast<unsigned long long *>(c->bar + 4);
+    m.redo = c->redo;
     return m;
 }
 

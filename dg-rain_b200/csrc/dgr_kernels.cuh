@@ -30,6 +30,15 @@
 #ifndef DGR_MINB_EDGE
 #define DGR_MINB_EDGE 3
 #endif
+/* 1: the edge and limiter kernels take their divisions through shared reciprocals
+ * (div_rcp), queueing the items where that is not valid for a plain-division redo launch;
+ * 0: plain divisions.  Chosen by measurement, overridable at build time. */
+#ifndef DGR_EDGE_RCP
+#define DGR_EDGE_RCP 0
+#endif
+#ifndef DGR_LIMIT_RCP
+#define DGR_LIMIT_RCP 1
+#endif
 
 namespace dgr {
 
@@ -79,6 +88,7 @@ struct MeshDev {
     const int *ed_sid;    /* scenario of each edge, NULL for a single mesh */
     int flux;             /* numerical flux: 0 Roe (2DCode), 1 local Lax-Friedrichs, 2 HLLC (DG-SWEM) */
     unsigned long long *bad_index; /* checked build: first out-of-range gather, (kernel << 32 | item) */
+    int *redo;            /* edges left to k_edge_redo: [0] count, [1] blocks done, [2..] edges */
 };
 
 /* Checked build (compiled with -DDGR_CHECKED): every index a kernel gathers from the
@@ -121,26 +131,16 @@ DGR_DEV void l2_prefetch_slice(const T *p0, int ld, int planes, int base, int n)
 /* ------------------------------------------------------------------ edges ---- */
 
 /* One edge (2DCode/compute2DL.c:17-331): traces, ghost state, Roe flux(es); stores Fhat.n
- * for both sides and returns the edge's max wave speed (0 for a finished scenario). */
-/* FT: the numerical flux as a compile-time constant (0 Roe, 1 LLF, 2 HLLC), or -1 to take
- * it from the mesh at run time.  RCP: the Roe flux's divisions share one reciprocal per
- * divisor (RcpDiv, the same bits); an edge where that is not valid is redone by
- * edge_flux_item_plain (plain divisions, kept out of line). */
-template <bool WD, bool COH = false, int FT = -1, bool RCP = false>
+ * for both sides and returns the edge's max wave speed (0 for a finished scenario).
+ * FT: the numerical flux as a compile-time constant (0 Roe, 1 LLF, 2 HLLC), or -1 to take
+ * it from the mesh at run time.  With `redo` non-null the Roe flux's divisions share one
+ * reciprocal per divisor (RcpDiv, the same bits); an edge where that is not valid reports
+ * no error and no speed and sets *redo: the caller queues it for k_edge_redo, which
+ * redoes it with plain divisions in a launch of its own and overwrites its fluxes. */
+template <bool WD, bool COH = false, int FT = -1>
 DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, const double *bzeta,
-                              const double *bqn, double *flux, DevClock *clk, int phase, double g, int i);
-
-template <bool WD, bool COH, int FT>
-__device__ __noinline__ double edge_flux_item_plain(const MeshDev &m, const double *S, const int *wd,
-                                                    const double *bzeta, const double *bqn, double *flux,
-                                                    DevClock *clk, int phase, double g, int i)
-{
-    return edge_flux_item<WD, COH, FT, false>(m, S, wd, bzeta, bqn, flux, clk, phase, g, i);
-}
-
-template <bool WD, bool COH, int FT, bool RCP>
-DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, const double *bzeta,
-                              const double *bqn, double *flux, DevClock *clk, int phase, double g, int i)
+                              const double *bqn, double *flux, DevClock *clk, int phase, double g, int i,
+                              bool *redo = nullptr)
 {
     double lam = 0.0;
     DevClock *ck = clk + (m.ed_sid ? m.ed_sid[i] : 0);
@@ -167,11 +167,15 @@ DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, 
         const int wdi = WD ? ldm<COH>(&wd[el_in]) : 1, wde = WD ? ldm<COH>(&wd[el_ex]) : 1;
         double fin[3], fex[3];
         int code;
-        if constexpr (RCP) {
+        if (redo) {
             RcpDiv dv;
             lam = flux_core<double, WD, RcpDiv>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex,
                                                 code, FT >= 0 ? FT : m.flux, &dv);
-            if (!dv.ok) return edge_flux_item_plain<WD, COH, FT>(m, S, wd, bzeta, bqn, flux, clk, phase, g, i);
+            if (!dv.ok) { /* k_edge_redo rewrites this edge's fluxes, error and speed */
+                *redo = true;
+                code = 0;
+                lam = 0.0;
+            }
         } else {
             lam = flux_core<double, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code,
                                         FT >= 0 ? FT : m.flux);
@@ -218,7 +222,7 @@ DGR_DEV void block_max_speed(double lam, int sid, bool valid, DevClock *clk, int
 }
 
 template <bool WD, int FT>
-__global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, const double *__restrict__ S,
+__global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(const __grid_constant__ MeshDev m, const double *__restrict__ S,
                                                                   const int *__restrict__ wd,
                                                                   const double *__restrict__ bzeta,
                                                                   const double *__restrict__ bqn,
@@ -228,8 +232,40 @@ __global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(MeshDev m, con
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < m.nf;
     const int sid = (valid && m.ed_sid) ? m.ed_sid[i] : 0;
-    const double lam = valid ? edge_flux_item<WD, false, FT>(m, S, wd, bzeta, bqn, flux, clk, phase, g, i) : 0.0;
+    bool redo = false;
+    const double lam =
+        valid ? edge_flux_item<WD, false, FT>(m, S, wd, bzeta, bqn, flux, clk, phase, g, i,
+                                              DGR_EDGE_RCP ? &redo : nullptr)
+              : 0.0;
+    if (redo) m.redo[2 + atomicAdd(&m.redo[0], 1)] = i;
     block_max_speed(lam, sid, valid, clk, lam_slot);
+}
+
+/* The edges k_edge_flux queued (m.redo: [0] count, [1] blocks done, [2..] edges), with
+ * plain divisions: fluxes, error and wave speed as k_edge_flux would have given them.
+ * Launched after every k_edge_flux; with nothing queued each block returns at once.  The
+ * last block to finish clears the queue for the next launch. */
+template <bool WD, int FT>
+__global__ void __launch_bounds__(256) k_edge_redo(const __grid_constant__ MeshDev m, const double *__restrict__ S,
+                                                   const int *__restrict__ wd, const double *__restrict__ bzeta,
+                                                   const double *__restrict__ bqn, double *__restrict__ flux,
+                                                   DevClock *clk, int lam_slot, int phase, double g)
+{
+    const int n = *(volatile int *)&m.redo[0];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int i = m.redo[2 + k];
+        const double lam = edge_flux_item<WD, false, FT>(m, S, wd, bzeta, bqn, flux, clk, phase, g, i);
+        const int sid = m.ed_sid ? m.ed_sid[i] : 0;
+        if (lam > 0.0) atomicMax(&clk[sid].lam_bits[lam_slot], (unsigned long long)__double_as_longlong(lam));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&m.redo[1], 1) == (int)gridDim.x - 1) {
+            m.redo[0] = 0;
+            m.redo[1] = 0;
+        }
+    }
 }
 
 /* ---------------------------------------------------------------- elements ---- */
@@ -310,7 +346,7 @@ DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, co
 }
 
 template <int MODE, int BS>
-__global__ void __launch_bounds__(BS, 512 / BS) k_element(MeshDev m, const double *__restrict__ S,
+__global__ void __launch_bounds__(BS, 512 / BS) k_element(const __grid_constant__ MeshDev m, const double *__restrict__ S,
                                                           const double *__restrict__ U, const int *__restrict__ wd,
                                                           const double *__restrict__ flux, double *__restrict__ out,
                                                           double *__restrict__ avg, const DevClock *clk, double g)
@@ -393,7 +429,7 @@ static __global__ void __launch_bounds__(256) k_wd_status(MeshDev m, const doubl
  * wet/dry status (2DCode/wetDry2D.c:16-60) that the reference calls next.  wd_in is the
  * status the element had; the new status goes to wd_out.
  */
-template <bool LIMIT, bool PDOP, bool STATUS, bool COH = false>
+template <bool LIMIT, bool PDOP, bool STATUS, bool COH = false, bool RCP = false>
 DGR_DEV void limit_item(const MeshDev &m, double *S, const double *bounds, const int *wd_in, int *wd_out,
                         DevClock *clk, double h0, double velzero, int phase, int *dec_limit, int *dec_pdop, int el)
 {
@@ -415,7 +451,16 @@ DGR_DEV void limit_item(const MeshDev &m, double *S, const double *bounds, const
         return ldm<COH>(&bounds[(3 * is_min + v) * lb + nd[k]]);
     };
     LimitDecisions dec;
-    limit_core<LIMIT, PDOP, double>(w, bnd, zn, h0, velzero, dec);
+    RcpDiv dv;
+    if constexpr (RCP) {
+        limit_core<LIMIT, PDOP, double, decltype(bnd), false, RcpDiv>(w, bnd, zn, h0, velzero, dec, nullptr, &dv);
+        if (!dv.ok) { /* k_limit_redo redoes it with plain divisions from the untouched state */
+            m.redo[2 + atomicAdd(&m.redo[0], 1)] = el;
+            return;
+        }
+    } else {
+        limit_core<LIMIT, PDOP, double>(w, bnd, zn, h0, velzero, dec);
+    }
     if (LIMIT && dec_limit) dec_limit[el] = dec.modify;
     if (PDOP) {
         if (dec.code) atomicMin(&ck->err, err_key(ldm<COH>(&ck->step), phase, dec.code, el - ck->el_off));
@@ -425,11 +470,20 @@ DGR_DEV void limit_item(const MeshDev &m, double *S, const double *bounds, const
     for (int v = 0; v < 3; ++v)
 #pragma unroll
         for (int k = 0; k < 3; ++k) S[(3 * v + k) * ld + el] = w[v][k];
-    if (STATUS) wd_out[el] = wd_status(w[0], zn, ldm<COH>(&wd_in[el]), h0);
+    if (STATUS) {
+        if constexpr (RCP) {
+            const int st = wd_status(w[0], zn, ldm<COH>(&wd_in[el]), h0, &dv);
+            /* the element's state is written: a status that needs the plain division is
+             * taken with it here (one division, so inline) */
+            wd_out[el] = dv.ok ? st : wd_status(w[0], zn, ldm<COH>(&wd_in[el]), h0);
+        } else {
+            wd_out[el] = wd_status(w[0], zn, ldm<COH>(&wd_in[el]), h0);
+        }
+    }
 }
 
 template <bool LIMIT, bool PDOP, bool STATUS, int BS>
-__global__ void __launch_bounds__(BS, 768 / BS) k_limit(MeshDev m, double *__restrict__ S,
+__global__ void __launch_bounds__(BS, 768 / BS) k_limit(const __grid_constant__ MeshDev m, double *__restrict__ S,
                                                         const double *__restrict__ bounds,
                                                         const int *__restrict__ wd_in, int *__restrict__ wd_out,
                                                         DevClock *clk, double h0, double velzero, int phase,
@@ -437,8 +491,31 @@ __global__ void __launch_bounds__(BS, 768 / BS) k_limit(MeshDev m, double *__res
 {
     const int el = blockIdx.x * BS + threadIdx.x;
     if (el < m.ne)
+        limit_item<LIMIT, PDOP, STATUS, false, DGR_LIMIT_RCP>(m, S, bounds, wd_in, wd_out, clk, h0, velzero, phase,
+                                                             dec_limit, dec_pdop, el);
+}
+
+/* The elements k_limit queued (m.redo, as k_edge_redo), with plain divisions, from their
+ * state as k_limit left it (untouched).  The last block to finish clears the queue. */
+template <bool LIMIT, bool PDOP, bool STATUS>
+__global__ void __launch_bounds__(128) k_limit_redo(const __grid_constant__ MeshDev m, double *__restrict__ S,
+                                                    const double *__restrict__ bounds, const int *__restrict__ wd_in,
+                                                    int *__restrict__ wd_out, DevClock *clk, double h0,
+                                                    double velzero, int phase, int *__restrict__ dec_limit,
+                                                    int *__restrict__ dec_pdop)
+{
+    const int n = *(volatile int *)&m.redo[0];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
         limit_item<LIMIT, PDOP, STATUS>(m, S, bounds, wd_in, wd_out, clk, h0, velzero, phase, dec_limit, dec_pdop,
-                                        el);
+                                        m.redo[2 + k]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&m.redo[1], 1) == (int)gridDim.x - 1) {
+            m.redo[0] = 0;
+            m.redo[1] = 0;
+        }
+    }
 }
 
 /* ------------------------------------------------------------------ clock ---- */
@@ -642,7 +719,7 @@ DGR_DEV bool grid_barrier(unsigned *bar, unsigned polls, unsigned phantom)
  * (COH loads).  Same items, same arithmetic: results are identical to the separate kernels.
  */
 template <bool WD, int BS>
-__global__ void __launch_bounds__(BS, 512 / BS) k_step_fused(FusedArgs a, int stage_begin, int stage_end,
+__global__ void __launch_bounds__(BS, 512 / BS) k_step_fused(const __grid_constant__ FusedArgs a, int stage_begin, int stage_end,
                                                              int with_clock)
 {
     if (with_clock) {

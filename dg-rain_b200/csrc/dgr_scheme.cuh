@@ -10,6 +10,8 @@
  */
 #pragma once
 
+#include <type_traits>
+
 #include "dgr_device.cuh"
 
 namespace dgr {
@@ -440,10 +442,19 @@ struct LimitTrace {
  * at the element's vertex k; zn are the vertex depths.  With TRACE the limiter's path is
  * recorded in *trace (values are unaffected).
  */
-template <bool LIMIT, bool PDOP, class T, class Bnd, bool TRACE = false>
+template <bool LIMIT, bool PDOP, class T, class Bnd, bool TRACE = false, class Div = PlainDiv>
 DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, double velzero, LimitDecisions &dec,
-                       LimitTrace *trace = nullptr)
+                       LimitTrace *trace = nullptr, Div *dv = nullptr)
 {
+    /* divisions by 3 and by the vertex depths: plain, or (Div = RcpDiv) through shared
+     * reciprocals (div_rcp, the same bits; dv->ok reports where that is not valid) */
+    constexpr bool rcp = std::is_same<Div, RcpDiv>::value;
+    const auto div3 = [&](const T &x) -> T {
+        if constexpr (rcp)
+            return dv->div(x, RcpDiv::By{3.0, 1.0 / 3});
+        else
+            return x / 3;
+    };
     dec.modify = 0;
     dec.mass_branch = 0;
     dec.mom_branch = 0;
@@ -461,7 +472,7 @@ DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, doub
                 vmax[k] = bnd(v, k, 0);
                 vmin[k] = bnd(v, k, 1);
             }
-            const T avg = (w1 + w2 + w3) / 3;
+            const T avg = div3(w1 + w2 + w3);
             if (v == 0) { /* :189-200 */
                 const T h1 = vx[0] + zn[0], h2 = vx[1] + zn[1], h3 = vx[2] + zn[2];
                 const T m0 = vmin[0] + zn[0], m1 = vmin[1] + zn[1], m2 = vmin[2] + zn[2];
@@ -482,7 +493,7 @@ DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, doub
              * the instruction cache (measured: 8 % off the limiter kernel rolled) */
 #pragma unroll 1
             for (int ll = 0; ll < 3; ++ll) { /* :254-299 */
-                const T sumloc = (vx[0] + vx[1] + vx[2]) / 3;
+                const T sumloc = div3(vx[0] + vx[1] + vx[2]);
                 T sumdiff = (sumloc - avg) * 3;
                 const int sd = sgn(sumdiff);
                 const double sdd = (double)sd;
@@ -494,7 +505,12 @@ DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, doub
                     const double div = fmax(1.0, kdp);
                     T redfac;
                     if (diff[k] > 0) {
-                        redfac = div_by_count(T(sumdiff * sdd), div);
+                        if constexpr (rcp) {
+                            const T x = sumdiff * sdd;
+                            redfac = div == 1.0 ? x : (div == 2.0 ? x * 0.5 : div3(x));
+                        } else {
+                            redfac = div_by_count(T(sumdiff * sdd), div);
+                        }
                         kdp -= 1;
                     } else {
                         redfac = 0;
@@ -531,7 +547,7 @@ DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, doub
         const T midz0 = 0.5 * (zn[0] + zn[1]), midz1 = 0.5 * (zn[1] + zn[2]), midz2 = 0.5 * (zn[2] + zn[0]);
         T mh0 = w[0][0] + midz0, mh1 = w[0][1] + midz1, mh2 = w[0][2] + midz2;
         T ht[3] = {mh0 - mh1 + mh2, mh0 + mh1 - mh2, -mh0 + mh1 + mh2};
-        const T avg_h = (ht[0] + ht[1] + ht[2]) / 3;
+        const T avg_h = div3(ht[0] + ht[1] + ht[2]);
         int code = 0;
         if (ht[0] <= h0 || ht[1] <= h0 || ht[2] <= h0) { /* :93-156 */
             if (avg_h <= h0) {
@@ -587,8 +603,14 @@ DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, doub
                 T u[3], vv[3];
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    u[i] = qxe[i] / ht[i];
-                    vv[i] = qye[i] / ht[i];
+                    if constexpr (rcp) {
+                        const auto by_h = dv->by(ht[i]);
+                        u[i] = dv->div(qxe[i], by_h);
+                        vv[i] = dv->div(qye[i], by_h);
+                    } else {
+                        u[i] = qxe[i] / ht[i];
+                        vv[i] = qye[i] / ht[i];
+                    }
                 }
                 int npos = 0;
                 T delu = 0, delv = 0;
@@ -625,11 +647,11 @@ DGR_HD void limit_core(T w[3][3], const Bnd &bnd, const T zn[3], double h0, doub
 DGR_HD int big_theta(double a) { return a > 0 ? 1 : 0; }
 
 /* wetDryStatus2D for one element (2DCode/wetDry2D.c:18-57). */
-DGR_HD int wd_status(const double mz[3], const double zn[3], int wd_prev, double h0)
+DGR_HD int wd_status(const double mz[3], const double zn[3], int wd_prev, double h0, RcpDiv *dv = nullptr)
 {
     const double zv[3] = {mz[0] - mz[1] + mz[2], mz[0] + mz[1] - mz[2], -mz[0] + mz[1] + mz[2]};
     const double h[3] = {zv[0] + zn[0], zv[1] + zn[1], zv[2] + zn[2]};
-    const double avg_h = (h[0] + h[1] + h[2]) / 3;
+    const double avg_h = dv ? dv->div(h[0] + h[1] + h[2], RcpDiv::By{3.0, 1.0 / 3}) : (h[0] + h[1] + h[2]) / 3;
     int imax = 0;
     double hmax = h[0];
     if (h[1] > hmax) { imax = 1; hmax = h[1]; }

@@ -10,9 +10,11 @@ import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 # DGRAIN_LIBRARY=checked selects the build whose kernels test every gathered index
-# (libdgrain_checked.so, compiled with -DDGR_CHECKED by build.py --checked)
-LIB_PATH = os.path.join(_HERE, "libdgrain_checked.so" if os.environ.get("DGRAIN_LIBRARY") == "checked"
-                        else "libdgrain.so")
+# (libdgrain_checked.so, compiled with -DDGR_CHECKED by build.py --checked); a path to a
+# .so selects that build of the same sources (build.py's `out`, e.g. for tuning sweeps)
+_choice = os.environ.get("DGRAIN_LIBRARY", "")
+LIB_PATH = (os.path.join(_HERE, "libdgrain_checked.so") if _choice == "checked"
+            else os.path.abspath(_choice) if _choice.endswith(".so") else os.path.join(_HERE, "libdgrain.so"))
 
 DGR_OK = 0
 DGR_ERR_NAN_FLUX = 1
