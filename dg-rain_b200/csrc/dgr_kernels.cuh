@@ -34,7 +34,7 @@
  * (div_rcp), queueing the items where that is not valid for a plain-division redo launch;
  * 0: plain divisions.  Chosen by measurement, overridable at build time. */
 #ifndef DGR_EDGE_RCP
-#define DGR_EDGE_RCP 0
+#define DGR_EDGE_RCP 1
 #endif
 #ifndef DGR_LIMIT_RCP
 #define DGR_LIMIT_RCP 1
