@@ -33,6 +33,15 @@
 /* 1: the edge and limiter kernels take their divisions through shared reciprocals
  * (div_rcp), queueing the items where that is not valid for a plain-division redo launch;
  * 0: plain divisions.  Chosen by measurement, overridable at build time. */
+/* Resident threads per SM requested for the element kernel (register cap 65536 / this). */
+#ifndef DGR_ELEMENT_THREADS_PER_SM
+#define DGR_ELEMENT_THREADS_PER_SM 384
+#endif
+/* 1: the forward element kernel reads the compact geometry (CompactGeo, 22 planes) and
+ * recomputes the rest; 0: the 63 precomputed planes. */
+#ifndef DGR_ELEMENT_COMPACT
+#define DGR_ELEMENT_COMPACT 1
+#endif
 #ifndef DGR_EDGE_RCP
 #define DGR_EDGE_RCP 1
 #endif
@@ -82,6 +91,7 @@ struct MeshDev {
     const int *e_in, *e_ex, *e_info; /* [nf]; info = k_in | k_ex<<2 | bdry<<4 */
     const double *e_geo;  /* [3][ldF] */
     const double *geo;    /* [NG][ldE] */
+    const double *geoc;   /* [NGC][ldE], the compact planes of the forward element kernel */
     const int *n2e_ptr, *n2e;
     const double *zn;     /* node depth [nn] */
     const int *el_sid;    /* scenario of each element, NULL for a single mesh */
@@ -325,15 +335,22 @@ DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, co
         qyr[k] = ldm<COH>(&S[(6 + k) * ld + el]);
     }
     const double local_g = (ldm<COH>(&wd[el]) == 0) ? 0.0 : g;
-    const auto geo = [G, ld](int j) { return G[(size_t)j * ld]; };
-    const PlaneZGeo zg{G, ld};
     const auto uin = [U, ld, el](int v, int k) { return ldm<COH>(&U[(3 * v + k) * ld + el]); };
     const double dt = (MODE == MODE_RHS) ? 0.0 : ldm<COH>(&ck->dt);
     double w[3][3], a[3];
-    bool rcp_ok = true;
+    bool rcp_ok = true, geo_ok = true;
+#if DGR_ELEMENT_COMPACT
+    (void)G;
+    const CompactGeo<RCP> cg{m.geoc + el, ld, &geo_ok};
+    element_core<MODE, double, CompactGeo<RCP>, CompactGeo<RCP>, decltype(uin), RCP>(
+        F, zr, qxr, qyr, cg, cg, uin, local_g, rain, dt, w, a, &rcp_ok);
+#else
+    const auto geo = [G, ld](int j) { return G[(size_t)j * ld]; };
+    const PlaneZGeo zg{G, ld};
     element_core<MODE, double, decltype(geo), PlaneZGeo, decltype(uin), RCP>(F, zr, qxr, qyr, geo, zg, uin, local_g,
                                                                           rain, dt, w, a, &rcp_ok);
-    if (RCP && !rcp_ok) {
+#endif
+    if (RCP && !(rcp_ok && geo_ok)) {
         element_item_plain<MODE, COH>(m, S, U, wd, flux, out, avg, clk, g, el);
         return;
     }
@@ -346,14 +363,18 @@ DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, co
 }
 
 template <int MODE, int BS>
-__global__ void __launch_bounds__(BS, 512 / BS) k_element(const __grid_constant__ MeshDev m, const double *__restrict__ S,
+__global__ void __launch_bounds__(BS, DGR_ELEMENT_THREADS_PER_SM / BS) k_element(const __grid_constant__ MeshDev m, const double *__restrict__ S,
                                                           const double *__restrict__ U, const int *__restrict__ wd,
                                                           const double *__restrict__ flux, double *__restrict__ out,
                                                           double *__restrict__ avg, const DevClock *clk, double g)
 {
-    /* the block's 63 geometry planes are requested from DRAM at once instead of in the
-     * order the element computation reaches them (measured: 4 % off this kernel) */
+    /* the block's geometry planes are requested from DRAM at once instead of in the order
+     * the element computation reaches them (measured: 4 % off this kernel) */
+#if DGR_ELEMENT_COMPACT
+    l2_prefetch_slice(m.geoc, m.ldE, NGC, blockIdx.x * BS, min(BS, m.ne - blockIdx.x * BS));
+#else
     l2_prefetch_slice(m.geo, m.ldE, NG, blockIdx.x * BS, min(BS, m.ne - blockIdx.x * BS));
+#endif
     const int el = blockIdx.x * BS + threadIdx.x;
     if (el < m.ne) element_item<MODE>(m, S, U, wd, flux, out, avg, clk, g, el);
 }
@@ -828,7 +849,7 @@ static __global__ void k_edge_setup(int nf, int ldE, int ldF, const int *__restr
 static __global__ void k_element_setup(int ne, int ldE, const int *__restrict__ el2v_aos, const double *__restrict__ x,
                                 const double *__restrict__ y, const double *__restrict__ z,
                                 const double *__restrict__ nfric, const double *__restrict__ n_el, double g,
-                                int *el2v, double *geo)
+                                int *el2v, double *geo, double *geoc)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ne) return;
@@ -841,6 +862,12 @@ static __global__ void k_element_setup(int ne, int ldE, const int *__restrict__ 
     double *G = geo + i;
     element_geometry(xv, yv, zv, nfv, n_el ? n_el[i] : -1.0, g,
                      [G, ldE](int j, double val) { G[(size_t)j * ldE] = val; });
+    /* the compact planes: the same values, and element_geometry's edge midpoints */
+    const double xm[3] = {(xv[0] + xv[1]) / 2, (xv[1] + xv[2]) / 2, (xv[2] + xv[0]) / 2};
+    const double ym[3] = {(yv[0] + yv[1]) / 2, (yv[1] + yv[2]) / 2, (yv[2] + yv[0]) / 2};
+    double *Gc = geoc + i;
+    compact_geometry([G, ldE](int j) { return G[(size_t)j * ldE]; }, xm, ym,
+                     [Gc, ldE](int j, double val) { Gc[(size_t)j * ldE] = val; });
 }
 
 /* the Manning power on n arguments (diagnostic entry point) */

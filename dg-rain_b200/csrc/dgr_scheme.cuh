@@ -132,6 +132,130 @@ DGR_HD void element_geometry(const double xv[3], const double yv[3], const doubl
     set(G_M11, 6 / fabs(jv));
 }
 
+/*
+ * Compact element geometry: the planes the forward element kernel keeps in memory (22 of
+ * element_geometry's 63, 176 B per element), the rest recomputed from them on the fly with
+ * element_geometry's own expressions, so every value has the bits of the full plane:
+ *   kept        normals, edge Jacobians, mid-edge depths, g n^2, 6/|J|, and the three edge
+ *               midpoints (x1..x3, y1..y3, which the full layout does not hold);
+ *   recomputed  Gauss points (/sqrt 3), basis values at them (/den), the RT0 matrix column
+ *               and determinant, the Jacobian and grad psi (4/jac), grad psi . (sum of
+ *               midpoints), grad z, |jac| and |jac|/6.
+ * RCP: the divisions by sqrt 3 and by den take div_rcp (the same bits), clearing *ok where
+ * that path is not valid; otherwise plain divisions.
+ */
+enum { GC_NX = 0, GC_NY = 3, GC_EJ = 6, GC_XM = 9, GC_YM = 12, GC_MIDZ = 15, GC_GNN = 18, GC_M11 = 21, NGC = 22 };
+
+/* the compact planes from the full geometry and the midpoints (element_geometry's x1..y3) */
+template <class GetG, class SetC>
+DGR_HD void compact_geometry(const GetG &full, const double xm[3], const double ym[3], const SetC &set)
+{
+    for (int k = 0; k < 3; ++k) {
+        set(GC_NX + k, full(G_NX + k));
+        set(GC_NY + k, full(G_NY + k));
+        set(GC_EJ + k, full(G_EJ + k));
+        set(GC_XM + k, xm[k]);
+        set(GC_YM + k, ym[k]);
+        set(GC_MIDZ + k, full(G_MIDZ + k));
+        set(GC_GNN + k, full(G_GNN + k));
+    }
+    set(GC_M11, full(G_M11));
+}
+
+template <bool RCP>
+struct CompactGeo {
+    const double *C; /* this element's first compact plane */
+    int ld;
+    bool *ok;
+    DGR_HD double c(int j) const { return C[(size_t)j * ld]; }
+    DGR_HD double x(int k) const { return c(GC_XM + k); }
+    DGR_HD double y(int k) const { return c(GC_YM + k); }
+    DGR_HD double by_s3(double a) const
+    {
+        const double s3 = sqrt(3.0);
+        if constexpr (RCP) return div_rcp(a, s3, 1.0 / s3, *ok);
+        else return a / s3;
+    }
+    DGR_HD double den() const
+    {
+        const double x1 = x(0), x2 = x(1), x3 = x(2), y1 = y(0), y2 = y(1), y3 = y(2);
+        return x1 * y2 - x1 * y3 + x2 * y3 - x2 * y1 + x3 * y1 - x3 * y2;
+    }
+    DGR_HD double by_den(double a) const
+    {
+        const double d = den();
+        if constexpr (RCP) {
+            *ok = *ok && rcp_divisor_ok(d);
+            return div_rcp(a, d, 1.0 / d, *ok);
+        } else {
+            return a / d;
+        }
+    }
+    /* Gauss point n of edge e, element_geometry's xe/ye */
+    DGR_HD double xe(int e, int n) const { return gauss(e, n, x(0), x(1), x(2)); }
+    DGR_HD double ye(int e, int n) const { return gauss(e, n, y(0), y(1), y(2)); }
+    DGR_HD double gauss(int e, int n, double p1, double p2, double p3) const
+    {
+        const double s3 = sqrt(3.0);
+        if (e == 0) return n == 0 ? by_s3(s3 * p1 - p2 + p3) : by_s3(s3 * p1 + p2 - p3);
+        if (e == 1) return n == 0 ? by_s3(p1 + s3 * p2 - p3) : by_s3(-p1 + s3 * p2 + p3);
+        return n == 0 ? by_s3(-p1 + p2 + s3 * p3) : by_s3(p1 - p2 + s3 * p3);
+    }
+    DGR_HD double psi(int b, int e, int n) const
+    {
+        const double x1 = x(0), x2 = x(1), x3 = x(2), y1 = y(0), y2 = y(1), y3 = y(2);
+        const double xq = xe(e, n), yq = ye(e, n);
+        if (b == 0) return -by_den(yq * x2 - yq * x3 - xq * y2 + x3 * y2 + xq * y3 - x2 * y3);
+        if (b == 1) return -by_den(-x1 * yq + x3 * yq - x3 * y1 + xq * y1 - xq * y3 + x1 * y3);
+        return -by_den(yq * x1 - yq * x2 - xq * y1 + x2 * y1 + xq * y2 - x1 * y2);
+    }
+    DGR_HD double jac() const
+    {
+        const double x1 = x(0), x2 = x(1), x3 = x(2), y1 = y(0), y2 = y(1), y3 = y(2);
+        return 4 * (x2 - x3) * (y2 - y1) - 4 * (x2 - x1) * (y2 - y3);
+    }
+    DGR_HD double gp(int b, int j) const
+    {
+        const double t = 4 / jac();
+        const double x1 = x(0), x2 = x(1), x3 = x(2), y1 = y(0), y2 = y(1), y3 = y(2);
+        if (b == 0) return j == 0 ? t * (y2 - y3) : t * (x3 - x2);
+        if (b == 1) return j == 0 ? t * (y3 - y1) : t * (x1 - x3);
+        return j == 0 ? t * (y1 - y2) : t * (x2 - x1);
+    }
+    DGR_HD double m12(int k) const { return x(k) * c(GC_NX + k) + y(k) * c(GC_NY + k); }
+    DGR_HD double dm() const
+    {
+        const double M11 = c(GC_NX), M12 = m12(0), M13 = c(GC_NY);
+        const double M21 = c(GC_NX + 1), M22 = m12(1), M23 = c(GC_NY + 1);
+        const double M31 = c(GC_NX + 2), M32 = m12(2), M33 = c(GC_NY + 2);
+        return M13 * M22 * M31 - M12 * M23 * M31 - M13 * M21 * M32 + M11 * M23 * M32 + M12 * M21 * M33 -
+               M11 * M22 * M33;
+    }
+    /* the full layout's plane j */
+    DGR_HD double operator()(int j) const
+    {
+        if (j < G_NY + 3) return c(GC_NX + j); /* G_NX, G_NY */
+        if (j < G_DM) return m12(j - G_M12);
+        if (j == G_DM) return dm();
+        if (j < G_YE) return xe((j - G_XE) / 2, (j - G_XE) % 2);
+        if (j < G_EJ) return ye((j - G_YE) / 2, (j - G_YE) % 2);
+        if (j < G_PSI) return c(GC_EJ + j - G_EJ);
+        if (j < G_MIDZ) return psi((j - G_PSI) / 6, ((j - G_PSI) % 6) / 2, (j - G_PSI) % 2);
+        if (j < G_GNN) return c(GC_MIDZ + j - G_MIDZ);
+        if (j < G_GP) return c(GC_GNN + j - G_GNN);
+        if (j < G_GRADZ) return gp((j - G_GP) / 2, (j - G_GP) % 2);
+        if (j < G_AJ) return gradz(j - G_GRADZ);
+        if (j == G_AJ) return fabs(jac());
+        if (j < G_AJW) return gp(j - G_P, 0) * (x(0) + x(1) + x(2)) + gp(j - G_P, 1) * (y(0) + y(1) + y(2));
+        if (j == G_AJW) return fabs(jac()) * (1.0 / 6);
+        return c(GC_M11);
+    }
+    /* the ZGeo interface of element_core */
+    DGR_HD double midz(int e) const { return c(GC_MIDZ + e); }
+    DGR_HD double gnn(int e) const { return c(GC_GNN + e); }
+    DGR_HD double gradz(int j) const { return midz(0) * gp(0, j) + midz(1) * gp(1, j) + midz(2) * gp(2, j); }
+};
+
 /* Depth- and Manning-dependent element factors read from the geometry planes. */
 struct PlaneZGeo {
     const double *G;
@@ -292,26 +416,35 @@ DGR_HD void element_core(const T F[3][3], const T zr[3], const T qxr[3], const T
             rt0_fit(R1, R2, R3, M11, M12, M13, M21, M22, M23, M31, M32, M33, dM, a, b, c);
     };
 
-    /* surface integrals SI[9] (:95-239) */
+    /* surface integrals SI[9] (:95-239), edge by edge: the three fits first, then per edge
+     * its two Gauss points and basis values, each variable's normal fluxes there and their
+     * products, added to si in the reference's order (edge 0, 1, 2); every value is the
+     * reference's expression, only evaluated in this order (fewer values live at once) */
     T si[9];
     {
-        const double ej0 = geo(G_EJ), ej1 = geo(G_EJ + 1), ej2 = geo(G_EJ + 2);
+        T fa[3], fb[3], fc[3];
 #pragma unroll
-        for (int v = 0; v < 3; ++v) {
-            T a, b, c;
-            fit(F[v][0], F[v][1], F[v][2], a, b, c);
-            T fd[3][2];
+        for (int v = 0; v < 3; ++v) fit(F[v][0], F[v][1], F[v][2], fa[v], fb[v], fc[v]);
 #pragma unroll
-            for (int e = 0; e < 3; ++e)
-#pragma unroll
-                for (int n = 0; n < 2; ++n)
-                    fd[e][n] = (a + b * geo(G_XE + 2 * e + n)) * nx[e] + (c + b * geo(G_YE + 2 * e + n)) * ny[e];
+        for (int e = 0; e < 3; ++e) {
+            const double ej = geo(G_EJ + e);
+            const double xq[2] = {geo(G_XE + 2 * e), geo(G_XE + 2 * e + 1)};
+            const double yq[2] = {geo(G_YE + 2 * e), geo(G_YE + 2 * e + 1)};
+            double ps[3][2];
 #pragma unroll
             for (int bf = 0; bf < 3; ++bf) {
-                const int p = G_PSI + 6 * bf;
-                si[3 * v + bf] = ej0 * (fd[0][0] * geo(p) + fd[0][1] * geo(p + 1)) +
-                                 ej1 * (fd[1][0] * geo(p + 2) + fd[1][1] * geo(p + 3)) +
-                                 ej2 * (fd[2][0] * geo(p + 4) + fd[2][1] * geo(p + 5));
+                ps[bf][0] = geo(G_PSI + 6 * bf + 2 * e);
+                ps[bf][1] = geo(G_PSI + 6 * bf + 2 * e + 1);
+            }
+#pragma unroll
+            for (int v = 0; v < 3; ++v) {
+                const T fd0 = (fa[v] + fb[v] * xq[0]) * nx[e] + (fc[v] + fb[v] * yq[0]) * ny[e];
+                const T fd1 = (fa[v] + fb[v] * xq[1]) * nx[e] + (fc[v] + fb[v] * yq[1]) * ny[e];
+#pragma unroll
+                for (int bf = 0; bf < 3; ++bf) {
+                    const T term = ej * (fd0 * ps[bf][0] + fd1 * ps[bf][1]);
+                    si[3 * v + bf] = e == 0 ? term : si[3 * v + bf] + term;
+                }
             }
         }
     }
