@@ -77,7 +77,7 @@ static void release(dgr_ctx *c)
     drop_graph(c);
     void *ptrs[] = {c->x, c->y, c->zn, c->nfric, c->n_el, c->el2v_aos, c->el2v, c->elem_edge, c->e_in, c->redo,
                     c->e_ex, c->e_info, c->n2e_ptr, c->n2e, c->bnd_edges, c->bnd_type, c->bnd_sid, c->bdry,
-                    c->el_sid, c->ed_sid, c->e_geo, c->geo, c->geoc, c->U, c->W, c->flux, c->avg, c->bounds, c->bzeta,
+                    c->el_sid, c->ed_sid, c->e_geo, c->geo, c->U, c->W, c->flux, c->avg, c->bounds, c->bzeta,
                     c->bqn, c->bstage, c->wdA, c->wdB, c->wdC, c->dec, c->bar, c->clk, c->p2g,
                     c->gauge_el, c->gauge_sid, c->gauge_w, c->gauge_series};
     for (void *q : ptrs)
@@ -95,7 +95,7 @@ static void release(dgr_ctx *c)
 int upload_geometry(dgr_ctx *c)
 {
     k_element_setup<<<blocks(c->ne, 128), 128, 0, c->stream>>>(c->ne, c->ldE, c->el2v_aos, c->x, c->y, c->zn,
-                                                               c->nfric, c->n_el, c->p.g, c->el2v, c->geo, c->geoc);
+                                                               c->nfric, c->n_el, c->p.g, c->el2v, c->geo);
     c->launches++;
     if (c->p.order == 2) {
         k_p2_setup<<<blocks(c->ne, 256), 256, 0, c->stream>>>(c->ne, c->ldE, c->el2v_aos, c->x, c->y, c->zn,
@@ -292,7 +292,6 @@ static int create_impl(int nscen, const dgr_mesh_view *views, const dgr_scenario
     TRY(dalloc(&c->bdry, nf));
     TRY(dalloc(&c->e_geo, 3 * lF));
     TRY(dalloc(&c->geo, (size_t)NG * lE));
-    TRY(dalloc(&c->geoc, (size_t)NGC * lE));
     const size_t nst = 3 * (size_t)c->nm;
     TRY(dalloc(&c->U, nst * lE));
     TRY(dalloc(&c->W, nst * lE));

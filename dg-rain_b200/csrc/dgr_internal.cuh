@@ -73,7 +73,6 @@ struct dgr_ctx {
     int *el2v_aos, *el2v, *elem_edge, *e_in, *e_ex, *e_info, *n2e_ptr, *n2e, *bnd_edges, *bnd_type, *bnd_sid;
     int *bdry, *el_sid, *ed_sid;
     double *e_geo, *geo;
-    double *geoc; /* compact planes of the forward element kernel [NGC][ldE] */
     /* state and work */
     double *U, *W, *flux, *avg, *bounds, *bzeta, *bqn, *bstage;
     int *wdA, *wdB, *wdC; /* wet/dry flags: stage s reads buffer s, writes buffer (s+1) mod stages */
@@ -133,7 +132,6 @@ static inline dgr::MeshDev mesh_dev(const dgr_ctx *c)
     m.e_info = c->e_info;
     m.e_geo = c->e_geo;
     m.geo = c->geo;
-    m.geoc = c->geoc;
     m.n2e_ptr = c->n2e_ptr;
     m.n2e = c->n2e;
     m.zn = c->zn;

@@ -33,14 +33,14 @@
 /* 1: the edge and limiter kernels take their divisions through shared reciprocals
  * (div_rcp), queueing the items where that is not valid for a plain-division redo launch;
  * 0: plain divisions.  Chosen by measurement, overridable at build time. */
-/* Resident threads per SM requested for the element kernel (register cap 65536 / this). */
-#ifndef DGR_ELEMENT_THREADS_PER_SM
-#define DGR_ELEMENT_THREADS_PER_SM 384
+/* 1: the forward edge kernel makes its one to three flux calls with one copy of the flux
+ * code in a loop (flux_core_rolled); 0: three inlined copies (flux_core). */
+#ifndef DGR_EDGE_ROLLED
+#define DGR_EDGE_ROLLED 1
 #endif
-/* 1: the forward element kernel reads the compact geometry (CompactGeo, 22 planes) and
- * recomputes the rest; 0: the 63 precomputed planes. */
-#ifndef DGR_ELEMENT_COMPACT
-#define DGR_ELEMENT_COMPACT 1
+/* Resident threads per SM requested for the limiter kernel (register cap 65536 / this). */
+#ifndef DGR_LIMIT_THREADS_PER_SM
+#define DGR_LIMIT_THREADS_PER_SM 768
 #endif
 #ifndef DGR_EDGE_RCP
 #define DGR_EDGE_RCP 1
@@ -91,7 +91,6 @@ struct MeshDev {
     const int *e_in, *e_ex, *e_info; /* [nf]; info = k_in | k_ex<<2 | bdry<<4 */
     const double *e_geo;  /* [3][ldF] */
     const double *geo;    /* [NG][ldE] */
-    const double *geoc;   /* [NGC][ldE], the compact planes of the forward element kernel */
     const int *n2e_ptr, *n2e;
     const double *zn;     /* node depth [nn] */
     const int *el_sid;    /* scenario of each element, NULL for a single mesh */
@@ -179,16 +178,21 @@ DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, 
         int code;
         if (redo) {
             RcpDiv dv;
+#if DGR_EDGE_ROLLED
+            lam = flux_core_rolled<WD, RcpDiv>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex,
+                                               code, FT >= 0 ? FT : m.flux, &dv);
+#else
             lam = flux_core<double, WD, RcpDiv>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex,
                                                 code, FT >= 0 ? FT : m.flux, &dv);
+#endif
             if (!dv.ok) { /* k_edge_redo rewrites this edge's fluxes, error and speed */
                 *redo = true;
                 code = 0;
                 lam = 0.0;
             }
         } else {
-            lam = flux_core<double, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code,
-                                        FT >= 0 ? FT : m.flux);
+            lam = flux_core_rolled<WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code,
+                                       FT >= 0 ? FT : m.flux);
         }
         if (code) atomicMin(&ck->err, err_key(ldm<COH>(&ck->step), phase, code, i - ck->ed_off));
         const int lf = m.ldF;
@@ -338,19 +342,12 @@ DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, co
     const auto uin = [U, ld, el](int v, int k) { return ldm<COH>(&U[(3 * v + k) * ld + el]); };
     const double dt = (MODE == MODE_RHS) ? 0.0 : ldm<COH>(&ck->dt);
     double w[3][3], a[3];
-    bool rcp_ok = true, geo_ok = true;
-#if DGR_ELEMENT_COMPACT
-    (void)G;
-    const CompactGeo<RCP> cg{m.geoc + el, ld, &geo_ok};
-    element_core<MODE, double, CompactGeo<RCP>, CompactGeo<RCP>, decltype(uin), RCP>(
-        F, zr, qxr, qyr, cg, cg, uin, local_g, rain, dt, w, a, &rcp_ok);
-#else
+    bool rcp_ok = true;
     const auto geo = [G, ld](int j) { return G[(size_t)j * ld]; };
     const PlaneZGeo zg{G, ld};
     element_core<MODE, double, decltype(geo), PlaneZGeo, decltype(uin), RCP>(F, zr, qxr, qyr, geo, zg, uin, local_g,
                                                                           rain, dt, w, a, &rcp_ok);
-#endif
-    if (RCP && !(rcp_ok && geo_ok)) {
+    if (RCP && !rcp_ok) {
         element_item_plain<MODE, COH>(m, S, U, wd, flux, out, avg, clk, g, el);
         return;
     }
@@ -363,18 +360,14 @@ DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, co
 }
 
 template <int MODE, int BS>
-__global__ void __launch_bounds__(BS, DGR_ELEMENT_THREADS_PER_SM / BS) k_element(const __grid_constant__ MeshDev m, const double *__restrict__ S,
+__global__ void __launch_bounds__(BS, 512 / BS) k_element(const __grid_constant__ MeshDev m, const double *__restrict__ S,
                                                           const double *__restrict__ U, const int *__restrict__ wd,
                                                           const double *__restrict__ flux, double *__restrict__ out,
                                                           double *__restrict__ avg, const DevClock *clk, double g)
 {
     /* the block's geometry planes are requested from DRAM at once instead of in the order
      * the element computation reaches them (measured: 4 % off this kernel) */
-#if DGR_ELEMENT_COMPACT
-    l2_prefetch_slice(m.geoc, m.ldE, NGC, blockIdx.x * BS, min(BS, m.ne - blockIdx.x * BS));
-#else
     l2_prefetch_slice(m.geo, m.ldE, NG, blockIdx.x * BS, min(BS, m.ne - blockIdx.x * BS));
-#endif
     const int el = blockIdx.x * BS + threadIdx.x;
     if (el < m.ne) element_item<MODE>(m, S, U, wd, flux, out, avg, clk, g, el);
 }
@@ -504,7 +497,7 @@ DGR_DEV void limit_item(const MeshDev &m, double *S, const double *bounds, const
 }
 
 template <bool LIMIT, bool PDOP, bool STATUS, int BS>
-__global__ void __launch_bounds__(BS, 768 / BS) k_limit(const __grid_constant__ MeshDev m, double *__restrict__ S,
+__global__ void __launch_bounds__(BS, DGR_LIMIT_THREADS_PER_SM / BS) k_limit(const __grid_constant__ MeshDev m, double *__restrict__ S,
                                                         const double *__restrict__ bounds,
                                                         const int *__restrict__ wd_in, int *__restrict__ wd_out,
                                                         DevClock *clk, double h0, double velzero, int phase,
@@ -849,7 +842,7 @@ static __global__ void k_edge_setup(int nf, int ldE, int ldF, const int *__restr
 static __global__ void k_element_setup(int ne, int ldE, const int *__restrict__ el2v_aos, const double *__restrict__ x,
                                 const double *__restrict__ y, const double *__restrict__ z,
                                 const double *__restrict__ nfric, const double *__restrict__ n_el, double g,
-                                int *el2v, double *geo, double *geoc)
+                                int *el2v, double *geo)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ne) return;
@@ -862,12 +855,6 @@ static __global__ void k_element_setup(int ne, int ldE, const int *__restrict__ 
     double *G = geo + i;
     element_geometry(xv, yv, zv, nfv, n_el ? n_el[i] : -1.0, g,
                      [G, ldE](int j, double val) { G[(size_t)j * ldE] = val; });
-    /* the compact planes: the same values, and element_geometry's edge midpoints */
-    const double xm[3] = {(xv[0] + xv[1]) / 2, (xv[1] + xv[2]) / 2, (xv[2] + xv[0]) / 2};
-    const double ym[3] = {(yv[0] + yv[1]) / 2, (yv[1] + yv[2]) / 2, (yv[2] + yv[0]) / 2};
-    double *Gc = geoc + i;
-    compact_geometry([G, ldE](int j) { return G[(size_t)j * ldE]; }, xm, ym,
-                     [Gc, ldE](int j, double val) { Gc[(size_t)j * ldE] = val; });
 }
 
 /* the Manning power on n arguments (diagnostic entry point) */

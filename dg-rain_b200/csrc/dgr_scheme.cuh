@@ -132,130 +132,6 @@ DGR_HD void element_geometry(const double xv[3], const double yv[3], const doubl
     set(G_M11, 6 / fabs(jv));
 }
 
-/*
- * Compact element geometry: the planes the forward element kernel keeps in memory (22 of
- * element_geometry's 63, 176 B per element), the rest recomputed from them on the fly with
- * element_geometry's own expressions, so every value has the bits of the full plane:
- *   kept        normals, edge Jacobians, mid-edge depths, g n^2, 6/|J|, and the three edge
- *               midpoints (x1..x3, y1..y3, which the full layout does not hold);
- *   recomputed  Gauss points (/sqrt 3), basis values at them (/den), the RT0 matrix column
- *               and determinant, the Jacobian and grad psi (4/jac), grad psi . (sum of
- *               midpoints), grad z, |jac| and |jac|/6.
- * RCP: the divisions by sqrt 3 and by den take div_rcp (the same bits), clearing *ok where
- * that path is not valid; otherwise plain divisions.
- */
-enum { GC_NX = 0, GC_NY = 3, GC_EJ = 6, GC_XM = 9, GC_YM = 12, GC_MIDZ = 15, GC_GNN = 18, GC_M11 = 21, NGC = 22 };
-
-/* the compact planes from the full geometry and the midpoints (element_geometry's x1..y3) */
-template <class GetG, class SetC>
-DGR_HD void compact_geometry(const GetG &full, const double xm[3], const double ym[3], const SetC &set)
-{
-    for (int k = 0; k < 3; ++k) {
-        set(GC_NX + k, full(G_NX + k));
-        set(GC_NY + k, full(G_NY + k));
-        set(GC_EJ + k, full(G_EJ + k));
-        set(GC_XM + k, xm[k]);
-        set(GC_YM + k, ym[k]);
-        set(GC_MIDZ + k, full(G_MIDZ + k));
-        set(GC_GNN + k, full(G_GNN + k));
-    }
-    set(GC_M11, full(G_M11));
-}
-
-template <bool RCP>
-struct CompactGeo {
-    const double *C; /* this element's first compact plane */
-    int ld;
-    bool *ok;
-    DGR_HD double c(int j) const { return C[(size_t)j * ld]; }
-    DGR_HD double x(int k) const { return c(GC_XM + k); }
-    DGR_HD double y(int k) const { return c(GC_YM + k); }
-    DGR_HD double by_s3(double a) const
-    {
-        const double s3 = sqrt(3.0);
-        if constexpr (RCP) return div_rcp(a, s3, 1.0 / s3, *ok);
-        else return a / s3;
-    }
-    DGR_HD double den() const
-    {
-        const double x1 = x(0), x2 = x(1), x3 = x(2), y1 = y(0), y2 = y(1), y3 = y(2);
-        return x1 * y2 - x1 * y3 + x2 * y3 - x2 * y1 + x3 * y1 - x3 * y2;
-    }
-    DGR_HD double by_den(double a) const
-    {
-        const double d = den();
-        if constexpr (RCP) {
-            *ok = *ok && rcp_divisor_ok(d);
-            return div_rcp(a, d, 1.0 / d, *ok);
-        } else {
-            return a / d;
-        }
-    }
-    /* Gauss point n of edge e, element_geometry's xe/ye */
-    DGR_HD double xe(int e, int n) const { return gauss(e, n, x(0), x(1), x(2)); }
-    DGR_HD double ye(int e, int n) const { return gauss(e, n, y(0), y(1), y(2)); }
-    DGR_HD double gauss(int e, int n, double p1, double p2, double p3) const
-    {
-        const double s3 = sqrt(3.0);
-        if (e == 0) return n == 0 ? by_s3(s3 * p1 - p2 + p3) : by_s3(s3 * p1 + p2 - p3);
-        if (e == 1) return n == 0 ? by_s3(p1 + s3 * p2 - p3) : by_s3(-p1 + s3 * p2 + p3);
-        return n == 0 ? by_s3(-p1 + p2 + s3 * p3) : by_s3(p1 - p2 + s3 * p3);
-    }
-    DGR_HD double psi(int b, int e, int n) const
-    {
-        const double x1 = x(0), x2 = x(1), x3 = x(2), y1 = y(0), y2 = y(1), y3 = y(2);
-        const double xq = xe(e, n), yq = ye(e, n);
-        if (b == 0) return -by_den(yq * x2 - yq * x3 - xq * y2 + x3 * y2 + xq * y3 - x2 * y3);
-        if (b == 1) return -by_den(-x1 * yq + x3 * yq - x3 * y1 + xq * y1 - xq * y3 + x1 * y3);
-        return -by_den(yq * x1 - yq * x2 - xq * y1 + x2 * y1 + xq * y2 - x1 * y2);
-    }
-    DGR_HD double jac() const
-    {
-        const double x1 = x(0), x2 = x(1), x3 = x(2), y1 = y(0), y2 = y(1), y3 = y(2);
-        return 4 * (x2 - x3) * (y2 - y1) - 4 * (x2 - x1) * (y2 - y3);
-    }
-    DGR_HD double gp(int b, int j) const
-    {
-        const double t = 4 / jac();
-        const double x1 = x(0), x2 = x(1), x3 = x(2), y1 = y(0), y2 = y(1), y3 = y(2);
-        if (b == 0) return j == 0 ? t * (y2 - y3) : t * (x3 - x2);
-        if (b == 1) return j == 0 ? t * (y3 - y1) : t * (x1 - x3);
-        return j == 0 ? t * (y1 - y2) : t * (x2 - x1);
-    }
-    DGR_HD double m12(int k) const { return x(k) * c(GC_NX + k) + y(k) * c(GC_NY + k); }
-    DGR_HD double dm() const
-    {
-        const double M11 = c(GC_NX), M12 = m12(0), M13 = c(GC_NY);
-        const double M21 = c(GC_NX + 1), M22 = m12(1), M23 = c(GC_NY + 1);
-        const double M31 = c(GC_NX + 2), M32 = m12(2), M33 = c(GC_NY + 2);
-        return M13 * M22 * M31 - M12 * M23 * M31 - M13 * M21 * M32 + M11 * M23 * M32 + M12 * M21 * M33 -
-               M11 * M22 * M33;
-    }
-    /* the full layout's plane j */
-    DGR_HD double operator()(int j) const
-    {
-        if (j < G_NY + 3) return c(GC_NX + j); /* G_NX, G_NY */
-        if (j < G_DM) return m12(j - G_M12);
-        if (j == G_DM) return dm();
-        if (j < G_YE) return xe((j - G_XE) / 2, (j - G_XE) % 2);
-        if (j < G_EJ) return ye((j - G_YE) / 2, (j - G_YE) % 2);
-        if (j < G_PSI) return c(GC_EJ + j - G_EJ);
-        if (j < G_MIDZ) return psi((j - G_PSI) / 6, ((j - G_PSI) % 6) / 2, (j - G_PSI) % 2);
-        if (j < G_GNN) return c(GC_MIDZ + j - G_MIDZ);
-        if (j < G_GP) return c(GC_GNN + j - G_GNN);
-        if (j < G_GRADZ) return gp((j - G_GP) / 2, (j - G_GP) % 2);
-        if (j < G_AJ) return gradz(j - G_GRADZ);
-        if (j == G_AJ) return fabs(jac());
-        if (j < G_AJW) return gp(j - G_P, 0) * (x(0) + x(1) + x(2)) + gp(j - G_P, 1) * (y(0) + y(1) + y(2));
-        if (j == G_AJW) return fabs(jac()) * (1.0 / 6);
-        return c(GC_M11);
-    }
-    /* the ZGeo interface of element_core */
-    DGR_HD double midz(int e) const { return c(GC_MIDZ + e); }
-    DGR_HD double gnn(int e) const { return c(GC_GNN + e); }
-    DGR_HD double gradz(int j) const { return midz(0) * gp(0, j) + midz(1) * gp(1, j) + midz(2) * gp(2, j); }
-};
-
 /* Depth- and Manning-dependent element factors read from the geometry planes. */
 struct PlaneZGeo {
     const double *G;
@@ -357,6 +233,72 @@ DGR_HD T flux_core(const T &zi, const T &qxi, const T &qyi, const T &ze, const T
                 numerical_flux<T, Div>(ftype, fex, zi, ze, qxi, qxe, qyi, qye, z_edge, nx, ny, 0.0, g, dv);
             if (!code && (isnan(fex[0]) || isnan(fex[1]) || isnan(fex[2]))) code = 3;
             lam = rmax(lam, l2);
+        }
+    }
+    return lam;
+}
+
+/*
+ * flux_core for the forward kernels (doubles), with its one to three numerical-flux calls
+ * made by one copy of the flux code in a loop instead of three inlined copies (fewer
+ * registers).  The calls, their arguments, the order in which their wave speeds are
+ * combined and the NaN checks are flux_core's, so the results are the same bits.
+ */
+template <bool WD, class Div = PlainDiv>
+DGR_DEV double flux_core_rolled(double zi, double qxi, double qyi, double ze, double qxe, double qye,
+                                double z_edge, double nx, double ny, int wdi, int wde, double g, double fin[3],
+                                double fex[3], int &code, int ftype = 0, Div *dv = nullptr)
+{
+    const double tx = -ny, ty = nx;
+    code = 0;
+    /* roles: 0 shared flux (g), 1 the dry in side's g = 0 flux, 2 the dry ex side's; both
+     * sides dry: 3 the in side's reflective flux, 4 the ex side's */
+    const bool both_dry = WD && wdi == 0 && wde == 0;
+    double qxe_ref = 0, qye_ref = 0, qxi_ref = 0, qyi_ref = 0;
+    if (both_dry) { /* :203-239 */
+        const double d = 1. / (nx * ty - ny * tx);
+        const double qn_in = qxi * nx + qyi * ny;
+        const double qt_in = qxi * tx + qyi * ty;
+        const double qn_ex0 = -qn_in, qt_ex0 = qt_in;
+        qxe_ref = (ty * qn_ex0 - ny * qt_ex0) * d;
+        qye_ref = (-tx * qn_ex0 + nx * qt_ex0) * d;
+        const double qn_ex = qxe * nx + qye * ny;
+        const double qt_ex = qxe * tx + qye * ty;
+        const double qn_in1 = -qn_ex, qt_in1 = qt_ex;
+        qxi_ref = (ty * qn_in1 - ny * qt_in1) * d;
+        qyi_ref = (-tx * qn_in1 + nx * qt_ex) * d;
+    }
+    unsigned roles = both_dry ? (3u | (4u << 3)) : (0u | ((WD && wdi != 1) ? (1u << 3) : (2u << 3)));
+    int ncalls = both_dry ? 2 : 1 + ((WD && wdi != 1) ? 1 : 0) + ((WD && wde != 1) ? 1 : 0);
+    if (!both_dry && WD && wdi != 1 && wde != 1) roles |= 2u << 6;
+    double lam = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < ncalls; ++k) {
+        const unsigned role = (roles >> (3 * k)) & 7u;
+        const double a_zi = role == 4 ? ze : zi;
+        const double a_ze = role == 3 ? zi : ze;
+        const double a_qxi = role == 4 ? qxi_ref : qxi, a_qyi = role == 4 ? qyi_ref : qyi;
+        const double a_qxe = role == 3 ? qxe_ref : qxe, a_qye = role == 3 ? qye_ref : qye;
+        const double lg = role == 0 ? g : 0.0;
+        double f[3];
+        const double l = numerical_flux<double, Div>(ftype, f, a_zi, a_ze, a_qxi, a_qxe, a_qyi, a_qye, z_edge, nx, ny,
+                                                     lg, g, dv);
+        const bool nan = isnan(f[0]) || isnan(f[1]) || isnan(f[2]);
+        if (role == 0) {
+            if (nan) code = 1;
+            lam = l;
+        } else if (role == 3) {
+            lam = l;
+        } else {
+            if (role != 4 && !code && nan) code = role == 1 ? 2 : 3;
+            lam = rmax(lam, l);
+        }
+        const bool to_in = role == 3 || role == 1 || (role == 0 && (!WD || wdi == 1));
+        const bool to_ex = role == 4 || role == 2 || (role == 0 && (!WD || wde == 1));
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            if (to_in) fin[j] = f[j];
+            if (to_ex) fex[j] = f[j];
         }
     }
     return lam;
