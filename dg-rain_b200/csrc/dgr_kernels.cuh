@@ -33,14 +33,11 @@
 /* 1: the edge and limiter kernels take their divisions through shared reciprocals
  * (div_rcp), queueing the items where that is not valid for a plain-division redo launch;
  * 0: plain divisions.  Chosen by measurement, overridable at build time. */
-/* 1: the forward edge kernel makes its one to three flux calls with one copy of the flux
- * code in a loop (flux_core_rolled); 0: three inlined copies (flux_core). */
-#ifndef DGR_EDGE_ROLLED
-#define DGR_EDGE_ROLLED 1
-#endif
-/* Resident threads per SM requested for the limiter kernel (register cap 65536 / this). */
+/* Resident threads per SM requested for the limiter kernel (register cap 65536 / this);
+ * chosen by measurement (1024: 64 registers, 0.244 ms at 4M triangles; 768: 80 registers,
+ * 0.271 ms; 512: 0.350 ms). */
 #ifndef DGR_LIMIT_THREADS_PER_SM
-#define DGR_LIMIT_THREADS_PER_SM 768
+#define DGR_LIMIT_THREADS_PER_SM 1024
 #endif
 #ifndef DGR_EDGE_RCP
 #define DGR_EDGE_RCP 1
@@ -178,21 +175,16 @@ DGR_DEV double edge_flux_item(const MeshDev &m, const double *S, const int *wd, 
         int code;
         if (redo) {
             RcpDiv dv;
-#if DGR_EDGE_ROLLED
-            lam = flux_core_rolled<WD, RcpDiv>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex,
-                                               code, FT >= 0 ? FT : m.flux, &dv);
-#else
             lam = flux_core<double, WD, RcpDiv>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex,
                                                 code, FT >= 0 ? FT : m.flux, &dv);
-#endif
             if (!dv.ok) { /* k_edge_redo rewrites this edge's fluxes, error and speed */
                 *redo = true;
                 code = 0;
                 lam = 0.0;
             }
         } else {
-            lam = flux_core_rolled<WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code,
-                                       FT >= 0 ? FT : m.flux);
+            lam = flux_core<double, WD>(zi, qxi, qyi, ze, qxe, qye, z_edge, nx, ny, wdi, wde, g, fin, fex, code,
+                                        FT >= 0 ? FT : m.flux);
         }
         if (code) atomicMin(&ck->err, err_key(ldm<COH>(&ck->step), phase, code, i - ck->ed_off));
         const int lf = m.ldF;

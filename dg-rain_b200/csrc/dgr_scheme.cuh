@@ -238,72 +238,6 @@ DGR_HD T flux_core(const T &zi, const T &qxi, const T &qyi, const T &ze, const T
     return lam;
 }
 
-/*
- * flux_core for the forward kernels (doubles), with its one to three numerical-flux calls
- * made by one copy of the flux code in a loop instead of three inlined copies (fewer
- * registers).  The calls, their arguments, the order in which their wave speeds are
- * combined and the NaN checks are flux_core's, so the results are the same bits.
- */
-template <bool WD, class Div = PlainDiv>
-DGR_DEV double flux_core_rolled(double zi, double qxi, double qyi, double ze, double qxe, double qye,
-                                double z_edge, double nx, double ny, int wdi, int wde, double g, double fin[3],
-                                double fex[3], int &code, int ftype = 0, Div *dv = nullptr)
-{
-    const double tx = -ny, ty = nx;
-    code = 0;
-    /* roles: 0 shared flux (g), 1 the dry in side's g = 0 flux, 2 the dry ex side's; both
-     * sides dry: 3 the in side's reflective flux, 4 the ex side's */
-    const bool both_dry = WD && wdi == 0 && wde == 0;
-    double qxe_ref = 0, qye_ref = 0, qxi_ref = 0, qyi_ref = 0;
-    if (both_dry) { /* :203-239 */
-        const double d = 1. / (nx * ty - ny * tx);
-        const double qn_in = qxi * nx + qyi * ny;
-        const double qt_in = qxi * tx + qyi * ty;
-        const double qn_ex0 = -qn_in, qt_ex0 = qt_in;
-        qxe_ref = (ty * qn_ex0 - ny * qt_ex0) * d;
-        qye_ref = (-tx * qn_ex0 + nx * qt_ex0) * d;
-        const double qn_ex = qxe * nx + qye * ny;
-        const double qt_ex = qxe * tx + qye * ty;
-        const double qn_in1 = -qn_ex, qt_in1 = qt_ex;
-        qxi_ref = (ty * qn_in1 - ny * qt_in1) * d;
-        qyi_ref = (-tx * qn_in1 + nx * qt_ex) * d;
-    }
-    unsigned roles = both_dry ? (3u | (4u << 3)) : (0u | ((WD && wdi != 1) ? (1u << 3) : (2u << 3)));
-    int ncalls = both_dry ? 2 : 1 + ((WD && wdi != 1) ? 1 : 0) + ((WD && wde != 1) ? 1 : 0);
-    if (!both_dry && WD && wdi != 1 && wde != 1) roles |= 2u << 6;
-    double lam = 0.0;
-#pragma unroll 1
-    for (int k = 0; k < ncalls; ++k) {
-        const unsigned role = (roles >> (3 * k)) & 7u;
-        const double a_zi = role == 4 ? ze : zi;
-        const double a_ze = role == 3 ? zi : ze;
-        const double a_qxi = role == 4 ? qxi_ref : qxi, a_qyi = role == 4 ? qyi_ref : qyi;
-        const double a_qxe = role == 3 ? qxe_ref : qxe, a_qye = role == 3 ? qye_ref : qye;
-        const double lg = role == 0 ? g : 0.0;
-        double f[3];
-        const double l = numerical_flux<double, Div>(ftype, f, a_zi, a_ze, a_qxi, a_qxe, a_qyi, a_qye, z_edge, nx, ny,
-                                                     lg, g, dv);
-        const bool nan = isnan(f[0]) || isnan(f[1]) || isnan(f[2]);
-        if (role == 0) {
-            if (nan) code = 1;
-            lam = l;
-        } else if (role == 3) {
-            lam = l;
-        } else {
-            if (role != 4 && !code && nan) code = role == 1 ? 2 : 3;
-            lam = rmax(lam, l);
-        }
-        const bool to_in = role == 3 || role == 1 || (role == 0 && (!WD || wdi == 1));
-        const bool to_ex = role == 4 || role == 2 || (role == 0 && (!WD || wde == 1));
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            if (to_in) fin[j] = f[j];
-            if (to_ex) fex[j] = f[j];
-        }
-    }
-    return lam;
-}
-
 /* Element stage modes: the RHS alone; SSP-RK2 stages 1 and 2; SSP(3,3) stages 2 and 3
  * (its stage 1 is MODE_STAGE1). */
 enum { MODE_RHS = 0, MODE_STAGE1 = 1, MODE_STAGE2 = 2, MODE_RK3_2 = 3, MODE_RK3_3 = 4 };
