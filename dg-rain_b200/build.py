@@ -10,6 +10,7 @@ operation so that the kernels reproduce the reference C step's arithmetic.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -71,16 +72,21 @@ def build(verbose: bool = False, ptxas_verbose: bool = False, force: bool = Fals
     all_src = [os.path.join(CSRC, f) for f in CU_SOURCES + C_SOURCES + DEPS]
     if not force and not _newer(lib, all_src + [__file__]):
         return lib
-    objs = []
+    objs, jobs = [], []
     for f in C_SOURCES:
         o = os.path.join(build_dir, f + ".o")
-        _run(["gcc", *CC_FLAGS, "-c", os.path.join(CSRC, f), "-o", o], verbose)
+        jobs.append((["gcc", *CC_FLAGS, "-c", os.path.join(CSRC, f), "-o", o], verbose))
         objs.append(o)
     for f in CU_SOURCES:
         o = os.path.join(build_dir, f + ".o")
         extra = ["-Xptxas", "-v"] if ptxas_verbose else []
-        _run([nvcc, *NVCC_FLAGS, *dflags, *extra, "-c", os.path.join(CSRC, f), "-o", o], verbose or ptxas_verbose)
+        jobs.append(([nvcc, *NVCC_FLAGS, *dflags, *extra, "-c", os.path.join(CSRC, f), "-o", o],
+                     verbose or ptxas_verbose))
         objs.append(o)
+    # the translation units are independent: compiled side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for fut in [ex.submit(_run, cmd, v) for cmd, v in jobs]:
+            fut.result()
     tmp = lib + ".tmp"
     _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp, *objs, "-lm"], verbose)
     os.replace(tmp, lib)

@@ -134,6 +134,24 @@ DGR_DEV void l2_prefetch_slice(const T *p0, int ld, int planes, int base, int n)
                      : "memory");
 }
 
+/* L2 prefetch of the geometry of elements [base, base + n) (whole tiles when tiled: the
+ * allocation holds every tile in full), in chunks of 4 KB over the block's threads. */
+DGR_DEV void prefetch_geometry(const MeshDev &m, int base, int n)
+{
+    if (!DGR_GEO_TILED) {
+        l2_prefetch_slice(m.geo, m.ldE, NG, base, n);
+        return;
+    }
+    if (n <= 0) return;
+    const char *p0 = reinterpret_cast<const char *>(m.geo + geo_offset(base & ~31, m.ldE));
+    const unsigned bytes = (unsigned)(((base + n + 31) >> 5) - (base >> 5)) * NG * 32 * 8;
+    for (unsigned off = threadIdx.x * 4096u; off < bytes; off += blockDim.x * 4096u) {
+        const unsigned len = min(4096u, bytes - off);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(__cvta_generic_to_global(p0 + off)), "r"(len)
+                     : "memory");
+    }
+}
+
 /* ------------------------------------------------------------------ edges ---- */
 
 /* One edge (2DCode/compute2DL.c:17-331): traces, ghost state, Roe flux(es); stores Fhat.n
@@ -320,7 +338,8 @@ DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, co
     if (ldm<COH>(&ck->done)) return;
     const double rain = ck->rain;
     const int ld = m.ldE;
-    const double *G = m.geo + el;
+    const double *G = m.geo + geo_offset(el, ld);
+    const int gs = geo_stride(ld);
     double F[3][3];
     if (!gather_flux<COH>(m, flux, el, F)) return;
     double zr[3], qxr[3], qyr[3];
@@ -335,8 +354,8 @@ DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, co
     const double dt = (MODE == MODE_RHS) ? 0.0 : ldm<COH>(&ck->dt);
     double w[3][3], a[3];
     bool rcp_ok = true;
-    const auto geo = [G, ld](int j) { return G[(size_t)j * ld]; };
-    const PlaneZGeo zg{G, ld};
+    const auto geo = [G, gs](int j) { return G[(size_t)j * gs]; };
+    const PlaneZGeo zg{G, gs};
     element_core<MODE, double, decltype(geo), PlaneZGeo, decltype(uin), RCP>(F, zr, qxr, qyr, geo, zg, uin, local_g,
                                                                           rain, dt, w, a, &rcp_ok);
     if (RCP && !rcp_ok) {
@@ -359,7 +378,7 @@ __global__ void __launch_bounds__(BS, 512 / BS) k_element(const __grid_constant_
 {
     /* the block's geometry planes are requested from DRAM at once instead of in the order
      * the element computation reaches them (measured: 4 % off this kernel) */
-    l2_prefetch_slice(m.geo, m.ldE, NG, blockIdx.x * BS, min(BS, m.ne - blockIdx.x * BS));
+    prefetch_geometry(m, blockIdx.x * BS, min(BS, m.ne - blockIdx.x * BS));
     const int el = blockIdx.x * BS + threadIdx.x;
     if (el < m.ne) element_item<MODE>(m, S, U, wd, flux, out, avg, clk, g, el);
 }
@@ -844,9 +863,10 @@ static __global__ void k_element_setup(int ne, int ldE, const int *__restrict__ 
     el2v[2 * ldE + i] = v2;
     const double xv[3] = {x[v0], x[v1], x[v2]}, yv[3] = {y[v0], y[v1], y[v2]}, zv[3] = {z[v0], z[v1], z[v2]};
     const double nfv[3] = {nfric[v0], nfric[v1], nfric[v2]};
-    double *G = geo + i;
+    double *G = geo + geo_offset(i, ldE);
+    const int gs = geo_stride(ldE);
     element_geometry(xv, yv, zv, nfv, n_el ? n_el[i] : -1.0, g,
-                     [G, ldE](int j, double val) { G[(size_t)j * ldE] = val; });
+                     [G, gs](int j, double val) { G[(size_t)j * gs] = val; });
 }
 
 /* the Manning power on n arguments (diagnostic entry point) */

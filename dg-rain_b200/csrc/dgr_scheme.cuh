@@ -37,6 +37,19 @@ enum {
     NG = 63
 };
 
+/* Storage of the planes: tiles of 32 consecutive elements, each tile's NG planes one after
+ * another (element el, plane j at ((el / 32) * NG + j) * 32 + el % 32).  A warp reads 256
+ * contiguous bytes per plane as with whole planes, and a block's geometry is one
+ * contiguous range.  DGR_GEO_TILED=0 (measurement builds): whole planes of stride ldE. */
+#ifndef DGR_GEO_TILED
+#define DGR_GEO_TILED 1
+#endif
+DGR_HD size_t geo_offset(int el, int ldE)
+{
+    return DGR_GEO_TILED ? (size_t)(el >> 5) * (NG * 32) + (el & 31) : (size_t)el;
+}
+DGR_HD int geo_stride(int ldE) { return DGR_GEO_TILED ? 32 : ldE; }
+
 /* Per-element factors of 2DCode/2DInnerProducts.c and 2DCode/compute2DL.c:373-382 from the
  * vertex coordinates, depths and Manning n (nel >= 0: per-element n, else the node
  * average), each with the reference's own expression; set(j, value) stores plane j. */

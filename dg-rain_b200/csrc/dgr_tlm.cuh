@@ -286,13 +286,14 @@ __global__ void __launch_bounds__(128) k_tlm_element(MeshDev m, const double *__
                                                      double *__restrict__ avg, double *__restrict__ avg_x,
                                                      const DevClock *clk, double g, const double *__restrict__ dt_n)
 {
-    l2_prefetch_slice(m.geo, m.ldE, NG, blockIdx.x * blockDim.x, min((int)blockDim.x, m.ne - (int)(blockIdx.x * blockDim.x)));
+    prefetch_geometry(m, blockIdx.x * blockDim.x, min((int)blockDim.x, m.ne - (int)(blockIdx.x * blockDim.x)));
     const int el = blockIdx.x * blockDim.x + threadIdx.x;
     if (el >= m.ne) return;
     const T *tag = nullptr;
     const int sid = m.el_sid ? m.el_sid[el] : 0;
     const int ld = m.ldE;
-    const double *G = m.geo + el;
+    const double *G = m.geo + geo_offset(el, ld);
+    const int gs = geo_stride(ld);
     T F[3][3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -312,7 +313,7 @@ __global__ void __launch_bounds__(128) k_tlm_element(MeshDev m, const double *__
         qyr[k] = lane(tag, S[(6 + k) * ld + el], Sx[(6 + k) * ld + el]);
     }
     const double local_g = (wd[el] == 0) ? 0.0 : g;
-    const auto geo = [G, ld](int j) { return G[(size_t)j * ld]; };
+    const auto geo = [G, gs](int j) { return G[(size_t)j * gs]; };
     const double zvx[3] = {zx[m.el2v[el]], zx[m.el2v[ld + el]], zx[m.el2v[2 * ld + el]]};
     const LaneZGeo<T> zg = lane_zgeo<T>(geo, zvx, n_el ? n_el[el] : -1.0, nelx ? nelx[el] : 0.0, g);
     const auto uin = [U, Ux, ld, el, tag](int v, int k) {
@@ -498,7 +499,7 @@ __global__ void __launch_bounds__(128, DGR_ADJ_MINB_ELEMENT) k_adj_element(MeshD
                                                      double *__restrict__ nbar, const double *__restrict__ n_el,
                                                      double g, const double *__restrict__ dt_n)
 {
-    l2_prefetch_slice(m.geo, m.ldE, NG, blockIdx.x * blockDim.x, min((int)blockDim.x, m.ne - (int)(blockIdx.x * blockDim.x)));
+    prefetch_geometry(m, blockIdx.x * blockDim.x, min((int)blockDim.x, m.ne - (int)(blockIdx.x * blockDim.x)));
     const int el = blockIdx.x * blockDim.x + threadIdx.x;
     if (el >= m.ne) return;
     const int ld = m.ldE, lb = m.ldN;
@@ -523,9 +524,10 @@ __global__ void __launch_bounds__(128, DGR_ADJ_MINB_ELEMENT) k_adj_element(MeshD
         qyr[k] = S[(6 + k) * ld + el];
     }
     const double local_g = (wd[el] == 0) ? 0.0 : g;
-    const double *G = m.geo + el;
-    const auto geo = [G, ld](int j) { return G[(size_t)j * ld]; };
-    const PlaneZGeo zg{G, ld};
+    const double *G = m.geo + geo_offset(el, ld);
+    const int gs = geo_stride(ld);
+    const auto geo = [G, gs](int j) { return G[(size_t)j * gs]; };
+    const PlaneZGeo zg{G, gs};
     double Fb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Sb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     double midzb[3] = {0, 0, 0}, gnnb[3] = {0, 0, 0}, gradzb[2] = {0, 0};
     element_core_rev<MODE>(wb, zr, qxr, qyr, geo, zg, local_g, dt_n[m.el_sid ? m.el_sid[el] : 0], Fb, Sb, midzb, gnnb, gradzb);
