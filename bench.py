@@ -649,6 +649,9 @@ def headline(ens, adj, cal) -> dict:
         h["tlm_vs_adjoint_max_rel"] = adj["tlm_vs_adjoint_max_rel"]
     if ok(cal):
         h["calibration_adjoint_over_forward"] = round(cal["adjoint_over_forward"], 3)
+        if "n_error" in cal:
+            h["calibration_n_error"] = [round(cal["n_error_initial"], 4), round(cal["n_error"], 4),
+                                        cal["lbfgs_iterations"], cal["steps"]]
     return h
 
 
@@ -701,7 +704,7 @@ def main():
     ap.add_argument("--calib-scenarios", type=int, default=64)
     ap.add_argument("--calib-steps", type=int, default=200)
     ap.add_argument("--calib-ckpt", type=int, default=50)
-    ap.add_argument("--calib-iterations", type=int, default=0)
+    ap.add_argument("--calib-iterations", type=int, default=3)
     ap.add_argument("--no-calibration", action="store_true")
     ap.add_argument("--io", action="store_true",
                     help="the mesh-ingest and .dat-writer comparison also at N > 1 (on by default at N = 1)")
@@ -795,8 +798,12 @@ def main():
         wdp = lib.dgr_host_alloc(m.num_el * 4)
         host["wd"] = np.ctypeslib.as_array((C.c_int * m.num_el).from_address(wdp))
         host["z"][:], host["qx"][:], host["qy"][:], host["wd"][:] = st
-        bz = np.zeros(m.num_edges)
-        bq = np.zeros(m.num_edges)
+        # the caller's boundary arrays exist before the run, as the reference's globals do:
+        # filled here so that their first-touch page faults fall outside the timed region
+        bz = np.empty(m.num_edges)
+        bq = np.empty(m.num_edges)
+        bz.fill(0.0)
+        bq.fill(0.0)
         typ = m.bdry
         nbnd = int((typ != 0).sum())
         tidal = np.nonzero(typ == 2)[0]  # the edges boundary_conditions() rewrites each step
@@ -826,7 +833,7 @@ def main():
                "d2h_bytes_per_step": int(8 + state_bytes / args.e2e_steps),
                "steps": args.e2e_steps,
                "path": "dgr_upload_state, per step dgr_set_boundary + dgr_step (oneTimeStep2D), "
-                       "dgr_download_state; pageable->pinned host buffers"}
+                       "dgr_download_state; pinned host buffers (dgr_host_alloc)"}
         for k in ("z", "qx", "qy"):
             lib.dgr_host_free(C.c_void_p(host[k].ctypes.data))
         lib.dgr_host_free(C.c_void_p(wdp))

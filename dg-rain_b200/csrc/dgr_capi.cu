@@ -69,6 +69,10 @@ void drop_graph(dgr_ctx *c)
     if (c->graph) cudaGraphDestroy(c->graph);
     c->graph_exec = nullptr;
     c->graph = nullptr;
+    if (c->stage_graph_exec) cudaGraphExecDestroy(c->stage_graph_exec);
+    if (c->stage_graph) cudaGraphDestroy(c->stage_graph);
+    c->stage_graph_exec = nullptr;
+    c->stage_graph = nullptr;
 }
 
 static void release(dgr_ctx *c)
@@ -1057,6 +1061,34 @@ static int check_barrier(dgr_ctx *c)
     return flag ? DGR_ERR_TIMEOUT : DGR_OK;
 }
 
+/* The RK stages of one host-driven step (dgr_step) captured into a graph of their own,
+ * on the first call after the context's launches last changed (drop_graph); where the
+ * capture fails the stages run eagerly. */
+static void build_stage_graph(dgr_ctx *c)
+{
+    cudaStream_t s = c->stream;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    for (int st = 0; st < c->p.rk_stages; ++st) launch_stage(c, st, false);
+    cudaError_t e = cudaGetLastError();
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(s, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return;
+    }
+    if (cudaGraphInstantiate(&c->stage_graph_exec, g, 0) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphDestroy(g);
+        c->stage_graph_exec = nullptr;
+        return;
+    }
+    c->stage_graph = g;
+}
+
 extern "C" int dgr_step(dgr_ctx *c, double time, double dt, double *max_lambda)
 {
     NvtxRange nv("dgr_step");
@@ -1064,10 +1096,16 @@ extern "C" int dgr_step(dgr_ctx *c, double time, double dt, double *max_lambda)
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     CK(cudaEventRecord(c->ev0, s));
+    if (!c->stage_graph_exec) build_stage_graph(c);
     k_clock_set<<<1, 1, 0, s>>>(c->clk, time, dt);
     c->launches++;
     launch_wd_refresh(c);
-    for (int st = 0; st < c->p.rk_stages; ++st) launch_stage(c, st, true);
+    if (c->stage_graph_exec) {
+        CK(cudaGraphLaunch(c->stage_graph_exec, s));
+        c->launches += (long long)c->p.rk_stages * (c->p.order == 2 ? 2 : 4 + DGR_EDGE_RCP + DGR_LIMIT_RCP);
+    } else {
+        for (int st = 0; st < c->p.rk_stages; ++st) launch_stage(c, st, true);
+    }
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev1, s));
     if (c->p.wet_dry) {

@@ -94,6 +94,8 @@ struct dgr_ctx {
     int fusion; /* 0, 1 or 2 */
     cudaGraph_t graph;
     cudaGraphExec_t graph_exec;
+    cudaGraph_t stage_graph;          /* the RK stages of one dgr_step, without the clock */
+    cudaGraphExec_t stage_graph_exec;
     dgr::AdjointState *adj; /* discrete adjoint storage, created on first use */
     /* gauge series recorded by the device loop (dgr_set_gauges) */
     int gauge_n, gauge_cap;
