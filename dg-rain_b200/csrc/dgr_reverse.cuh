@@ -491,14 +491,14 @@ DGR_HD void flux_core_rev(double zi, double qxi, double qyi, double ze, double q
     b.zed += r.zed;
 }
 
-/* Reverse of the RT0 fit (Cramer's rule): adjoints of (a, b, c) -> adjoints of R1..R3. */
+/* Reverse of the RT0 fit (Cramer's rule): adjoints of (a, b, c) -> adjoints of R1..R3 (idM = 1/dM). */
 DGR_HD void rt0_fit_rev(double ab, double bb, double cb, double M11, double M12, double M13, double M21, double M22,
-                        double M23, double M31, double M32, double M33, double dM, double &R1b, double &R2b,
+                        double M23, double M31, double M32, double M33, double idM, double &R1b, double &R2b,
                         double &R3b)
 {
-    R1b += (ab * (M23 * M32 - M22 * M33) - bb * (M23 * M31 - M21 * M33) + cb * (M22 * M31 - M21 * M32)) / dM;
-    R2b += (ab * (M12 * M33 - M13 * M32) - bb * (M11 * M33 - M13 * M31) + cb * (M11 * M32 - M12 * M31)) / dM;
-    R3b += (ab * (M13 * M22 - M12 * M23) - bb * (M13 * M21 - M11 * M23) + cb * (M12 * M21 - M11 * M22)) / dM;
+    R1b += (ab * (M23 * M32 - M22 * M33) - bb * (M23 * M31 - M21 * M33) + cb * (M22 * M31 - M21 * M32)) * idM;
+    R2b += (ab * (M12 * M33 - M13 * M32) - bb * (M11 * M33 - M13 * M31) + cb * (M11 * M32 - M12 * M31)) * idM;
+    R3b += (ab * (M13 * M22 - M12 * M23) - bb * (M13 * M21 - M11 * M23) + cb * (M12 * M21 - M11 * M22)) * idM;
 }
 
 /*
@@ -519,6 +519,10 @@ DGR_HD void element_core_rev(const double wb[3][3], const double zr[3], const do
     const double aj = geo(G_AJ), ajw = geo(G_AJW);
     const double weight = 1.0 / 6;
     const double m11 = geo(G_M11);
+    /* The quotients below only scale derivatives (no decision of the forward depends on
+     * them), so they are taken as products with one reciprocal per divisor: their last bit
+     * does not matter, their count does (this kernel is latency-bound). */
+    const double idM = 1.0 / dM;
 
     /* RK combination w = cu u + cs s + cr dt rhs, and the diagonal mass inverse */
     double Xb[3][3];
@@ -534,16 +538,18 @@ DGR_HD void element_core_rev(const double wb[3][3], const double zr[3], const do
         }
 
     /* volume terms: forward values */
-    double H[3], u[3], v[3], sp[3], tau[3], midz[3], gnn[3];
+    double H[3], iH[3], u[3], v[3], sp[3], iP[3], tau[3], midz[3], gnn[3];
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
         midz[e] = zg.midz(e);
         gnn[e] = zg.gnn(e);
         H[e] = zr[e] + midz[e];
-        u[e] = qxr[e] / H[e];
-        v[e] = qyr[e] / H[e];
+        iH[e] = 1.0 / H[e];
+        u[e] = qxr[e] * iH[e];
+        v[e] = qyr[e] * iH[e];
         sp[e] = sqrt(u[e] * u[e] + v[e] * v[e]);
-        tau[e] = gnn[e] * sp[e] / pow43(H[e]);
+        iP[e] = 1.0 / pow43(H[e]);
+        tau[e] = gnn[e] * sp[e] * iP[e];
     }
     const double bedx = local_g * aj * zg.gradz(0) * weight;
     const double bedy = local_g * aj * zg.gradz(1) * weight;
@@ -574,7 +580,7 @@ DGR_HD void element_core_rev(const double wb[3][3], const double zr[3], const do
             cb += Xb[vv][bf] * geo(G_GP + 2 * bf + 1);
             bb += Xb[vv][bf] * geo(G_P + bf);
         }
-        rt0_fit_rev(aj * 0.5 * ab, aj * weight * bb, aj * 0.5 * cb, M11, M12, M13, M21, M22, M23, M31, M32, M33, dM,
+        rt0_fit_rev(aj * 0.5 * ab, aj * weight * bb, aj * 0.5 * cb, M11, M12, M13, M21, M22, M23, M31, M32, M33, idM,
                     Rb[vv][0], Rb[vv][1], Rb[vv][2]);
     }
 
@@ -597,15 +603,15 @@ DGR_HD void element_core_rev(const double wb[3][3], const double zr[3], const do
         Hb += prb * local_g * H[e];
         midzb[e] -= prb * local_g * midz[e];
         const double tb = taub[e];
-        const double P = pow43(H[e]);
-        gnnb[e] += tb * sp[e] / P;
-        Hb -= tb * tau[e] * (4.0 / 3.0) / H[e];
+        gnnb[e] += tb * sp[e] * iP[e];
+        Hb -= tb * tau[e] * (4.0 / 3.0) * iH[e];
         if (sp[e] != 0.0) {
-            const double spb = tb * gnn[e] / P;
-            const double ub = spb * u[e] / sp[e], vb = spb * v[e] / sp[e];
-            qxb += ub / H[e];
-            qyb += vb / H[e];
-            Hb -= (ub * u[e] + vb * v[e]) / H[e];
+            const double spb = tb * gnn[e] * iP[e];
+            const double isp = 1.0 / sp[e];
+            const double ub = spb * u[e] * isp, vb = spb * v[e] * isp;
+            qxb += ub * iH[e];
+            qyb += vb * iH[e];
+            Hb -= (ub * u[e] + vb * v[e]) * iH[e];
         }
         zrb[e] += Hb;
         midzb[e] += Hb;
@@ -636,7 +642,7 @@ DGR_HD void element_core_rev(const double wb[3][3], const double zr[3], const do
                 bb += fdb * (geo(G_XE + 2 * e + n) * nx[e] + geo(G_YE + 2 * e + n) * ny[e]);
                 cb += fdb * ny[e];
             }
-        rt0_fit_rev(ab, bb, cb, M11, M12, M13, M21, M22, M23, M31, M32, M33, dM, Fb[vv][0], Fb[vv][1], Fb[vv][2]);
+        rt0_fit_rev(ab, bb, cb, M11, M12, M13, M21, M22, M23, M31, M32, M33, idM, Fb[vv][0], Fb[vv][1], Fb[vv][2]);
     }
 }
 
