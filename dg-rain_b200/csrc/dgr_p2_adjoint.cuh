@@ -167,10 +167,13 @@ DGR_HD void p2_area_rev(const P2Ref &ref, const double S[3][P2_NM], const double
         }
         const double zq = ref.lam[q][0] * zv[0] + ref.lam[q][1] * zv[1] + ref.lam[q][2] * zv[2];
         const double H = uq[0] + zq;
-        const double u = uq[1] / H, vv = uq[2] / H;
+        /* these quotients only scale derivatives (no decision depends on them): products
+         * with one reciprocal per divisor, whose last bit does not matter */
+        const double iH = 1.0 / H;
+        const double u = uq[1] * iH, vv = uq[2] * iH;
         const double sp = sqrt(u * u + vv * vv);
-        const double P = pow43(H);
-        const double tau = gnn * sp / P;
+        const double iP = 1.0 / pow43(H);
+        const double tau = gnn * sp * iP;
         const double wj = 2.0 * ref.wq[q] * detJ;
         /* adjoints of fx, fy, src */
         double fxb[3] = {0, 0, 0}, fyb[3] = {0, 0, 0}, srcb[3] = {0, 0, 0};
@@ -206,20 +209,21 @@ DGR_HD void p2_area_rev(const P2Ref &ref, const double S[3][P2_NM], const double
         q1b -= tau * srcb[1];
         q2b -= tau * srcb[2];
         /* tau = gnn sp / H^(4/3) */
-        gnnb += taub * sp / P;
-        Hb -= taub * tau * (4.0 / 3.0) / H;
+        gnnb += taub * sp * iP;
+        Hb -= taub * tau * (4.0 / 3.0) * iH;
         if (sp != 0.0) {
-            const double spb = taub * gnn / P;
-            ub += spb * u / sp;
-            vb += spb * vv / sp;
+            const double spb = taub * gnn * iP;
+            const double isp = 1.0 / sp;
+            ub += spb * u * isp;
+            vb += spb * vv * isp;
         }
         /* p = g (H^2 - zq^2) / 2 */
         Hb += pb * g * H;
         zqb -= pb * g * zq;
         /* u = q1 / H, vv = q2 / H */
-        q1b += ub / H;
-        q2b += vb / H;
-        Hb -= (ub * u + vb * vv) / H;
+        q1b += ub * iH;
+        q2b += vb * iH;
+        Hb -= (ub * u + vb * vv) * iH;
         zb += Hb;
         zqb += Hb;
 #pragma unroll
