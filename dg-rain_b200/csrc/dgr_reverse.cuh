@@ -56,16 +56,34 @@ DGR_HD void normal_flux_rev(const double fb[3], double h, double u, double v, do
 DGR_HD void roe_flux_rev(const double fhb[3], double zeta_in, double zeta_ex, double qx_in, double qx_ex, double qy_in,
                          double qy_ex, double z_edge, double nx, double ny, double local_g, double g, RoeBar &b)
 {
-    /* forward values, same expressions as roe_flux */
+    /* forward values, same expressions as roe_flux (the entropy fix's selections depend
+     * on them): the quotients through one reciprocal per divisor, corrected to the IEEE
+     * bits (div_rcp), and plain divisions where that is not valid */
     const double h_in = zeta_in + z_edge, h_ex = zeta_ex + z_edge;
-    const double u_in = qx_in / h_in, u_ex = qx_ex / h_ex;
-    const double v_in = qy_in / h_in, v_ex = qy_ex / h_ex;
     const double jump[3] = {zeta_in - zeta_ex, qx_in - qx_ex, qy_in - qy_ex};
     const double s_in = sqrt(h_in), s_ex = sqrt(h_ex);
     const double h_hat = 0.5 * (h_in + h_ex);
     const double D = s_in + s_ex;
-    const double u_hat = (u_in * s_in + u_ex * s_ex) / D;
-    const double v_hat = (v_in * s_in + v_ex * s_ex) / D;
+    double u_in, u_ex, v_in, v_ex, u_hat, v_hat;
+    {
+        RcpDiv dv;
+        const auto bi = dv.by(h_in), be = dv.by(h_ex);
+        u_in = dv.div(qx_in, bi);
+        u_ex = dv.div(qx_ex, be);
+        v_in = dv.div(qy_in, bi);
+        v_ex = dv.div(qy_ex, be);
+        const auto bd = dv.by(D);
+        u_hat = dv.div(u_in * s_in + u_ex * s_ex, bd);
+        v_hat = dv.div(v_in * s_in + v_ex * s_ex, bd);
+        if (!dv.ok) {
+            u_in = qx_in / h_in;
+            u_ex = qx_ex / h_ex;
+            v_in = qy_in / h_in;
+            v_ex = qy_ex / h_ex;
+            u_hat = (u_in * s_in + u_ex * s_ex) / D;
+            v_hat = (v_in * s_in + v_ex * s_ex) / D;
+        }
+    }
     const double c = sqrt(g * h_hat);
     const double un_in = u_in * nx + v_in * ny, un_ex = u_ex * nx + v_ex * ny;
     const double c_in = sqrt(g * h_in), c_ex = sqrt(g * h_ex);
