@@ -266,7 +266,7 @@ class Solver:
 def _schedule_methods(cls):
     """Schedule controls shared by Solver and Ensemble (dgr_set_schedule / dgr_autotune)."""
 
-    def set_schedule(self, block_size: int = 128, fusion: int = 0) -> None:
+    def set_schedule(self, block_size: int = 64, fusion: int = 0) -> None:
         _lib.check(self.lib.dgr_set_schedule(self.ctx, block_size, fusion), "dgr_set_schedule")
 
     def get_schedule(self):

@@ -284,8 +284,9 @@ DGR_API int dgr_ensemble_run(dgr_ctx *ctx, int nsteps, const double *final_time,
 DGR_API int dgr_ensemble_last_error(dgr_ctx *ctx, int scenario, int *code, int *index, int *step);
 
 /* Schedule of the device loop: block size (elements per block of the element and limiter
- * work: 64, 128, 256) and fusion depth (0: ten kernels per step; 1: one persistent
- * cooperative kernel per RK stage; 2: one per step, clock included).  dgr_autotune times
+ * work: 64, the default, 128 or 256) and fusion depth (0, the default: ten kernels per
+ * step; 1: one persistent cooperative kernel per RK stage; 2: one per step, clock
+ * included).  dgr_autotune times
  * trial_steps steps of every schedule from the current state (restored afterwards),
  * keeps the fastest and reports it; ms_out (9 entries or NULL) gets ms per step at index
  * 3*b + f, b = 0,1,2 for 64,128,256.  Results do not depend on the schedule. */
