@@ -369,14 +369,15 @@ static void recorded_stage(dgr_ctx *c, int j, int stage, const double *S, double
     const bool wd = c->p.wet_dry != 0;
     double *R = seg_R(c, j, stage), *avg = seg_avg(c, j, stage), *bnd = seg_B(c, j, stage);
     launch_edge(c, S, wd_in, stage, 2 * stage);
+    const unsigned ne64 = blocks(c->ne, 64); /* the element kernel in blocks of 64, as the plain step's default */
     if (mode == MODE_STAGE1)
-        k_element<MODE_STAGE1, 128><<<nb, 128, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
+        k_element<MODE_STAGE1, 64><<<ne64, 64, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
     else if (mode == MODE_STAGE2)
-        k_element<MODE_STAGE2, 128><<<nb, 128, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
+        k_element<MODE_STAGE2, 64><<<ne64, 64, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
     else if (mode == MODE_RK3_2)
-        k_element<MODE_RK3_2, 128><<<nb, 128, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
+        k_element<MODE_RK3_2, 64><<<ne64, 64, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
     else
-        k_element<MODE_RK3_3, 128><<<nb, 128, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
+        k_element<MODE_RK3_3, 64><<<ne64, 64, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
     k_node_bounds<<<blocks(c->nn, 256), 256, 0, s>>>(m, avg, bnd);
     if (wd)
         k_limit_to<true><<<nb, 128, 0, s>>>(m, R, OUT, bnd, wd_in, wd_out, c->clk, c->p.H0, c->p.VELZERO,
