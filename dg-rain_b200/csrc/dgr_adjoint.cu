@@ -378,7 +378,7 @@ static void recorded_stage(dgr_ctx *c, int j, int stage, const double *S, double
         k_element<MODE_RK3_2, 64><<<ne64, 64, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
     else
         k_element<MODE_RK3_3, 64><<<ne64, 64, 0, s>>>(m, S, U, wd_in, c->flux, R, avg, c->clk, c->p.g);
-    k_node_bounds<<<blocks(c->nn, 256), 256, 0, s>>>(m, avg, bnd);
+    k_node_bounds<<<blocks(c->nn, DGR_NODE_BS), DGR_NODE_BS, 0, s>>>(m, avg, bnd);
     if (wd)
         k_limit_to<true><<<nb, 128, 0, s>>>(m, R, OUT, bnd, wd_in, wd_out, c->clk, c->p.H0, c->p.VELZERO,
                                             2 * stage + 1);
@@ -466,7 +466,8 @@ static void reverse_stage(dgr_ctx *c, int j, int n, int stage)
         ADJ_EL(MODE_RK3_3);
 #undef ADJ_EL
 #define ADJ_EDGE(W, F) \
-    k_adj_edge<W, F><<<blocks(c->nf, 256), 256, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn, a->fbar, lamS, a->zeb, g)
+    k_adj_edge<W, F><<<blocks(c->nf, DGR_ADJ_EDGE_BS), DGR_ADJ_EDGE_BS, 0, s>>>(m, S, wd_in, c->bzeta, c->bqn,   \
+                                                                          a->fbar, lamS, a->zeb, g)
     if (c->p.flux == 0) { /* the reference's Roe flux, compiled alone */
         if (wd)
             ADJ_EDGE(true, 0);

@@ -795,7 +795,7 @@ template <bool WD, int FT>
 static void launch_edge_ft(dgr_ctx *c, const double *S, const int *wd, int lam_slot, int phase)
 {
     const MeshDev m = mesh_dev(c);
-    k_edge_flux<WD, FT><<<blocks(c->nf, 256), 256, 0, c->stream>>>(m, S, wd, c->bzeta, c->bqn, c->flux, c->clk,
+    k_edge_flux<WD, FT><<<blocks(c->nf, DGR_EDGE_BS), DGR_EDGE_BS, 0, c->stream>>>(m, S, wd, c->bzeta, c->bqn, c->flux, c->clk,
                                                                    lam_slot, phase, c->p.g);
     if (DGR_EDGE_RCP) {
         k_edge_redo<WD, FT><<<c->num_sms, 256, 0, c->stream>>>(m, S, wd, c->bzeta, c->bqn, c->flux, c->clk,
@@ -882,7 +882,7 @@ void launch_stage(dgr_ctx *c, int stage, bool count)
     }
     {
         NvtxRange r("k_node_bounds");
-        k_node_bounds<<<blocks(c->nn, 256), 256, 0, c->stream>>>(mesh_dev(c), c->avg, c->bounds);
+        k_node_bounds<<<blocks(c->nn, DGR_NODE_BS), DGR_NODE_BS, 0, c->stream>>>(mesh_dev(c), c->avg, c->bounds);
     }
     {
         NvtxRange r("k_limit");
@@ -1188,7 +1188,7 @@ extern "C" int dgr_slope_limiter(dgr_ctx *c)
     const MeshDev m = mesh_dev(c);
     k_clock_set<<<1, 1, 0, s>>>(c->clk, 0.0, 0.0);
     k_avg<<<blocks(c->ne, 256), 256, 0, s>>>(m, c->U, c->avg);
-    k_node_bounds<<<blocks(c->nn, 256), 256, 0, s>>>(m, c->avg, c->bounds);
+    k_node_bounds<<<blocks(c->nn, DGR_NODE_BS), DGR_NODE_BS, 0, s>>>(m, c->avg, c->bounds);
     int *dl = c->p.record_decisions ? c->dec : nullptr;
     k_limit<true, false, false, 128><<<blocks(c->ne, 128), 128, 0, s>>>(m, c->U, c->bounds, c->wdA, c->wdA, c->clk,
                                                                          c->p.H0, c->p.VELZERO, 0, dl, nullptr);
@@ -1617,7 +1617,7 @@ extern "C" int dgr_profile_step(dgr_ctx *c, int nsteps, double *kernel_ms, int n
             default: launch_element<MODE_RK3_3>(c, S, wd_in, OUT);
             }
             cudaEventRecord(ev[2], s);
-            k_node_bounds<<<blocks(c->nn, 256), 256, 0, s>>>(mesh_dev(c), c->avg, c->bounds);
+            k_node_bounds<<<blocks(c->nn, DGR_NODE_BS), DGR_NODE_BS, 0, s>>>(mesh_dev(c), c->avg, c->bounds);
             cudaEventRecord(ev[3], s);
             if (wd)
                 launch_limit<true, true, true>(c, OUT, wd_in, wd_out, 2 * stage + 1, nullptr, nullptr);

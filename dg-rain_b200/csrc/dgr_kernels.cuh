@@ -23,12 +23,17 @@
 #include "dgr_forcing.h"
 #include "dgr_scheme.cuh"
 
-/* Minimum resident blocks per SM requested from the compiler for the edge kernel
- * (register cap 65536 / (256 x blocks)); chosen by measurement, overridable at build time.
- * The element kernels are capped at 128 registers and the limiter kernels at 85
- * (launch bounds 512/BS and 768/BS blocks of BS threads). */
+/* Threads per block of the edge kernel, and the minimum resident blocks per SM requested
+ * from the compiler for it (register cap 65536 / (DGR_EDGE_BS x blocks) = 85, so 80);
+ * chosen by measurement (4,000,000 triangles: 0.332 ms per launch in blocks of 128, 0.338
+ * in blocks of 64, 0.352 in blocks of 256), overridable at build time.  The element
+ * kernels are capped at 128 registers (launch bounds 512/BS blocks of BS threads) and the
+ * limiter kernels at 64 (DGR_LIMIT_THREADS_PER_SM below). */
+#ifndef DGR_EDGE_BS
+#define DGR_EDGE_BS 128
+#endif
 #ifndef DGR_MINB_EDGE
-#define DGR_MINB_EDGE 3
+#define DGR_MINB_EDGE (768 / DGR_EDGE_BS)
 #endif
 /* 1: the edge and limiter kernels take their divisions through shared reciprocals
  * (div_rcp), queueing the items where that is not valid for a plain-division redo launch;
@@ -246,7 +251,7 @@ DGR_DEV void block_max_speed(double lam, int sid, bool valid, DevClock *clk, int
 }
 
 template <bool WD, int FT>
-__global__ void __launch_bounds__(256, DGR_MINB_EDGE) k_edge_flux(const __grid_constant__ MeshDev m, const double *__restrict__ S,
+__global__ void __launch_bounds__(DGR_EDGE_BS, DGR_MINB_EDGE) k_edge_flux(const __grid_constant__ MeshDev m, const double *__restrict__ S,
                                                                   const int *__restrict__ wd,
                                                                   const double *__restrict__ bzeta,
                                                                   const double *__restrict__ bqn,
@@ -415,7 +420,10 @@ DGR_DEV void node_item(const MeshDev &m, const double *avg, double *bounds, int 
     bounds[5 * l + n] = mn2;
 }
 
-static __global__ void __launch_bounds__(256) k_node_bounds(MeshDev m, const double *__restrict__ avg,
+#ifndef DGR_NODE_BS /* threads per block of the node-bounds kernel */
+#define DGR_NODE_BS 256
+#endif
+static __global__ void __launch_bounds__(DGR_NODE_BS) k_node_bounds(MeshDev m, const double *__restrict__ avg,
                                                      double *__restrict__ bounds)
 {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;

@@ -28,8 +28,11 @@
 
 /* Minimum resident blocks per SM of the reverse kernels (register caps 65536 / (threads x
  * blocks)); chosen by measurement, overridable at build time. */
+#ifndef DGR_ADJ_EDGE_BS /* threads per block of the reverse edge kernel */
+#define DGR_ADJ_EDGE_BS 256
+#endif
 #ifndef DGR_ADJ_MINB_EDGE
-#define DGR_ADJ_MINB_EDGE 2
+#define DGR_ADJ_MINB_EDGE (512 / DGR_ADJ_EDGE_BS)
 #endif
 #ifndef DGR_ADJ_MINB_ELEMENT
 #define DGR_ADJ_MINB_ELEMENT 4
@@ -562,7 +565,7 @@ __global__ void __launch_bounds__(128, DGR_ADJ_MINB_ELEMENT) k_adj_element(MeshD
 /* edge reverse: Roe flux(es), ghost states; adds the trace adjoints into the slots of the
  * adjacent elements (each slot belongs to one edge side) and the mid-edge depth adjoint */
 template <bool WD, int FT = -1>
-__global__ void __launch_bounds__(256, DGR_ADJ_MINB_EDGE) k_adj_edge(MeshDev m, const double *__restrict__ S, const int *__restrict__ wd,
+__global__ void __launch_bounds__(DGR_ADJ_EDGE_BS, DGR_ADJ_MINB_EDGE) k_adj_edge(MeshDev m, const double *__restrict__ S, const int *__restrict__ wd,
                                                   const double *__restrict__ bzeta, const double *__restrict__ bqn,
                                                   const double *__restrict__ fbar, double *__restrict__ lamS,
                                                   double *__restrict__ zeb, double g)
