@@ -253,7 +253,9 @@ DGR_API int dgr_wet_dry_status(dgr_ctx *ctx);
 
 /* oneTimeStep2D(time, dt): one SSP-RK2 step of the device state with the current
  * boundary values; returns the max wave speed of the second stage (the reference's
- * max_lambda), from which the caller sets the next dt. */
+ * max_lambda), from which the caller sets the next dt.  The step's kernels are replayed
+ * from a CUDA graph that the first call (and the first after dgr_set_params or
+ * dgr_set_schedule) captures on the context's own stream. */
 DGR_API int dgr_step(dgr_ctx *ctx, double time, double dt, double *max_lambda);
 
 /* time_evolution(): up to nsteps steps while time < final_time, entirely on the device
