@@ -44,6 +44,11 @@
 #ifndef DGR_LIMIT_THREADS_PER_SM
 #define DGR_LIMIT_THREADS_PER_SM 1024
 #endif
+/* Resident threads per SM requested for the element kernel (register cap 65536 / this:
+ * 128 registers at 512). */
+#ifndef DGR_ELEMENT_THREADS_PER_SM
+#define DGR_ELEMENT_THREADS_PER_SM 512
+#endif
 #ifndef DGR_EDGE_RCP
 #define DGR_EDGE_RCP 1
 #endif
@@ -376,7 +381,7 @@ DGR_DEV void element_item(const MeshDev &m, const double *S, const double *U, co
 }
 
 template <int MODE, int BS>
-__global__ void __launch_bounds__(BS, 512 / BS) k_element(const __grid_constant__ MeshDev m, const double *__restrict__ S,
+__global__ void __launch_bounds__(BS, DGR_ELEMENT_THREADS_PER_SM / BS) k_element(const __grid_constant__ MeshDev m, const double *__restrict__ S,
                                                           const double *__restrict__ U, const int *__restrict__ wd,
                                                           const double *__restrict__ flux, double *__restrict__ out,
                                                           double *__restrict__ avg, const DevClock *clk, double g)
