@@ -27,8 +27,8 @@
  * from the compiler for it (register cap 65536 / (DGR_EDGE_BS x blocks) = 85, so 80);
  * chosen by measurement (4,000,000 triangles: 0.332 ms per launch in blocks of 128, 0.338
  * in blocks of 64, 0.352 in blocks of 256), overridable at build time.  The element
- * kernels are capped at 128 registers (launch bounds 512/BS blocks of BS threads) and the
- * limiter kernels at 64 (DGR_LIMIT_THREADS_PER_SM below). */
+ * kernels are capped at 128 registers and the limiter kernels at 64
+ * (DGR_ELEMENT_THREADS_PER_SM and DGR_LIMIT_THREADS_PER_SM below). */
 #ifndef DGR_EDGE_BS
 #define DGR_EDGE_BS 128
 #endif
