@@ -171,6 +171,20 @@ def test_run_bitexact_without_friction(dgrain, oracle_mod, mesh_c1):
     expect_same_run(dgrain, s, o, rc, t_o, dt_o, n_o, 150)
 
 
+@pytest.mark.parametrize("block_size", [64, 128, 256])
+def test_run_partial_tiles_and_blocks(dgrain, oracle_mod, block_size):
+    """A jittered 23 x 11-cell mesh (506 triangles: not a whole number of the geometry's
+    32-element tiles, nor of any block size) repeats the oracle bit for bit over 60 wet/dry
+    steps with every block size of the element and limiter kernels."""
+    m = no_friction(dgrain, dgrain.rectangle(23, 11, jitter=0.1, seed=4))
+    assert m.num_el % 32 != 0
+    st = land_film_state(dgrain, m)
+    s, o = make_pair(dgrain, oracle_mod, m, st, 1, cfl=0.3, tide_on=1, tide_amp=0.5)
+    s.set_schedule(block_size, 0)
+    rc, t_o, dt_o, n_o, _ = o.run(60, 1e9, 0.3, wet_dry=1, tide_on=1, amp=0.5)
+    expect_same_run(dgrain, s, o, rc, t_o, dt_o, n_o, 60)
+
+
 def test_run_golden_with_friction(dgrain):
     """120 wet/dry steps with tide and friction against the reference's own output."""
     g = load_golden("run120_wd_tide_rect1600.npz")
