@@ -73,6 +73,7 @@ void drop_graph(dgr_ctx *c)
     if (c->stage_graph) cudaGraphDestroy(c->stage_graph);
     c->stage_graph_exec = nullptr;
     c->stage_graph = nullptr;
+    c->stage_graph_tried = 0;
 }
 
 static void release(dgr_ctx *c)
@@ -1063,9 +1064,10 @@ static int check_barrier(dgr_ctx *c)
 
 /* The RK stages of one host-driven step (dgr_step) captured into a graph of their own,
  * on the first call after the context's launches last changed (drop_graph); where the
- * capture fails the stages run eagerly. */
+ * capture fails the stages run eagerly, without another attempt until then. */
 static void build_stage_graph(dgr_ctx *c)
 {
+    c->stage_graph_tried = 1;
     cudaStream_t s = c->stream;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGetLastError();
@@ -1098,7 +1100,7 @@ extern "C" int dgr_step(dgr_ctx *c, double time, double dt, double *max_lambda)
     CK(cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
     CK(cudaEventRecord(c->ev0, s));
-    if (!c->stage_graph_exec) build_stage_graph(c);
+    if (!c->stage_graph_exec && !c->stage_graph_tried) build_stage_graph(c);
     k_clock_set<<<1, 1, 0, s>>>(c->clk, time, dt);
     c->launches++;
     launch_wd_refresh(c);

@@ -96,6 +96,7 @@ struct dgr_ctx {
     cudaGraphExec_t graph_exec;
     cudaGraph_t stage_graph;          /* the RK stages of one dgr_step, without the clock */
     cudaGraphExec_t stage_graph_exec;
+    int stage_graph_tried;            /* its capture was attempted since the last drop_graph */
     dgr::AdjointState *adj; /* discrete adjoint storage, created on first use */
     /* gauge series recorded by the device loop (dgr_set_gauges) */
     int gauge_n, gauge_cap;
